@@ -1,0 +1,325 @@
+"""B200-native elastic reverse-time migration: Python front end of libertm.so.
+
+The C ABI (include/ertm.h) is the product boundary; this module is a thin
+ctypes mirror of it whose method names follow the reference's per-shot calls
+(3D_elastic_RTM/3D_forward_or_back_together.cu):
+
+    ctx = Context(Config(nx=..., ny=..., nz=..., dx=..., dy=..., dz=..., dt_ms=..., nt=...))
+    ctx.set_model(TRUE_MODEL, vp, vs, rho)
+    ctx.set_model(MIGRATION_MODEL, svp, svs, srho)
+    data = ctx.forward_together_using_real_model(shot)             # observed data
+    ctx.forward_together_using_smoothed_model(shot)                 # source pass
+    pp, ps, tp = ctx.backward_together_using_smoothed_model(shot, data)  # receiver pass
+
+Arrays are float32 with shape (nz, ny, nx) (x fastest).  Inputs and outputs
+may be numpy arrays (host) or CUDA torch tensors (passed by pointer, no copy).
+There is no CPU fallback: if libertm.so is missing or no GPU is present the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libertm.so")
+
+TRUE_MODEL, MIGRATION_MODEL = 0, 1
+BOUNDARY_CPML, BOUNDARY_SPONGE_COS, BOUNDARY_SPONGE_CUBIC = 0, 1, 2
+COEF_TAYLOR, COEF_REFERENCE12, COEF_USER = 0, 1, 2
+INJECT_ADD, INJECT_REPLACE = 1, 2
+FIELDS = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz", "tp", "vxp", "vyp", "vzp")
+ERRORS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENOTSUP",
+          -6: "EDEVICE"}
+
+
+class ErtmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Config(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
+                ("dt_ms", C.c_float), ("nt", C.c_int), ("src_steps", C.c_int),
+                ("order", C.c_int), ("coef_kind", C.c_int), ("coef", C.c_float * 8),
+                ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_float),
+                ("pml_f0", C.c_float), ("pml_vmax", C.c_float), ("sponge_coef", C.c_float),
+                ("device", C.c_int), ("reserved", C.c_int * 7)]
+
+
+class _Shot(C.Structure):
+    _fields_ = [("sx", C.c_int), ("sy", C.c_int), ("sz", C.c_int), ("nw", C.c_int),
+                ("wavelet", C.c_void_p),
+                ("rx0", C.c_int), ("nrx", C.c_int), ("drx", C.c_int),
+                ("ry0", C.c_int), ("nry", C.c_int), ("dry", C.c_int),
+                ("rz", C.c_int), ("inject_mode", C.c_int)]
+
+
+# every entry point of include/ertm.h: name -> (restype, argtypes)
+_P = C.c_void_p
+SIGNATURES = {
+    "ertm_abi_version": (C.c_int, []),
+    "ertm_create": (C.c_int, [C.POINTER(_Config), C.POINTER(_P)]),
+    "ertm_destroy": (C.c_int, [_P]),
+    "ertm_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "ertm_set_stream": (C.c_int, [_P, _P]),
+    "ertm_set_model": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "ertm_forward_together_using_real_model": (C.c_int, [_P, C.POINTER(_Shot), _P]),
+    "ertm_forward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot)]),
+    "ertm_backward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_rtm_shot": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_get_wavefield": (C.c_int, [_P, C.c_int, _P]),
+    "ertm_get_excitation": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "ertm_divcurl": (C.c_int, [_P, C.c_int, _P, _P, _P, _P]),
+    "ertm_propagate": (C.c_int, [_P, C.c_int, C.POINTER(_Shot), C.c_int]),
+    "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
+    "ertm_kernel_launches": (C.c_int64, [_P]),
+}
+
+_lib_handle: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """Load libertm.so (built by build.py); raise if it is missing."""
+    global _lib_handle
+    if _lib_handle is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libertm.so not built ({LIB_PATH}); run __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib_handle = L
+    return _lib_handle
+
+
+@dataclass
+class Config:
+    """Mirror of ertm_config (grid includes the absorbing layers; dt in ms)."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dz: float
+    dt_ms: float
+    nt: int
+    src_steps: int = 0
+    order: int = 8
+    coef_kind: int = COEF_TAYLOR
+    coef: tuple = ()
+    boundary: int = BOUNDARY_CPML
+    pml: tuple = (0, 0, 0, 0, 0, 0)
+    pml_r: float = 1e-3
+    pml_f0: float = 10.0
+    pml_vmax: float = 0.0
+    sponge_coef: float = 0.0
+    device: int = 0
+
+    def struct(self) -> _Config:
+        c = _Config()
+        for f in ("nx", "ny", "nz", "dx", "dy", "dz", "dt_ms", "nt", "src_steps", "order",
+                  "coef_kind", "boundary", "pml_r", "pml_f0", "pml_vmax", "sponge_coef", "device"):
+            setattr(c, f, getattr(self, f))
+        for i, v in enumerate(self.coef[:8]):
+            c.coef[i] = v
+        for i in range(6):
+            c.pml[i] = int(self.pml[i])
+        return c
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+
+@dataclass
+class Shot:
+    """Mirror of ertm_shot: explosive source cell, wavelet, receiver grid."""
+    sx: int
+    sy: int
+    sz: int
+    wavelet: np.ndarray
+    rx0: int = 0
+    nrx: int = 0
+    drx: int = 1
+    ry0: int = 0
+    nry: int = 1
+    dry: int = 1
+    rz: int = 0
+    inject_mode: int = INJECT_ADD
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def nrec(self) -> int:
+        return self.nrx * self.nry
+
+    def struct(self) -> _Shot:
+        s = _Shot()
+        s.sx, s.sy, s.sz = self.sx, self.sy, self.sz
+        w = self.wavelet
+        if _is_torch(w):
+            s.nw = int(w.numel())
+            s.wavelet = w.data_ptr()
+        else:
+            w = np.ascontiguousarray(w, np.float32)
+            self._keep[:] = [w]
+            s.nw = len(w)
+            s.wavelet = w.ctypes.data
+        s.rx0, s.nrx, s.drx = self.rx0, self.nrx, self.drx
+        s.ry0, s.nry, s.dry = self.ry0, self.nry, self.dry
+        s.rz, s.inject_mode = self.rz, self.inject_mode
+        return s
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a, n: int | None = None, writable: bool = False):
+    """Raw pointer of a float32/int32 numpy array or torch tensor (contiguous)."""
+    if a is None:
+        return None
+    if _is_torch(a):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        if n is not None and a.numel() != n:
+            raise ValueError(f"tensor has {a.numel()} elements, expected {n}")
+        return a.data_ptr()
+    if not isinstance(a, np.ndarray) or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be a C-contiguous numpy array")
+    if a.dtype not in (np.float32, np.int32):
+        raise ValueError(f"dtype {a.dtype}: float32/int32 expected")
+    if n is not None and a.size != n:
+        raise ValueError(f"array has {a.size} elements, expected {n}")
+    if writable and not a.flags["WRITEABLE"]:
+        raise ValueError("output array is read-only")
+    return a.ctypes.data
+
+
+class Context:
+    """One GPU context: device state of one grid (the reference's GPUdevice)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self._L = lib()
+        h = C.c_void_p()
+        self._cs = cfg.struct()
+        rc = self._L.ertm_create(C.byref(self._cs), C.byref(h))
+        if rc != 0:
+            raise ErtmError(rc, self._msg(None))
+        self._h = h
+
+    def _msg(self, h) -> str:
+        buf = C.create_string_buffer(1024)
+        self._L.ertm_last_error(h, buf, len(buf))
+        return buf.value.decode(errors="replace")
+
+    def _ck(self, rc: int):
+        if rc != 0:
+            raise ErtmError(rc, self._msg(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ertm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def ncell(self) -> int:
+        return self.cfg.nx * self.cfg.ny * self.cfg.nz
+
+    def _vol(self, out):
+        return np.zeros(self.cfg.shape, np.float32) if out is None else out
+
+    def set_stream(self, stream_ptr: int | None):
+        self._ck(self._L.ertm_set_stream(self._h, stream_ptr))
+
+    def set_model(self, which: int, vp, vs, rho):
+        n = self.ncell
+        args = [vp, vs, rho]
+        args = [a if _is_torch(a) else np.ascontiguousarray(a, np.float32) for a in args]
+        self._ck(self._L.ertm_set_model(self._h, which, *[_ptr(a, n) for a in args]))
+
+    def forward_together_using_real_model(self, shot: Shot, out=None):
+        n = 3 * self.cfg.nt * shot.nrec
+        if out is None:
+            out = np.zeros((3, self.cfg.nt, shot.nrec), np.float32)
+        s = shot.struct()
+        self._ck(self._L.ertm_forward_together_using_real_model(self._h, C.byref(s),
+                                                                _ptr(out, n, True)))
+        return out
+
+    def forward_together_using_smoothed_model(self, shot: Shot):
+        s = shot.struct()
+        self._ck(self._L.ertm_forward_together_using_smoothed_model(self._h, C.byref(s)))
+
+    def backward_together_using_smoothed_model(self, shot: Shot, data, pp=None, ps=None, tp=None):
+        n = self.ncell
+        pp, ps, tp = self._vol(pp), self._vol(ps), self._vol(tp)
+        d = data if _is_torch(data) else np.ascontiguousarray(data, np.float32)
+        s = shot.struct()
+        self._ck(self._L.ertm_backward_together_using_smoothed_model(
+            self._h, C.byref(s), _ptr(d, 3 * self.cfg.nt * shot.nrec), _ptr(pp, n, True),
+            _ptr(ps, n, True), _ptr(tp, n, True)))
+        return pp, ps, tp
+
+    def rtm_shot(self, shot: Shot, data, pp=None, ps=None, tp=None):
+        n = self.ncell
+        pp, ps, tp = self._vol(pp), self._vol(ps), self._vol(tp)
+        d = data if _is_torch(data) else np.ascontiguousarray(data, np.float32)
+        s = shot.struct()
+        self._ck(self._L.ertm_rtm_shot(self._h, C.byref(s), _ptr(d, 3 * self.cfg.nt * shot.nrec),
+                                       _ptr(pp, n, True), _ptr(ps, n, True), _ptr(tp, n, True)))
+        return pp, ps, tp
+
+    def get_wavefield(self, name_or_id, out=None):
+        fid = FIELDS.index(name_or_id) if isinstance(name_or_id, str) else int(name_or_id)
+        out = self._vol(out)
+        self._ck(self._L.ertm_get_wavefield(self._h, fid, _ptr(out, self.ncell, True)))
+        return out
+
+    def get_excitation(self):
+        n = self.ncell
+        amp = np.zeros(self.cfg.shape, np.float32)
+        t = np.zeros(self.cfg.shape, np.int32)
+        ev = [np.zeros(self.cfg.shape, np.float32) for _ in range(4)]
+        self._ck(self._L.ertm_get_excitation(self._h, _ptr(amp, n, True), _ptr(t, n, True),
+                                             *[_ptr(e, n, True) for e in ev]))
+        return {"amp": amp, "time": t, "evx": ev[0], "evy": ev[1], "evz": ev[2], "etp": ev[3]}
+
+    def divcurl(self, which: int = MIGRATION_MODEL):
+        n = self.ncell
+        outs = [np.zeros(self.cfg.shape, np.float32) for _ in range(4)]
+        self._ck(self._L.ertm_divcurl(self._h, which, *[_ptr(o, n, True) for o in outs]))
+        return tuple(outs)
+
+    def propagate(self, which: int, shot: Shot, nsteps: int):
+        s = shot.struct()
+        self._ck(self._L.ertm_propagate(self._h, which, C.byref(s), nsteps))
+
+    def time_kernels(self, shot: Shot, nsteps: int):
+        ms = (C.c_float * 2)()
+        s = shot.struct()
+        self._ck(self._L.ertm_time_kernels(self._h, C.byref(s), nsteps, ms))
+        return float(ms[0]), float(ms[1])
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._L.ertm_kernel_launches(self._h))

@@ -1,0 +1,917 @@
+// Host side of libertm: the C ABI declared in include/ertm.h.
+//
+// The context replaces the reference's GPUdevice struct and its globals
+// (3D_elastic_RTM/3D_elastic_modeling_typedef_struct:1-55,
+//  3D_elastic_RTM/3D_elastic_modeling_parameter:1-141).  It owns every device
+// buffer; passes are stream-ordered on the context stream and each public call
+// synchronises that stream before returning.  The whole grid lives on one GPU
+// (no z-slab decomposition, unlike the reference's exchange_device_nz_kernel_*).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ertm.h"
+#include "ertm_internal.cuh"
+
+using namespace ertm;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+enum Mode { MODE_MODEL = 0, MODE_SOURCE = 1, MODE_RECEIVER = 2, MODE_PLAIN = 3 };
+
+// axis of each C-PML memory-variable slot (0 x, 1 y, 2 z)
+const int kPsiAxis[NPSI] = {0, 1, 2, 1, 0, 2, 0, 2, 1, 0, 1, 2, 0, 1, 2, 0, 1, 2};
+// slots that exist in 2D (no y derivative, no vy/txy/tyz)
+const bool kPsi2D[NPSI] = {true, false, true, false, false, true, true, false, false,
+                           true, false, true, false, false, false, true, false, true};
+
+}  // namespace
+
+struct ertm_ctx {
+    ertm_config cfg{};
+    int R = 4;
+    Geom g{};
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    float coef[8] = {0};
+
+    float* f_base[NFIELD] = {nullptr};
+    float* f[NFIELD] = {nullptr};
+    // per model: M, MU, B, VP, VS (padded)
+    float* m_base[2][5] = {{nullptr}};
+    float* m[2][5] = {{nullptr}};
+    bool model_set[2] = {false, false};
+    float vpmax[2] = {0.f, 0.f};
+
+    // boundary
+    float* att[3] = {nullptr, nullptr, nullptr};
+    float* pa[3][2] = {{nullptr}};
+    float* pb[3][2] = {{nullptr}};
+    float* psi[NPSI] = {nullptr};
+    long long psi_n[NPSI] = {0};
+    float profile_vmax = -1.f;
+
+    // excitation and images (padded)
+    float* ex_amp2_base = nullptr;
+    int* ex_time_base = nullptr;
+    float* ex_v_base[3] = {nullptr};
+    float* ex_tp_base = nullptr;
+    float* img_base[3] = {nullptr};
+    bool have_excitation = false;
+    int last_shot_key = 0;
+
+    // staging
+    float* stage = nullptr;          // 3 contiguous volumes
+    float* traces = nullptr;
+    size_t traces_cap = 0;
+    float* wavelet = nullptr;
+    int wavelet_cap = 0;
+    int* it_d = nullptr;
+    float* vmax_d = nullptr;
+
+    std::string err;
+    long long launches = 0;
+};
+
+namespace {
+
+int fail(ertm_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    else g_create_error = buf;
+    return code;
+}
+
+#define CK(ctx, call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? ERTM_ENOMEM : ERTM_ECUDA, \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+Geom make_geom(const ertm_config& c, int R)
+{
+    Geom g{};
+    g.nx = c.nx;
+    g.ny = c.ny;
+    g.nz = c.nz;
+    g.R = R;
+    g.two_d = (c.ny == 1);
+    g.tyb = g.two_d ? TY2 : TY3;
+    g.hx = XH;
+    g.hy = g.two_d ? 0 : R;
+    g.hz = R;
+    g.px = round_up(2LL * g.hx + round_up(c.nx, TX), 32);
+    g.py = 2LL * g.hy + round_up(c.ny, g.tyb);
+    g.pz = 2LL * g.hz + c.nz + 1;
+    g.sy = g.px;
+    g.sz = g.px * g.py;
+    g.off0 = g.hz * g.sz + g.hy * g.sy + g.hx;
+    g.total = g.px * g.py * g.pz;
+    return g;
+}
+
+bool field_used(const Geom& g, int f)
+{
+    if (!g.two_d) return true;
+    return !(f == F_VY || f == F_TYY || f == F_TXY || f == F_TYZ || f == F_VYP);
+}
+
+int alloc_volume(ertm_ctx* c, float** base, float** origin)
+{
+    CK(c, cudaMalloc(base, sizeof(float) * c->g.total));
+    CK(c, cudaMemsetAsync(*base, 0, sizeof(float) * c->g.total, c->stream));
+    *origin = *base + c->g.off0;
+    return ERTM_OK;
+}
+
+int ensure_stage(ertm_ctx* c)
+{
+    if (c->stage) return ERTM_OK;
+    long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
+    CK(c, cudaMalloc(&c->stage, sizeof(float) * 3 * n));
+    return ERTM_OK;
+}
+
+__global__ void k_absmax(const float* __restrict__ v, long long n, float* out)
+{
+    float m = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(v[i]));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax((int*)out, __float_as_int(m));
+}
+
+// Fill host-side double profiles, upload as float.
+int upload_profiles(ertm_ctx* c, float vmax)
+{
+    const ertm_config& cf = c->cfg;
+    const Geom& g = c->g;
+    const double dts = cf.dt_ms / 1000.0;
+    int ns[3] = {g.nx, g.ny, g.nz};
+    double hs[3] = {cf.dx, cf.dy, cf.dz};
+    if (cf.boundary == ERTM_BOUNDARY_CPML) {
+        if (c->profile_vmax == vmax) return ERTM_OK;
+        double rc = cf.pml_r > 0 ? cf.pml_r : 1e-3;
+        double f0 = cf.pml_f0 > 0 ? cf.pml_f0 : 10.0;
+        for (int ax = 0; ax < 3; ax++) {
+            int n = ns[ax];
+            int w0 = cf.pml[2 * ax], w1 = cf.pml[2 * ax + 1];
+            if (ax == 1 && g.two_d) w0 = w1 = 0;
+            for (int h = 0; h < 2; h++) {
+                int stg = h == 0 ? 0 : (ax == 2 ? 1 : -1);
+                std::vector<float> a(n), b(n);
+                for (int i = 0; i < n; i++) {
+                    // C-PML (Komatitsch & Martin 2007), kappa = 1; see orc_cpml_profile
+                    double p = i + 0.5 * stg, dist = 0.0, L = 1.0;
+                    if (w0 > 0 && p < w0 - 1) { dist = (w0 - 1) - p; L = w0; }
+                    else if (w1 > 0 && p > n - w1) { dist = p - (n - w1); L = w1; }
+                    if (dist <= 0.0) { a[i] = 0.f; b[i] = 1.f; continue; }
+                    double Lm = L * hs[ax], x = dist * hs[ax] / Lm;
+                    double d0 = -3.0 * vmax * std::log(rc) / (2.0 * Lm);
+                    double d = d0 * x * x;
+                    double al = M_PI * f0 * (1.0 - x);
+                    if (al < 0) al = 0;
+                    double bb = std::exp(-(d + al) * dts);
+                    b[i] = (float)bb;
+                    a[i] = (float)(d * (bb - 1.0) / (d + al));
+                }
+                if (!c->pa[ax][h]) {
+                    CK(c, cudaMalloc(&c->pa[ax][h], sizeof(float) * n));
+                    CK(c, cudaMalloc(&c->pb[ax][h], sizeof(float) * n));
+                }
+                CK(c, cudaMemcpyAsync(c->pa[ax][h], a.data(), sizeof(float) * n,
+                                      cudaMemcpyHostToDevice, c->stream));
+                CK(c, cudaMemcpyAsync(c->pb[ax][h], b.data(), sizeof(float) * n,
+                                      cudaMemcpyHostToDevice, c->stream));
+                CK(c, cudaStreamSynchronize(c->stream));
+            }
+        }
+        c->profile_vmax = vmax;
+        return ERTM_OK;
+    }
+    if (c->att[0]) return ERTM_OK;
+    const double pai = 3.1415926;   // 3D_zzzzz:1
+    for (int ax = 0; ax < 3; ax++) {
+        int n = ns[ax];
+        std::vector<float> v(n, 0.f);
+        int w0 = cf.pml[2 * ax], w1 = cf.pml[2 * ax + 1];
+        if (!(ax == 1 && g.two_d)) {
+            float coe = cf.sponge_coef;
+            // coe_attenuation_3d_new2 (3D_zzzzz:261-300) / make_attenuation_new (zzzzz:238-280)
+            for (int i = 0; i < w0 && i < n; i++) {
+                float val;
+                if (cf.boundary == ERTM_BOUNDARY_SPONGE_COS)
+                    val = (float)(coe * (1.0 - std::cos(pai / 2 * (w0 - i - 1) / (w0 - 1))));
+                else {
+                    float x = (float)((w0 - 1.0 - i) / (w0 - 1.0));
+                    val = (float)(coe * std::pow(x * 1.0, 3.0));
+                }
+                v[i] += val;
+            }
+            for (int q = 0; q < w1; q++) {
+                int i = n - w1 + q;
+                if (i < 0) continue;
+                float val;
+                if (cf.boundary == ERTM_BOUNDARY_SPONGE_COS)
+                    val = (float)(coe * (1.0 - std::cos(pai / 2 * q / (w1 - 1))));
+                else {
+                    float x = (float)(q / (w1 - 1.0));
+                    val = (float)(coe * std::pow(x * 1.0, 3.0));
+                }
+                v[i] += val;
+            }
+        }
+        CK(c, cudaMalloc(&c->att[ax], sizeof(float) * n));
+        CK(c, cudaMemcpyAsync(c->att[ax], v.data(), sizeof(float) * n, cudaMemcpyHostToDevice,
+                              c->stream));
+    }
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int validate_shot(ertm_ctx* c, const ertm_shot* s, bool need_source)
+{
+    if (!s) return fail(c, ERTM_EINVAL, "shot is NULL");
+    const Geom& g = c->g;
+    if (need_source) {
+        if (s->sx < 0 || s->sx >= g.nx || s->sy < 0 || s->sy >= g.ny || s->sz < 0 || s->sz >= g.nz)
+            return fail(c, ERTM_EINVAL, "source cell (%d,%d,%d) outside the %dx%dx%d grid", s->sx,
+                        s->sy, s->sz, g.nx, g.ny, g.nz);
+        if (s->nw < 0 || (s->nw > 0 && !s->wavelet))
+            return fail(c, ERTM_EINVAL, "wavelet of %d samples with NULL pointer", s->nw);
+    }
+    if (s->nrx < 0 || s->nry < 0 || s->drx <= 0 || s->dry <= 0)
+        return fail(c, ERTM_EINVAL, "bad receiver grid (nrx=%d nry=%d drx=%d dry=%d)", s->nrx,
+                    s->nry, s->drx, s->dry);
+    if (g.two_d && (s->nry > 1 || s->ry0 != 0 || s->sy != 0))
+        return fail(c, ERTM_EINVAL, "2D grid: receivers and source must sit at y = 0");
+    if (s->inject_mode != 0 && s->inject_mode != ERTM_INJECT_ADD && s->inject_mode != ERTM_INJECT_REPLACE)
+        return fail(c, ERTM_EINVAL, "inject_mode %d", s->inject_mode);
+    return ERTM_OK;
+}
+
+int ensure_traces(ertm_ctx* c, size_t n)
+{
+    if (c->traces_cap >= n) return ERTM_OK;
+    if (c->traces) cudaFree(c->traces);
+    c->traces = nullptr;
+    c->traces_cap = 0;
+    CK(c, cudaMalloc(&c->traces, sizeof(float) * n));
+    c->traces_cap = n;
+    return ERTM_OK;
+}
+
+int ensure_excitation(ertm_ctx* c)
+{
+    if (c->ex_amp2_base) return ERTM_OK;
+    float* dummy;
+    int rc;
+    if ((rc = alloc_volume(c, &c->ex_amp2_base, &dummy))) return rc;
+    CK(c, cudaMalloc(&c->ex_time_base, sizeof(int) * c->g.total));
+    for (int q = 0; q < 3; q++) {
+        if (q == 1 && c->g.two_d) continue;
+        if ((rc = alloc_volume(c, &c->ex_v_base[q], &dummy))) return rc;
+    }
+    if ((rc = alloc_volume(c, &c->ex_tp_base, &dummy))) return rc;
+    return ERTM_OK;
+}
+
+int ensure_images(ertm_ctx* c)
+{
+    if (c->img_base[0]) return ERTM_OK;
+    float* dummy;
+    for (int q = 0; q < 3; q++) {
+        int rc = alloc_volume(c, &c->img_base[q], &dummy);
+        if (rc) return rc;
+    }
+    return ERTM_OK;
+}
+
+// Common kernel arguments for a pass in model `which`.
+void fill_args(ertm_ctx* c, int which, const ertm_shot* s, KArgs& a)
+{
+    const Geom& g = c->g;
+    std::memset(&a, 0, sizeof a);
+    for (int q = 0; q < NFIELD; q++) a.f[q] = c->f[q];
+    a.M = c->m[which][0];
+    a.MU = c->m[which][1];
+    a.B = c->m[which][2];
+    a.sy = g.sy;
+    a.sz = g.sz;
+    a.msy = g.sy;
+    a.msz = g.sz;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.kchunk = g.nz;
+    for (int n = 0; n < 8; n++) {
+        a.cx[n] = (float)(c->coef[n] / c->cfg.dx);
+        a.cy[n] = (float)(c->coef[n] / c->cfg.dy);
+        a.cz[n] = (float)(c->coef[n] / c->cfg.dz);
+    }
+    a.dt = c->cfg.dt_ms / 1000.f;
+    for (int ax = 0; ax < 3; ax++) {
+        a.att[ax] = c->att[ax];
+        for (int h = 0; h < 2; h++) {
+            a.pa[ax][h] = c->pa[ax][h];
+            a.pb[ax][h] = c->pb[ax][h];
+        }
+    }
+    for (int p = 0; p < NPSI; p++) a.psi[p] = c->psi[p];
+    for (int q = 0; q < 6; q++) a.w[q] = c->cfg.pml[q];
+    if (g.two_d) a.w[2] = a.w[3] = 0;
+    if (s) {
+        a.ssx = s->sx;
+        a.ssy = s->sy;
+        a.ssz = s->sz;
+        a.nw = s->nw;
+        a.rx0 = s->rx0;
+        a.nrx = s->nrx;
+        a.drx = s->drx;
+        a.ry0 = s->ry0;
+        a.nry = s->nry;
+        a.dry = s->dry;
+        a.rz = s->rz;
+        a.inject_mode = s->inject_mode == 0 ? ERTM_INJECT_ADD : s->inject_mode;
+    } else {
+        a.nw = 0;
+        a.drx = a.dry = 1;
+        a.rz = -1;
+    }
+    a.wavelet = c->wavelet;
+    a.nt = c->cfg.nt;
+    a.it_ptr = c->it_d;
+    a.ex_amp2 = c->ex_amp2_base ? c->ex_amp2_base + g.off0 : nullptr;
+    a.ex_time = c->ex_time_base ? c->ex_time_base + g.off0 : nullptr;
+    for (int q = 0; q < 3; q++) {
+        a.ex_v[q] = c->ex_v_base[q] ? c->ex_v_base[q] + g.off0 : nullptr;
+        a.img[q] = c->img_base[q] ? c->img_base[q] + g.off0 : nullptr;
+    }
+    a.ex_tp = c->ex_tp_base ? c->ex_tp_base + g.off0 : nullptr;
+}
+
+// z planes per CTA: enough CTAs to fill the GPU at least twice.
+int choose_kchunk(const ertm_ctx* c)
+{
+    const Geom& g = c->g;
+    long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    long long want = 4LL * sms;
+    int chunks = (int)std::max(1LL, std::min((long long)g.nz, (want + cols - 1) / cols));
+    // keep at least 8R planes per chunk so the 2R-plane queue warm-up stays small
+    int kc = (g.nz + chunks - 1) / chunks;
+    kc = std::max(kc, std::min(g.nz, 8 * c->R));
+    return kc;
+}
+
+int reset_state(ertm_ctx* c)
+{
+    for (int q = 0; q < NFIELD; q++)
+        if (c->f_base[q]) CK(c, cudaMemsetAsync(c->f_base[q], 0, sizeof(float) * c->g.total, c->stream));
+    for (int p = 0; p < NPSI; p++)
+        if (c->psi[p]) CK(c, cudaMemsetAsync(c->psi[p], 0, sizeof(float) * c->psi_n[p], c->stream));
+    return ERTM_OK;
+}
+
+int upload_wavelet(ertm_ctx* c, const ertm_shot* s)
+{
+    if (s->nw <= 0) return ERTM_OK;
+    if (c->wavelet_cap < s->nw) {
+        if (c->wavelet) cudaFree(c->wavelet);
+        c->wavelet = nullptr;
+        CK(c, cudaMalloc(&c->wavelet, sizeof(float) * s->nw));
+        c->wavelet_cap = s->nw;
+    }
+    CK(c, cudaMemcpyAsync(c->wavelet, s->wavelet, sizeof(float) * s->nw, cudaMemcpyDefault, c->stream));
+    return ERTM_OK;
+}
+
+// One pass of `nsteps` steps.  MODE_MODEL records into `traces` ([3][nt][nrec],
+// device), MODE_RECEIVER injects from it.
+int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, float* traces)
+{
+    if (!c->model_set[which])
+        return fail(c, ERTM_ESTATE, "%s model not set", which ? "migration" : "true");
+    int rc;
+    float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[which];
+    if ((rc = upload_profiles(c, vmax))) return rc;
+    if ((rc = reset_state(c))) return rc;
+    if (mode != MODE_RECEIVER && (rc = upload_wavelet(c, s))) return rc;
+    KArgs a;
+    fill_args(c, which, s, a);
+    a.kchunk = choose_kchunk(c);
+    a.traces = traces;
+    const bool cpml = c->cfg.boundary == ERTM_BOUNDARY_CPML;
+    const int R = c->R;
+    int epi = EPI_NONE;
+    bool psplit = false, record = false;
+    if (mode == MODE_SOURCE) { epi = EPI_EXCITE; psplit = true; }
+    if (mode == MODE_RECEIVER) { epi = EPI_IMAGE; psplit = true; }
+    if (mode == MODE_MODEL) record = (traces != nullptr);
+    if (mode == MODE_RECEIVER) a.nw = 0;
+    int it0 = (mode == MODE_RECEIVER) ? nsteps - 1 : 0;
+    int dir = (mode == MODE_RECEIVER) ? -1 : 1;
+    CK(c, launch_set_int(c->it_d, it0, c->stream));
+    c->launches++;
+    if (mode == MODE_RECEIVER && nsteps > 0) {
+        CK(c, launch_inject(a, nsteps - 1, c->stream));
+        c->launches++;
+    }
+    for (int step = 0; step < nsteps; step++) {
+        CK(c, launch_stress(R, c->g, a, cpml, psplit, c->stream));
+        CK(c, launch_velocity(R, c->g, a, cpml, epi, record, c->stream));
+        CK(c, launch_advance(c->it_d, dir, c->stream));
+        c->launches += 3;
+    }
+    return ERTM_OK;
+}
+
+int copy_out_volume(ertm_ctx* c, const float* padded_origin, float* out)
+{
+    if (!out) return ERTM_OK;
+    if (is_device_ptr(out)) {
+        CK(c, launch_gather(c->g, padded_origin, out, c->stream));
+        c->launches++;
+        return ERTM_OK;
+    }
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
+    CK(c, launch_gather(c->g, padded_origin, c->stage, c->stream));
+    c->launches++;
+    CK(c, cudaMemcpyAsync(out, c->stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+long long nrec_of(const ertm_shot* s) { return (long long)s->nrx * s->nry; }
+
+}  // namespace
+
+extern "C" {
+
+int ertm_abi_version(void) { return ERTM_ABI_VERSION; }
+
+int ertm_create(const ertm_config* cfg, ertm_ctx** out)
+{
+    if (!out) return fail(nullptr, ERTM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!cfg) return fail(nullptr, ERTM_EINVAL, "config is NULL");
+    const ertm_config& c = *cfg;
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1)
+        return fail(nullptr, ERTM_EINVAL, "grid %dx%dx%d", c.nx, c.ny, c.nz);
+    if (!(c.dx > 0) || !(c.dy > 0) || !(c.dz > 0) || !(c.dt_ms > 0))
+        return fail(nullptr, ERTM_EINVAL, "spacings and dt must be positive");
+    if (c.nt < 1) return fail(nullptr, ERTM_EINVAL, "nt = %d", c.nt);
+    if (c.order != 8 && c.order != 12)
+        return fail(nullptr, ERTM_ENOTSUP, "order %d (8 or 12 supported)", c.order);
+    if (c.boundary < 0 || c.boundary > 2) return fail(nullptr, ERTM_EINVAL, "boundary %d", c.boundary);
+    if (c.coef_kind == ERTM_COEF_REFERENCE12 && c.order != 12)
+        return fail(nullptr, ERTM_EINVAL, "reference coefficients need order 12");
+    if (c.coef_kind < 0 || c.coef_kind > 2) return fail(nullptr, ERTM_EINVAL, "coef_kind %d", c.coef_kind);
+    for (int q = 0; q < 6; q++)
+        if (c.pml[q] < 0) return fail(nullptr, ERTM_EINVAL, "negative absorbing width");
+    int ns[3] = {c.nx, c.ny, c.nz};
+    for (int ax = 0; ax < 3; ax++) {
+        if (ax == 1 && c.ny == 1) continue;
+        if (c.pml[2 * ax] + c.pml[2 * ax + 1] > ns[ax])
+            return fail(nullptr, ERTM_EINVAL, "absorbing widths exceed the grid on axis %d", ax);
+        if (c.boundary != ERTM_BOUNDARY_CPML && (c.pml[2 * ax] == 1 || c.pml[2 * ax + 1] == 1))
+            return fail(nullptr, ERTM_EINVAL, "sponge widths must be 0 or >= 2");
+    }
+    if (c.src_steps < 0 || c.src_steps > c.nt)
+        return fail(nullptr, ERTM_EINVAL, "src_steps %d outside [0, nt]", c.src_steps);
+    for (int q = 0; q < 7; q++)
+        if (c.reserved[q]) return fail(nullptr, ERTM_EINVAL, "reserved fields must be zero");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, ERTM_ECUDA, "no CUDA device");
+    }
+    if (c.device < 0 || c.device >= ndev) return fail(nullptr, ERTM_EINVAL, "device %d of %d", c.device, ndev);
+
+    ertm_ctx* x = new (std::nothrow) ertm_ctx();
+    if (!x) return fail(nullptr, ERTM_ENOMEM, "host allocation");
+    x->cfg = c;
+    x->R = c.order / 2;
+    x->device = c.device;
+    x->g = make_geom(c, x->R);
+    int rc = ERTM_OK;
+    auto bail = [&](int code) {
+        g_create_error = x->err;
+        ertm_destroy(x);
+        return code;
+    };
+    if (cudaSetDevice(c.device) != cudaSuccess) {
+        fail(x, ERTM_ECUDA, "cudaSetDevice(%d)", c.device);
+        return bail(ERTM_ECUDA);
+    }
+    if (cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        fail(x, ERTM_ECUDA, "stream create");
+        return bail(ERTM_ECUDA);
+    }
+    x->stream = x->own_stream;
+    // difference coefficients
+    if (c.coef_kind == ERTM_COEF_USER) {
+        for (int n = 0; n < 8; n++) x->coef[n] = n <= x->R ? c.coef[n] : 0.f;
+    } else if (c.coef_kind == ERTM_COEF_REFERENCE12) {
+        const float rc12[7] = {0.0f, 1.2213363647f, -0.096931457519f, 0.017447662353f,
+                               -0.0029672895159f, 0.00035900539822f, -0.00002184781161f};
+        for (int n = 0; n < 7; n++) x->coef[n] = rc12[n];
+    } else {
+        // Taylor coefficients: solve sum_n c_n (2n-1)^(2m-1) = delta_{m1}
+        const int R = x->R;
+        double A[8][9];
+        for (int m = 0; m < R; m++) {
+            for (int n = 0; n < R; n++) A[m][n] = std::pow(2.0 * n + 1.0, 2.0 * m + 1.0);
+            A[m][R] = (m == 0);
+        }
+        for (int cc = 0; cc < R; cc++) {
+            int p = cc;
+            for (int r = cc + 1; r < R; r++) if (std::fabs(A[r][cc]) > std::fabs(A[p][cc])) p = r;
+            for (int k = 0; k <= R; k++) std::swap(A[cc][k], A[p][k]);
+            for (int r = 0; r < R; r++) {
+                if (r == cc) continue;
+                double f = A[r][cc] / A[cc][cc];
+                for (int k = cc; k <= R; k++) A[r][k] -= f * A[cc][k];
+            }
+        }
+        x->coef[0] = 0.f;
+        for (int n = 0; n < R; n++) x->coef[n + 1] = (float)(A[n][R] / A[n][n]);
+    }
+    for (int q = 0; q < NFIELD; q++) {
+        if (!field_used(x->g, q)) continue;
+        if ((rc = alloc_volume(x, &x->f_base[q], &x->f[q]))) return bail(rc);
+    }
+    if (c.boundary == ERTM_BOUNDARY_CPML) {
+        const Geom& g = x->g;
+        for (int p = 0; p < NPSI; p++) {
+            if (g.two_d && !kPsi2D[p]) continue;
+            int ax = kPsiAxis[p];
+            long long w = c.pml[2 * ax] + c.pml[2 * ax + 1];
+            long long n = ax == 0 ? (long long)g.nz * g.ny * w
+                        : ax == 1 ? (long long)g.nz * w * g.nx
+                                  : w * g.ny * g.nx;
+            x->psi_n[p] = n;
+            if (n == 0) continue;
+            if (cudaMalloc(&x->psi[p], sizeof(float) * n) != cudaSuccess) {
+                cudaGetLastError();
+                fail(x, ERTM_ENOMEM, "C-PML memory variables");
+                return bail(ERTM_ENOMEM);
+            }
+        }
+    }
+    if (cudaMalloc(&x->it_d, sizeof(int)) != cudaSuccess || cudaMalloc(&x->vmax_d, sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        fail(x, ERTM_ENOMEM, "counters");
+        return bail(ERTM_ENOMEM);
+    }
+    if (cudaStreamSynchronize(x->stream) != cudaSuccess) {
+        fail(x, ERTM_ECUDA, "%s", cudaGetErrorString(cudaGetLastError()));
+        return bail(ERTM_ECUDA);
+    }
+    *out = x;
+    return ERTM_OK;
+}
+
+int ertm_destroy(ertm_ctx* c)
+{
+    if (!c) return ERTM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int q = 0; q < NFIELD; q++) cudaFree(c->f_base[q]);
+    for (int w = 0; w < 2; w++)
+        for (int q = 0; q < 5; q++) cudaFree(c->m_base[w][q]);
+    for (int ax = 0; ax < 3; ax++) {
+        cudaFree(c->att[ax]);
+        for (int h = 0; h < 2; h++) {
+            cudaFree(c->pa[ax][h]);
+            cudaFree(c->pb[ax][h]);
+        }
+    }
+    for (int p = 0; p < NPSI; p++) cudaFree(c->psi[p]);
+    cudaFree(c->ex_amp2_base);
+    cudaFree(c->ex_time_base);
+    for (int q = 0; q < 3; q++) {
+        cudaFree(c->ex_v_base[q]);
+        cudaFree(c->img_base[q]);
+    }
+    cudaFree(c->ex_tp_base);
+    cudaFree(c->stage);
+    cudaFree(c->traces);
+    cudaFree(c->wavelet);
+    cudaFree(c->it_d);
+    cudaFree(c->vmax_d);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return ERTM_OK;
+}
+
+int ertm_last_error(const ertm_ctx* c, char* buf, size_t len)
+{
+    if (!buf || len == 0) return ERTM_EINVAL;
+    const std::string& s = c ? c->err : g_create_error;
+    size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+    return ERTM_OK;
+}
+
+int ertm_set_stream(ertm_ctx* c, void* stream)
+{
+    if (!c) return ERTM_EINVAL;
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return ERTM_OK;
+}
+
+int ertm_set_model(ertm_ctx* c, int which, const float* vp, const float* vs, const float* rho)
+{
+    if (!c) return ERTM_EINVAL;
+    if (which != 0 && which != 1) return fail(c, ERTM_EINVAL, "which = %d", which);
+    if (!vp || !vs || !rho) return fail(c, ERTM_EINVAL, "NULL model array");
+    CK(c, cudaSetDevice(c->device));
+    int rc;
+    for (int q = 0; q < 5; q++)
+        if (!c->m_base[which][q] && (rc = alloc_volume(c, &c->m_base[which][q], &c->m[which][q])))
+            return rc;
+    if ((rc = ensure_stage(c))) return rc;
+    const long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
+    const float* src[3] = {vp, vs, rho};
+    for (int q = 0; q < 3; q++)
+        CK(c, cudaMemcpyAsync(c->stage + q * n, src[q], sizeof(float) * n, cudaMemcpyDefault, c->stream));
+    CK(c, launch_model(c->g, c->stage, c->stage + n, c->stage + 2 * n, c->m[which][0], c->m[which][1],
+                       c->m[which][2], c->stream));
+    CK(c, launch_scatter(c->g, c->stage, c->m[which][3], c->stream));
+    CK(c, launch_scatter(c->g, c->stage + n, c->m[which][4], c->stream));
+    CK(c, cudaMemsetAsync(c->vmax_d, 0, sizeof(float), c->stream));
+    k_absmax<<<std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(c->stage, n, c->vmax_d);
+    CK(c, cudaGetLastError());
+    c->launches += 4;
+    float vm = 0.f;
+    CK(c, cudaMemcpyAsync(&vm, c->vmax_d, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (!(vm > 0.f) || !std::isfinite(vm)) return fail(c, ERTM_EINVAL, "model vp has no positive finite maximum");
+    c->vpmax[which] = vm;
+    c->model_set[which] = true;
+    return ERTM_OK;
+}
+
+int ertm_forward_together_using_real_model(ertm_ctx* c, const ertm_shot* s, float* data_out)
+{
+    if (!c) return ERTM_EINVAL;
+    CK(c, cudaSetDevice(c->device));
+    int rc = validate_shot(c, s, true);
+    if (rc) return rc;
+    const long long nrec = nrec_of(s);
+    const size_t nd = 3 * (size_t)c->cfg.nt * nrec;
+    const bool dev = is_device_ptr(data_out);
+    float* traces = nullptr;
+    if (data_out && nd) {
+        if (dev) traces = data_out;
+        else {
+            if ((rc = ensure_traces(c, nd))) return rc;
+            traces = c->traces;
+        }
+        CK(c, cudaMemsetAsync(traces, 0, sizeof(float) * nd, c->stream));
+    }
+    if ((rc = run_pass(c, 0, s, MODE_MODEL, c->cfg.nt, traces))) return rc;
+    if (data_out && nd && !dev)
+        CK(c, cudaMemcpyAsync(data_out, traces, sizeof(float) * nd, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int ertm_forward_together_using_smoothed_model(ertm_ctx* c, const ertm_shot* s)
+{
+    if (!c) return ERTM_EINVAL;
+    CK(c, cudaSetDevice(c->device));
+    int rc = validate_shot(c, s, true);
+    if (rc) return rc;
+    if ((rc = ensure_excitation(c))) return rc;
+    const Geom& g = c->g;
+    CK(c, cudaMemsetAsync(c->ex_amp2_base, 0, sizeof(float) * g.total, c->stream));
+    CK(c, cudaMemsetAsync(c->ex_time_base, 0, sizeof(int) * g.total, c->stream));
+    for (int q = 0; q < 3; q++)
+        if (c->ex_v_base[q]) CK(c, cudaMemsetAsync(c->ex_v_base[q], 0, sizeof(float) * g.total, c->stream));
+    CK(c, cudaMemsetAsync(c->ex_tp_base, 0, sizeof(float) * g.total, c->stream));
+    int nsrc = c->cfg.src_steps > 0 ? c->cfg.src_steps : 2 * c->cfg.nt / 3;
+    c->have_excitation = false;
+    if ((rc = run_pass(c, 1, s, MODE_SOURCE, nsrc, nullptr))) return rc;
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->have_excitation = true;
+    return ERTM_OK;
+}
+
+int ertm_backward_together_using_smoothed_model(ertm_ctx* c, const ertm_shot* s, const float* data_in,
+                                                float* img_pp, float* img_ps, float* img_tp)
+{
+    if (!c) return ERTM_EINVAL;
+    CK(c, cudaSetDevice(c->device));
+    int rc = validate_shot(c, s, false);
+    if (rc) return rc;
+    if (!c->have_excitation) return fail(c, ERTM_ESTATE, "receiver pass before a source pass");
+    if (!data_in && nrec_of(s) > 0) return fail(c, ERTM_EINVAL, "data_in is NULL");
+    if ((rc = ensure_images(c))) return rc;
+    const Geom& g = c->g;
+    for (int q = 0; q < 3; q++) CK(c, cudaMemsetAsync(c->img_base[q], 0, sizeof(float) * g.total, c->stream));
+    const long long nrec = nrec_of(s);
+    const size_t nd = 3 * (size_t)c->cfg.nt * nrec;
+    float* traces = nullptr;
+    if (nd) {
+        if (is_device_ptr(data_in)) traces = const_cast<float*>(data_in);
+        else {
+            if ((rc = ensure_traces(c, nd))) return rc;
+            CK(c, cudaMemcpyAsync(c->traces, data_in, sizeof(float) * nd, cudaMemcpyHostToDevice, c->stream));
+            traces = c->traces;
+        }
+    }
+    if ((rc = run_pass(c, 1, s, MODE_RECEIVER, c->cfg.nt, traces))) return rc;
+    float* outs[3] = {img_pp, img_ps, img_tp};
+    for (int q = 0; q < 3; q++)
+        if ((rc = copy_out_volume(c, c->img_base[q] + g.off0, outs[q]))) return rc;
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int ertm_rtm_shot(ertm_ctx* c, const ertm_shot* s, const float* data_in, float* img_pp, float* img_ps,
+                  float* img_tp)
+{
+    int rc = ertm_forward_together_using_smoothed_model(c, s);
+    if (rc) return rc;
+    return ertm_backward_together_using_smoothed_model(c, s, data_in, img_pp, img_ps, img_tp);
+}
+
+int ertm_get_wavefield(ertm_ctx* c, int field, float* out)
+{
+    if (!c) return ERTM_EINVAL;
+    if (field < 0 || field >= NFIELD) return fail(c, ERTM_EINVAL, "field %d", field);
+    if (!out) return fail(c, ERTM_EINVAL, "out is NULL");
+    CK(c, cudaSetDevice(c->device));
+    if (!c->f[field]) {
+        long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
+        if (is_device_ptr(out)) CK(c, cudaMemsetAsync(out, 0, sizeof(float) * n, c->stream));
+        else std::memset(out, 0, sizeof(float) * n);
+        CK(c, cudaStreamSynchronize(c->stream));
+        return ERTM_OK;
+    }
+    return copy_out_volume(c, c->f[field], out);
+}
+
+int ertm_get_excitation(ertm_ctx* c, float* amp, int32_t* time, float* evx, float* evy, float* evz,
+                        float* etp)
+{
+    if (!c) return ERTM_EINVAL;
+    if (!c->have_excitation) return fail(c, ERTM_ESTATE, "no source pass has run");
+    CK(c, cudaSetDevice(c->device));
+    const Geom& g = c->g;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    if (amp) {
+        CK(c, launch_sqrt_gather(g, c->ex_amp2_base + g.off0, c->stage, c->stream));
+        CK(c, cudaMemcpyAsync(amp, c->stage, sizeof(float) * n, cudaMemcpyDefault, c->stream));
+    }
+    if (time) {
+        CK(c, launch_gather_int(g, c->ex_time_base + g.off0, (int*)c->stage, c->stream));
+        CK(c, cudaMemcpyAsync(time, c->stage, sizeof(int) * n, cudaMemcpyDefault, c->stream));
+    }
+    CK(c, cudaStreamSynchronize(c->stream));
+    float* outs[4] = {evx, evy, evz, etp};
+    float* srcs[4] = {c->ex_v_base[0], c->ex_v_base[1], c->ex_v_base[2], c->ex_tp_base};
+    for (int q = 0; q < 4; q++) {
+        if (!outs[q]) continue;
+        if (!srcs[q]) {
+            if (is_device_ptr(outs[q])) CK(c, cudaMemsetAsync(outs[q], 0, sizeof(float) * n, c->stream));
+            else std::memset(outs[q], 0, sizeof(float) * n);
+            continue;
+        }
+        if ((rc = copy_out_volume(c, srcs[q] + g.off0, outs[q]))) return rc;
+    }
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int ertm_divcurl(ertm_ctx* c, int which, float* p, float* sx, float* sy, float* sz)
+{
+    if (!c) return ERTM_EINVAL;
+    if (which != 0 && which != 1) return fail(c, ERTM_EINVAL, "which = %d", which);
+    if (!c->model_set[which]) return fail(c, ERTM_ESTATE, "model %d not set", which);
+    if (!p || !sy || (!c->g.two_d && (!sx || !sz))) return fail(c, ERTM_EINVAL, "NULL output");
+    CK(c, cudaSetDevice(c->device));
+    const Geom& g = c->g;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    KArgs a;
+    fill_args(c, which, nullptr, a);
+    float* outs[4] = {p, sx, sy, sz};
+    bool dev[4];
+    float* tmp[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < 4; q++) {
+        dev[q] = is_device_ptr(outs[q]);
+        if (!outs[q] || (g.two_d && (q == 1 || q == 3))) continue;
+        if (dev[q]) tmp[q] = outs[q];
+        else CK(c, cudaMalloc(&tmp[q], sizeof(float) * n));
+    }
+    cudaError_t e = launch_divcurl(c->R, g, a, c->m[which][3], c->m[which][4], tmp[0], tmp[1], tmp[2],
+                                   tmp[3], c->stream);
+    c->launches++;
+    for (int q = 0; q < 4 && e == cudaSuccess; q++)
+        if (tmp[q] && !dev[q])
+            e = cudaMemcpyAsync(outs[q], tmp[q], sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    for (int q = 0; q < 4; q++)
+        if (tmp[q] && !dev[q]) cudaFree(tmp[q]);
+    if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "divcurl: %s", cudaGetErrorString(e));
+    return ERTM_OK;
+}
+
+int ertm_propagate(ertm_ctx* c, int which, const ertm_shot* s, int nsteps)
+{
+    if (!c) return ERTM_EINVAL;
+    if (which != 0 && which != 1) return fail(c, ERTM_EINVAL, "which = %d", which);
+    if (nsteps < 0) return fail(c, ERTM_EINVAL, "nsteps = %d", nsteps);
+    CK(c, cudaSetDevice(c->device));
+    int rc = validate_shot(c, s, true);
+    if (rc) return rc;
+    if ((rc = run_pass(c, which, s, MODE_MODEL, nsteps, nullptr))) return rc;
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
+{
+    if (!c || !ms) return ERTM_EINVAL;
+    if (nsteps < 1) return fail(c, ERTM_EINVAL, "nsteps = %d", nsteps);
+    CK(c, cudaSetDevice(c->device));
+    int rc = validate_shot(c, s, true);
+    if (rc) return rc;
+    if (!c->model_set[1]) return fail(c, ERTM_ESTATE, "migration model not set");
+    if ((rc = ensure_excitation(c))) return rc;
+    float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[1];
+    if ((rc = upload_profiles(c, vmax))) return rc;
+    if ((rc = reset_state(c))) return rc;
+    if ((rc = upload_wavelet(c, s))) return rc;
+    KArgs a;
+    fill_args(c, 1, s, a);
+    a.kchunk = choose_kchunk(c);
+    const bool cpml = c->cfg.boundary == ERTM_BOUNDARY_CPML;
+    cudaEvent_t ev[3];
+    for (int q = 0; q < 3; q++) CK(c, cudaEventCreate(&ev[q]));
+    CK(c, launch_set_int(c->it_d, 0, c->stream));
+    float tot[2] = {0.f, 0.f};
+    for (int step = 0; step < nsteps; step++) {
+        CK(c, cudaEventRecord(ev[0], c->stream));
+        CK(c, launch_stress(c->R, c->g, a, cpml, true, c->stream));
+        CK(c, cudaEventRecord(ev[1], c->stream));
+        CK(c, launch_velocity(c->R, c->g, a, cpml, EPI_EXCITE, false, c->stream));
+        CK(c, cudaEventRecord(ev[2], c->stream));
+        CK(c, launch_advance(c->it_d, 1, c->stream));
+        c->launches += 3;
+        CK(c, cudaEventSynchronize(ev[2]));
+        float t0, t1;
+        CK(c, cudaEventElapsedTime(&t0, ev[0], ev[1]));
+        CK(c, cudaEventElapsedTime(&t1, ev[1], ev[2]));
+        tot[0] += t0;
+        tot[1] += t1;
+    }
+    for (int q = 0; q < 3; q++) cudaEventDestroy(ev[q]);
+    c->have_excitation = false;
+    ms[0] = tot[0];
+    ms[1] = tot[1];
+    return ERTM_OK;
+}
+
+int64_t ertm_kernel_launches(const ertm_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"

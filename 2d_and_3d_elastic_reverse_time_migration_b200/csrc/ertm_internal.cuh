@@ -1,0 +1,107 @@
+// Internal types of libertm: device geometry, kernel argument block, launchers.
+//
+// HBM layout.  Every wavefield, model, excitation and image volume is one
+// allocation of `Geom::total` floats with zero halos: x is padded by XH floats
+// on both sides and the row pitch rounded up to 32 floats (128 B), y by R rows
+// (3D only), z by R planes.  Pointers passed to kernels point at cell (0,0,0),
+// so the stencil reads k*sz + j*sy + i +/- n without bounds checks; halo cells
+// are never written and stay zero, which is the reference's `radius` padding
+// (nnx_radius, viscoelastic_equation.cu:100).  Rows past nx and ny up to the
+// tile size are allocated too and stay zero.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ertm {
+
+constexpr int TX = 32;        // x tile = one warp
+constexpr int TY3 = 16;       // y tile of the 3D kernels
+constexpr int TY2 = 4;        // y (= independent 2D shot) tile of the 2D kernels
+constexpr int XH = 8;         // allocated x halo, floats (>= R, 32-byte aligned)
+
+enum Field {
+    F_VX, F_VY, F_VZ, F_TXX, F_TYY, F_TZZ, F_TXY, F_TXZ, F_TYZ, F_TP, F_VXP, F_VYP, F_VZP, NFIELD
+};
+
+// C-PML memory-variable slots: one per spatial derivative that enters an update.
+enum Psi {
+    P_EXX, P_EYY, P_EZZ, P_DYVX, P_DXVY, P_DZVX, P_DXVZ, P_DZVY, P_DYVZ,
+    P_DXTXX, P_DYTXY, P_DZTXZ, P_DXTXY, P_DYTYY, P_DZTYZ, P_DXTXZ, P_DYTYZ, P_DZTZZ, NPSI
+};
+
+enum Epilogue { EPI_NONE = 0, EPI_EXCITE = 1, EPI_IMAGE = 2 };
+
+struct Geom {
+    int nx, ny, nz, R;
+    int hx, hy, hz;
+    long long px, py, pz;   // allocated extents
+    long long sy, sz;       // strides (floats)
+    long long off0;         // offset of cell (0,0,0)
+    long long total;        // floats per volume
+    int two_d;
+    int tyb;                // y tile of the kernels for this grid
+};
+
+// Everything a step kernel reads; passed by value (param space).
+struct KArgs {
+    float* f[NFIELD];                // origin pointers
+    const float* M;                  // rho*vp^2
+    const float* MU;                 // rho*vs^2
+    const float* B;                  // 1/rho
+    long long sy, sz;                // field strides
+    long long msy, msz;              // model strides
+    int nx, ny, nz;
+    int kchunk;
+    float cx[8], cy[8], cz[8];       // c_n / h
+    float dt;
+    // sponge boundary: per-axis damping profiles (1/s), summed per cell
+    const float* att[3];
+    // C-PML: per axis, [0] integer points, [1] half points
+    const float* pa[3][2];
+    const float* pb[3][2];
+    float* psi[NPSI];
+    int w[6];
+    // source (it < nw only)
+    int ssx, ssy, ssz, nw;
+    const float* wavelet;
+    // receivers on a regular grid at depth rz
+    int rx0, nrx, drx, ry0, nry, dry, rz;
+    int inject_mode;
+    float* traces;                   // [3][nt][nrec], recorded or injected
+    int nt;
+    const int* it_ptr;               // current step index (device)
+    // excitation state and images (same geometry as the fields)
+    float* ex_amp2;
+    int* ex_time;
+    float* ex_v[3];
+    float* ex_tp;
+    float* img[3];
+};
+
+// Launchers (one translation unit per stencil radius).
+cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, bool cpml, bool psplit,
+                          cudaStream_t s);
+cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, bool cpml, int epi,
+                            bool record, cudaStream_t s);
+cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s);
+cudaError_t launch_stress_r6(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s);
+cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
+                               cudaStream_t s);
+cudaError_t launch_velocity_r6(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
+                               cudaStream_t s);
+
+// Small kernels (aux.cu)
+cudaError_t launch_scatter(const Geom& g, const float* src, float* dst, cudaStream_t s);
+cudaError_t launch_gather(const Geom& g, const float* src, float* dst, cudaStream_t s);
+cudaError_t launch_gather_int(const Geom& g, const int* src, int* dst, cudaStream_t s);
+cudaError_t launch_model(const Geom& g, const float* vp, const float* vs, const float* rho,
+                         float* M, float* MU, float* B, cudaStream_t s);
+cudaError_t launch_inject(const KArgs& a, int it, cudaStream_t s);
+cudaError_t launch_advance(int* it_ptr, int delta, cudaStream_t s);
+cudaError_t launch_set_int(int* p, int v, cudaStream_t s);
+cudaError_t launch_sqrt_gather(const Geom& g, const float* amp2, float* out, cudaStream_t s);
+cudaError_t launch_divcurl(int R, const Geom& g, const KArgs& a, const float* vp, const float* vs,
+                           float* p, float* sx, float* sy, float* sz, cudaStream_t s);
+
+}  // namespace ertm

@@ -1,0 +1,17 @@
+// Instantiation of the step kernels for stencil half-width R=4 (8th order).
+#include "step_kernels.cuh"
+
+namespace ertm {
+
+cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s)
+{
+    return launch_stress_t<4>(g, a, cpml, psplit, s);
+}
+
+cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
+                               cudaStream_t s)
+{
+    return launch_velocity_t<4>(g, a, cpml, epi, record, s);
+}
+
+}  // namespace ertm

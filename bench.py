@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Throughput of the elastic RTM hot path on B200.
+
+One step = one RTM shot of the 3D workload: the source pass (src_steps = 2*nt/3 time
+steps with excitation capture) and the receiver pass (nt time steps with data
+injection and excitation-amplitude PP/PS/TP imaging), through the C ABI.
+
+Workload (seeded synthetic, no dataset): 400 x 400 x 300 interior at 10 m with a
+40-cell C-PML (480 x 480 x 380 = 87.55 M cells), 8th-order staggered grid, dt 0.8 ms,
+nt 4000, 10 Hz Ricker at the surface centre, 200 x 200 receivers every 20 m.
+
+Metric: Gcell-updates/s = cells x (src_steps + nt) / step time.  `value` has the
+observed data and the images in HBM; `e2e` passes pinned host buffers through the
+same API call (H2D of the data, D2H of the three images inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun each rank migrates its own shot (shots shard with no exchange);
+the per-shot images are stacked with one NCCL reduce per step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import datetime
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = "2d_and_3d_elastic_reverse_time_migration_b200"
+sys.path.insert(0, REPO)
+
+METRIC = "Gcell-updates/s (3D elastic RTM shot: source + receiver pass)"
+UNIT = "Gcell/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="small grid (debugging only)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--kernel-steps", type=int, default=60)
+    return ap.parse_args()
+
+
+def workload(small: bool):
+    synth = importlib.import_module(PKG + ".synthetic")
+    if small:
+        return synth.layered_3d(n_interior=(60, 80, 80), pml=20, nt=400, smooth_sigma=4.0)
+    return synth.layered_3d()
+
+
+def _shot(ertm, wl, synth, rank):
+    sx, sy, sz = wl.src
+    if rank:  # other ranks migrate other shots: shift the source laterally
+        nz, ny, nx = wl.shape
+        sx = wl.pml + (sx - wl.pml + 37 * rank) % (nx - 2 * wl.pml)
+        sy = wl.pml + (sy - wl.pml + 53 * rank) % (ny - 2 * wl.pml)
+    w = synth.ricker(wl.freq, wl.dt_ms / 1000.0)
+    return ertm.Shot(sx, sy, sz, wavelet=w, **wl.rec)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", uuid, f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 7]
+        os.unlink(self.f.name)
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+class CpuOracle:
+    """FP32 OpenMP oracle (a port of the reference's update loops, same scheme) holding
+    the full-grid state; `run(n)` times n source-pass steps with excitation capture."""
+
+    def __init__(self, wl):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as orc
+        self.orc, self.L = orc, orc.lib(32)
+        nz, ny, nx = wl.shape
+        self.cells = nx * ny * nz
+        self.g = orc.make_grid(nx, ny, nz, wl.dx, wl.dy, wl.dz, wl.dt_ms, R=4, boundary=orc.CPML,
+                               pml=(wl.pml,) * 6, pml_vmax=float(wl.svp.max()))
+        self.st = self.L.orc_state_create(C.byref(self.g), orc._fp(wl.svp), orc._fp(wl.svs),
+                                          orc._fp(wl.srho))
+        if not self.st:
+            raise RuntimeError("oracle state allocation failed")
+        self.shot = orc.make_shot(*wl.src, orc.ricker(wl.freq, wl.dt_ms / 1000.0))
+        self.ex = orc.ExcitationArrays(wl.shape)
+        self.es = self.ex.struct()
+        self.it = 0
+        self.run(1)  # first touch of every page, untimed by callers
+
+    @property
+    def threads(self):
+        return self.L.orc_threads()
+
+    def run(self, n: int) -> float:
+        t0 = time.perf_counter()
+        for _ in range(n):
+            self.L.orc_state_step(self.st, C.byref(self.shot), self.orc.SOURCE, self.it, 1 << 30,
+                                  None, C.byref(self.es), None, None, None)
+            self.it += 1
+        return time.perf_counter() - t0
+
+    def rate_for(self, seconds: float):
+        n, el = 0, 0.0
+        while el < seconds or n < 2:
+            el += self.run(1)
+            n += 1
+        return self.cells * n / el / 1e9, n
+
+    def close(self):
+        if self.st:
+            self.L.orc_state_destroy(self.st)
+            self.st = None
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    synth = importlib.import_module(PKG + ".synthetic")
+    wl = (synth.layered_3d(n_interior=(60, 80, 80), pml=20, nt=400, smooth_sigma=0)
+          if args.small else synth.layered_3d(smooth_sigma=0))
+    cpu = CpuOracle(wl)
+    per_step = 2
+    for _ in range(args.warmup):
+        cpu.run(per_step)
+    el = sum(cpu.run(per_step) for _ in range(args.steps))
+    v = cpu.cells * per_step * args.steps / el / 1e9
+    nz, ny, nx = wl.shape
+    sample = (f"{per_step} source-pass time steps (with excitation capture) of the full "
+              f"{nx}x{ny}x{nz} grid per step; FP32 OpenMP port of the update loops")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(el / args.steps * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered model with an ellipsoid)",
+        "config": {"workload": wl.name, "cells": cpu.cells, "order": 8, "boundary": "cpml40"},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cpu.threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+    cpu.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=dev)
+
+    ertm = importlib.import_module(PKG)
+    synth = importlib.import_module(PKG + ".synthetic")
+    wl = workload(args.small)
+    nz, ny, nx = wl.shape
+    cells = nx * ny * nz
+    cfg = ertm.Config(nx=nx, ny=ny, nz=nz, dx=wl.dx, dy=wl.dy, dz=wl.dz, dt_ms=wl.dt_ms,
+                      nt=wl.nt, order=8, boundary=ertm.BOUNDARY_CPML, pml=(wl.pml,) * 6,
+                      device=local)
+    src_steps = 2 * wl.nt // 3
+    updates = cells * (src_steps + wl.nt)
+    ctx = ertm.Context(cfg)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_model(ertm.TRUE_MODEL, wl.vp, wl.vs, wl.rho)
+    ctx.set_model(ertm.MIGRATION_MODEL, wl.svp, wl.svs, wl.srho)
+    shot = _shot(ertm, wl, synth, rank)
+
+    # observed data: modelling in the true model (setup, untimed), kept in HBM
+    data = torch.zeros((3, wl.nt, shot.nrec), dtype=torch.float32, device=dev)
+    ctx.forward_together_using_real_model(shot, out=data)
+    imgs = [torch.zeros(wl.shape, dtype=torch.float32, device=dev) for _ in range(3)]
+
+    def step():
+        ctx.rtm_shot(shot, data, *imgs)
+        if world > 1:
+            for t in imgs:
+                dist.reduce(t, dst=0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    clocks = ClockSampler(uuid)
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    launches = ctx.kernel_launches - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * updates / (ms_step / 1e3) / 1e9
+
+    # end to end: pinned host data in, pinned host images out, through the same call
+    data_h = torch.empty(data.shape, dtype=torch.float32, pin_memory=True)
+    data_h.copy_(data)
+    imgs_h = [torch.empty(wl.shape, dtype=torch.float32, pin_memory=True) for _ in range(3)]
+    torch.cuda.synchronize(dev)
+    ctx.rtm_shot(shot, data_h, *imgs_h)   # warm the host path
+    barrier()
+    e0.record(stream)
+    ctx.rtm_shot(shot, data_h, *imgs_h)
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    t = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = world * updates / (float(t.item()) / 1e3) / 1e9
+    h2d = data.numel() * 4
+    d2h = 3 * cells * 4
+
+    # per-kernel device time (CUDA events around each launch, source-pass kernels)
+    ks = args.kernel_steps
+    ms_stress, ms_vel = ctx.time_kernels(shot, ks)
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    # algorithmic bytes per cell of each source-pass kernel (FP32):
+    #   stress:   read v(3) sigma(6) tp(1) M, mu(2); write sigma(6) tp(1)          = 76 B
+    #   velocity: read sigma(6) tp(1) v(3) vP(3) b(1) |e|^2(1); write v(3) vP(3) = 84 B
+    bytes_k = {"stress": 76 * cells, "velocity": 84 * cells}
+    t_k = {"stress": ms_stress / ks, "velocity": ms_vel / ks}
+    dom = max(t_k, key=t_k.get)
+    achieved = bytes_k[dom] / (t_k[dom] / 1e3) / 1e9
+    step_ms = (ms_stress + ms_vel) / ks
+    step_gbs = (bytes_k["stress"] + bytes_k["velocity"]) / (step_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            co = CpuOracle(wl)
+            rate, n = co.rate_for(args.cpu_seconds)
+            cpu = {"value": round(rate, 4), "unit": UNIT, "cores": co.threads, "kind": "port",
+                   "sample": f"{n} source-pass time steps of the full {nx}x{ny}x{nz} grid, "
+                             f"FP32 OpenMP oracle (same scheme), after one untimed step"}
+            co.close()
+        except Exception as e:  # a missing oracle build must not hide the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered model with an ellipsoid; observed data modelled "
+                    "in the true model)",
+            "config": {"workload": wl.name, "cells": cells, "nt": wl.nt, "src_steps": src_steps,
+                       "order": 8, "boundary": "cpml40", "dt_ms": wl.dt_ms,
+                       "receivers": shot.nrec, "parallelism": f"shots x{world}",
+                       "l2": "inputs larger than L2 (13 wavefields + model, ~8 GB)"},
+            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": f"k_{dom} (source pass)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_source": peak_src,
+                         "bytes_per_cell": bytes_k[dom] // cells,
+                         "kernel_ms": {k: round(v, 4) for k, v in t_k.items()},
+                         "step_gbs": round(step_gbs, 1), "step_frac": round(step_gbs / peak, 4)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

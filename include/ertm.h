@@ -1,0 +1,181 @@
+/*
+ * ertm.h — C ABI of the B200 elastic reverse-time-migration library (libertm.so).
+ *
+ * Drop-in for the reference's per-shot "forward/backward together" calls
+ * (3D_elastic_RTM/3D_forward_or_back_together.cu):
+ *
+ *   reference                                         this library
+ *   forward_together_using_real_model(GPUdevice*)     ertm_forward_together_using_real_model
+ *       (:9-155, observed-data modelling)
+ *   forward_together_using_smoothed_model(GPUdevice*) ertm_forward_together_using_smoothed_model
+ *       (:161-290, source pass + excitation capture)
+ *   backward_together_using_smoothed_model(GPUdevice*) ertm_backward_together_using_smoothed_model
+ *       (:296-453, receiver pass + excitation-amplitude imaging)
+ *
+ * The reference functions read ~60 globals (3D_elastic_RTM/3D_elastic_modeling_parameter:1-141)
+ * and a GPUdevice struct (3D_elastic_modeling_typedef_struct:1-55); here they
+ * are an `ertm_config` (grid, time step, stencil, boundary), an `ertm_shot`
+ * (source and receiver geometry) and an opaque context that owns every device
+ * buffer.  Errors abort the process in the reference (checkCudaErrors); here
+ * every call returns an int status (0 = OK, negative = ERTM_E*) and
+ * ertm_last_error() returns the message.  No exception crosses this boundary.
+ *
+ * Conventions
+ *  - Arrays are float32, x fastest: cell (i,j,k) at k*ny*nx + j*nx + i
+ *    (the reference's 3D device layout, 3D_zzzzz:21).  ny == 1 is a 2D x–z grid.
+ *  - The grid includes the absorbing layers (the reference's nnx/nny/nnz).
+ *  - dt is in milliseconds (reference parameter `dt`, dt_real = dt/1000,
+ *    2D_elastic_RTM/viscoelastic_equation.cu:66).
+ *  - Pointer arguments may be host (pageable or pinned) or device memory of the
+ *    context's GPU; the library detects which.
+ *  - Calls are ordered on the context's stream and return when their results
+ *    are complete.  One context per host thread; a context is not re-entrant.
+ *  - Traces are [3][nt][nrec] (vx, vy, vz; vy is zero in 2D), receiver r =
+ *    iry*nrx + irx.
+ */
+#ifndef ERTM_H
+#define ERTM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ERTM_ABI_VERSION 1
+
+/* status codes */
+#define ERTM_OK        0
+#define ERTM_EINVAL   -1   /* bad argument or size */
+#define ERTM_ENOMEM   -2   /* device or host allocation failed */
+#define ERTM_ECUDA    -3   /* CUDA runtime error */
+#define ERTM_ESTATE   -4   /* call out of order (e.g. receiver pass before source pass) */
+#define ERTM_ENOTSUP  -5   /* configuration not supported by this build */
+#define ERTM_EDEVICE  -6   /* a device-side check failed (bounded wait expired, bad index) */
+
+/* absorbing boundary kinds */
+#define ERTM_BOUNDARY_CPML          0  /* convolutional PML (north-star default) */
+#define ERTM_BOUNDARY_SPONGE_COS    1  /* reference 3D damping, 3D_zzzzz:261-369 */
+#define ERTM_BOUNDARY_SPONGE_CUBIC  2  /* reference 2D damping, zzzzz:238-325 */
+
+/* difference coefficient sets */
+#define ERTM_COEF_TAYLOR        0  /* Taylor coefficients of order 2R */
+#define ERTM_COEF_REFERENCE12   1  /* reference optimised 12th order, zzzzz:202-210 (R=6) */
+#define ERTM_COEF_USER          2  /* ertm_config.coef[1..R] */
+
+/* receiver injection mode of the receiver pass (reference add_receiver_bool) */
+#define ERTM_INJECT_ADD      1
+#define ERTM_INJECT_REPLACE  2
+
+/* wavefield ids for ertm_get_wavefield */
+enum {
+    ERTM_F_VX = 0, ERTM_F_VY, ERTM_F_VZ, ERTM_F_TXX, ERTM_F_TYY, ERTM_F_TZZ,
+    ERTM_F_TXY, ERTM_F_TXZ, ERTM_F_TYZ, ERTM_F_TP, ERTM_F_VXP, ERTM_F_VYP, ERTM_F_VZP,
+    ERTM_NFIELDS
+};
+
+typedef struct ertm_ctx ertm_ctx;
+
+typedef struct {
+    int   nx, ny, nz;        /* grid incl. absorbing layers; ny == 1 -> 2D */
+    float dx, dy, dz;        /* metres */
+    float dt_ms;             /* time step, milliseconds */
+    int   nt;                /* samples of a full record (reference `lt`) */
+    int   src_steps;         /* steps of the source pass; 0 -> 2*nt/3 as the reference (:173) */
+    int   order;             /* 8 (R=4) or 12 (R=6) */
+    int   coef_kind;         /* ERTM_COEF_* */
+    float coef[8];           /* used when coef_kind == ERTM_COEF_USER */
+    int   boundary;          /* ERTM_BOUNDARY_* */
+    int   pml[6];            /* absorbing widths x0,x1,y0,y1,z0,z1 in cells */
+    float pml_r;             /* CPML reflection coefficient (default 1e-3 when 0) */
+    float pml_f0;            /* CPML alpha frequency in Hz (default 10 when 0) */
+    float pml_vmax;          /* CPML velocity; 0 -> max Vp of the model */
+    float sponge_coef;       /* reference coe_attenuation (sponge kinds) */
+    int   device;            /* CUDA device ordinal */
+    int   reserved[7];       /* must be zero */
+} ertm_config;
+
+typedef struct {
+    int sx, sy, sz;          /* explosive source cell (reference sx_real, sy_real, sz_real) */
+    int nw;                  /* wavelet samples (reference wavelet_length) */
+    const float *wavelet;    /* host or device, nw values */
+    int rx0, nrx, drx;       /* receiver grid along x (receiver_start_x/num_x/interval_x) */
+    int ry0, nry, dry;       /* along y; nry = 1 in 2D */
+    int rz;                  /* receiver depth index (receiver_start_z) */
+    int inject_mode;         /* ERTM_INJECT_*, receiver pass; 0 -> ADD */
+} ertm_shot;
+
+/* ---- lifecycle --------------------------------------------------------- */
+
+/* Replaces allocate_typedef_struct (3D_elastic_modeling_typedef_struct:57-210).
+ * Validates the config, selects the device, allocates every device buffer. */
+int ertm_create(const ertm_config *cfg, ertm_ctx **out);
+int ertm_destroy(ertm_ctx *ctx);
+/* Message of the last failing call on this context (or of a failed create
+ * when ctx is NULL, thread-local). Always NUL-terminates. */
+int ertm_last_error(const ertm_ctx *ctx, char *buf, size_t len);
+/* Use the caller's cudaStream_t (NULL restores the context's own stream). */
+int ertm_set_stream(ertm_ctx *ctx, void *cuda_stream);
+int ertm_abi_version(void);
+
+/* Load a model: which = 0 true model (velocity/velocity1/density),
+ * which = 1 migration model (s_velocity/s_velocity1/s_density).
+ * vp, vs, rho: nz*ny*nx floats (host or device), copied. */
+int ertm_set_model(ertm_ctx *ctx, int which, const float *vp, const float *vs, const float *rho);
+
+/* ---- the reference's three per-shot calls ------------------------------ */
+
+/* Observed-data modelling in the true model for cfg.nt steps
+ * (3D_forward_or_back_together.cu:9-155).  data_out: [3][nt][nrec]. */
+int ertm_forward_together_using_real_model(ertm_ctx *ctx, const ertm_shot *shot, float *data_out);
+
+/* Source pass in the migration model for src_steps steps with excitation
+ * amplitude/time capture of the P velocity (:161-290).  The excitation state
+ * stays in the context for the receiver pass. */
+int ertm_forward_together_using_smoothed_model(ertm_ctx *ctx, const ertm_shot *shot);
+
+/* Receiver pass it = nt-1 .. 0 injecting data_in [3][nt][nrec] and applying
+ * the vector excitation-amplitude imaging condition (:296-453):
+ *   PP = (e_P . r_P)/|e_P|^2,  PS = (e_P . r_S)/|e_P|^2,  TP = r_tp / e_tp
+ * at it == excitation time.  Images are nz*ny*nx (full grid); any may be NULL. */
+int ertm_backward_together_using_smoothed_model(ertm_ctx *ctx, const ertm_shot *shot,
+                                                const float *data_in, float *img_pp,
+                                                float *img_ps, float *img_tp);
+
+/* Source pass then receiver pass: one RTM shot. */
+int ertm_rtm_shot(ertm_ctx *ctx, const ertm_shot *shot, const float *data_in,
+                  float *img_pp, float *img_ps, float *img_tp);
+
+/* ---- inspection (the reference's output_3d_wavefiled_* / EA outputs,
+ *      3D_output_file.cu:2-250) ------------------------------------------ */
+
+/* Current wavefield `field` (ERTM_F_*) into out (nz*ny*nx). */
+int ertm_get_wavefield(ertm_ctx *ctx, int field, float *out);
+/* Excitation state of the last source pass (any pointer may be NULL):
+ * amplitude |v_P|, time index, v_P vector and P stress at that time. */
+int ertm_get_excitation(ertm_ctx *ctx, float *amp, int32_t *time, float *evx, float *evy,
+                        float *evz, float *etp);
+
+/* Divergence/curl P/S decomposition of the current velocity field
+ * (decom_new, 2D_elastic_RTM/elastic_2D_kernel_2.cu:671-791; 3D extension):
+ * p = vp * div v; 2D: sy = vs*(dvx/dz - dvz/dx); 3D: sx, sy, sz the curl
+ * components.  Uses the model `which`.  sx, sz ignored in 2D. */
+int ertm_divcurl(ertm_ctx *ctx, int which, float *p, float *sx, float *sy, float *sz);
+
+/* Run `nsteps` plain propagation steps of the modelling pass from a zero
+ * state in model `which` (0/1) without recording: for wavefield checks. */
+int ertm_propagate(ertm_ctx *ctx, int which, const ertm_shot *shot, int nsteps);
+
+/* Device time of each step kernel over `nsteps` propagation steps of the
+ * source pass, measured with CUDA events on the context stream:
+ * ms[0] stress kernel, ms[1] velocity kernel (totals over nsteps). */
+int ertm_time_kernels(ertm_ctx *ctx, const ertm_shot *shot, int nsteps, float *ms);
+
+/* Number of kernels this context has launched (for launch accounting). */
+int64_t ertm_kernel_launches(const ertm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ERTM_H */

@@ -1,0 +1,118 @@
+/*
+ * CPU oracle for the elastic RTM hot path — TEST INFRASTRUCTURE ONLY.
+ *
+ * This is a plain-loop restatement of the reference's staggered-grid
+ * velocity–stress propagation, P/S split, excitation-amplitude capture and
+ * excitation-amplitude imaging.  It exists to check the CUDA library and to
+ * time a CPU baseline; nothing in the product links or calls it.
+ *
+ * Built twice from the same source (oracle/Makefile):
+ *   liboracle64.so   REAL = double  (the parity oracle)
+ *   liboracle32.so   REAL = float   (the OpenMP CPU baseline)
+ * Every entry point below takes and returns float arrays; REAL is internal.
+ *
+ * Parity pinning: the helper functions (Ricker, difference coefficients,
+ * sponge profiles) and the 2D kernels that survive in the reference are
+ * checked against outputs of the reference's own code (tests/golden); the 3D
+ * assembly has no reference implementation (its kernels are absent from the
+ * reference tree), so the 3D oracle extends the 2D forms and is pinned only
+ * through those pieces.
+ *
+ * Grid convention (shared with the CUDA library, x fastest):
+ *   cell (i,j,k) -> k*ny*nx + j*nx + i,  ny == 1 means a 2D x–z grid.
+ *   txx,tyy,tzz,tp at (i, j, k)
+ *   vx at (i-1/2, j, k), vy at (i, j-1/2, k), vz at (i, j, k+1/2)
+ *   txy at (i-1/2, j-1/2, k), txz at (i-1/2, j, k+1/2), tyz at (i, j-1/2, k+1/2)
+ * which extends the 2D staggering of
+ *   2D_elastic_RTM/viscoelastic_equation.cu:137-149 (stress, D+x vx, D-z vz)
+ *   2D_elastic_RTM/viscoelastic_equation.cu:164-176 (shear, D-x vz, D+z vx)
+ *   2D_elastic_RTM/viscoelastic_equation.cu:1827-1973 (vx: D-x txx, D-z txz)
+ *   2D_elastic_RTM/viscoelastic_equation.cu:1976-2122 (vz: D+x txz, D+z tzz)
+ * Fields outside [0,n) are zero (the reference pads every array by `radius`).
+ */
+#ifndef ERTM_ORACLE_H
+#define ERTM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_BOUNDARY_CPML = 0, ORC_BOUNDARY_SPONGE_COS = 1, ORC_BOUNDARY_SPONGE_CUBIC = 2 };
+enum { ORC_MODE_MODEL = 0, ORC_MODE_SOURCE = 1, ORC_MODE_RECEIVER = 2 };
+
+typedef struct {
+    int nx, ny, nz;          /* grid including absorbing layers; ny == 1 -> 2D */
+    double dx, dy, dz;       /* metres */
+    double dt_ms;            /* milliseconds, as the reference's `dt` */
+    int R;                   /* stencil half-width: 4 (8th order) or 6 (12th order) */
+    double coef[8];          /* coef[1..R] */
+    int boundary;            /* ORC_BOUNDARY_* */
+    int pml[6];              /* absorbing widths x0,x1,y0,y1,z0,z1 (cells) */
+    double pml_r;            /* CPML target reflection coefficient */
+    double pml_f0;           /* CPML alpha frequency (Hz) */
+    double pml_vmax;         /* CPML reference velocity (m/s) */
+    double sponge_coef;      /* reference `coe_attenuation` */
+} orc_grid;
+
+typedef struct {
+    int sx, sy, sz;          /* explosive source cell */
+    int nw;                  /* wavelet samples */
+    const float *wavelet;    /* one sample per step */
+    int rx0, nrx, drx;       /* receiver grid along x */
+    int ry0, nry, dry;       /* receiver grid along y (nry = 1 in 2D) */
+    int rz;                  /* receiver depth index */
+    int inject_mode;         /* 1 add (default), 2 replace */
+} orc_shot;
+
+/* Excitation state written by the source pass, read by the receiver pass.
+ * All arrays nz*ny*nx. `amp2` is |v_P|^2 at the excitation time; `second2`
+ * is the largest |v_P|^2 seen at any other step (used only to detect ties). */
+typedef struct {
+    float *amp2, *second2;
+    int   *time;
+    float *evx, *evy, *evz, *etp;
+} orc_excitation;
+
+/* ---- model-independent helpers --------------------------------------- */
+int  orc_ricker(double freq_hz, double dt_s, float *out, int maxn);
+void orc_coef_taylor(int R, double *coef);
+void orc_coef_reference12(double *coef);
+void orc_sponge_profile(int kind, int n, int w0, int w1, double coe, double *out);
+void orc_cpml_profile(int n, int w0, int w1, double h, double dt_s, double vmax,
+                      double rc, double f0, int stagger, double *a, double *b);
+
+/* ---- propagation passes ---------------------------------------------- */
+/* Runs `nsteps` time steps of one pass in the model (vp, vs, rho).
+ *  MODEL:    records vx,vy,vz at the receivers into data[3][nsteps][nrec]
+ *            (it = 0 .. nsteps-1), source injected.
+ *  SOURCE:   source injected; P/S split on; excitation capture into `ex`.
+ *  RECEIVER: it = nsteps-1 .. 0; data[3][nsteps][nrec] injected; P/S split on;
+ *            imaging into img_pp, img_ps, img_tp (nz*ny*nx, zeroed here).
+ * If `final_fields` is non-NULL it receives 13 arrays of nz*ny*nx in the order
+ *  vx vy vz txx tyy tzz txy txz tyz tp vxp vyp vzp  (state after the pass).
+ * Returns 0 on success, negative on bad arguments / allocation failure. */
+int orc_run_pass(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                 const orc_shot *s, int mode, int nsteps, float *data,
+                 orc_excitation *ex, float *img_pp, float *img_ps, float *img_tp,
+                 float *final_fields);
+
+/* Divergence / curl P/S decomposition of a velocity field (restates
+ * 2D_elastic_RTM/elastic_2D_kernel_2.cu:671-791 decom_new, extended to 3D):
+ *   P = vp * div v  at (i,j,k)
+ *   2D: S = vs * (d vx/dz - d vz/dx) at the txz point
+ *   3D: Sx = vs*(d vz/dy - d vy/dz) at tyz, Sy = vs*(d vx/dz - d vz/dx) at txz,
+ *       Sz = vs*(d vy/dx - d vx/dy) at txy.
+ * In 2D only p and sy are written. */
+int orc_divcurl(const orc_grid *g, const float *vp, const float *vs,
+                const float *vx, const float *vy, const float *vz,
+                float *p, float *sx, float *sy, float *sz);
+
+/* Threads used by the OpenMP loops (1 if built without OpenMP). */
+int orc_threads(void);
+/* sizeof(REAL) of this build. */
+int orc_real_size(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,216 @@
+"""ctypes front end of the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+Loaded only by tests/, the smoke check and bench.py's CPU-baseline leg, as
+the checker.  The product library never imports this module.
+
+`Grid` and `Shot` mirror ``orc_grid`` / ``orc_shot`` in ertm_oracle.h.  All
+arrays are float32 numpy arrays in x-fastest order, shape (nz, ny, nx).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(_HERE, "build")
+
+MODEL, SOURCE, RECEIVER = 0, 1, 2
+CPML, SPONGE_COS, SPONGE_CUBIC = 0, 1, 2
+FIELD_NAMES = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz",
+               "tp", "vxp", "vyp", "vzp")
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("dt_ms", C.c_double), ("R", C.c_int), ("coef", C.c_double * 8),
+                ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_double),
+                ("pml_f0", C.c_double), ("pml_vmax", C.c_double),
+                ("sponge_coef", C.c_double)]
+
+
+class Shot(C.Structure):
+    _fields_ = [("sx", C.c_int), ("sy", C.c_int), ("sz", C.c_int), ("nw", C.c_int),
+                ("wavelet", C.POINTER(C.c_float)),
+                ("rx0", C.c_int), ("nrx", C.c_int), ("drx", C.c_int),
+                ("ry0", C.c_int), ("nry", C.c_int), ("dry", C.c_int),
+                ("rz", C.c_int), ("inject_mode", C.c_int)]
+
+
+class Excitation(C.Structure):
+    _fields_ = [("amp2", C.POINTER(C.c_float)), ("second2", C.POINTER(C.c_float)),
+                ("time", C.POINTER(C.c_int)), ("evx", C.POINTER(C.c_float)),
+                ("evy", C.POINTER(C.c_float)), ("evz", C.POINTER(C.c_float)),
+                ("etp", C.POINTER(C.c_float))]
+
+
+_libs: dict[int, C.CDLL] = {}
+
+
+def build() -> None:
+    """Compile both oracle builds with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib(bits: int = 64) -> C.CDLL:
+    if bits not in _libs:
+        path = os.path.join(_BUILD, f"liboracle{bits}.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        P = C.POINTER
+        f = P(C.c_float)
+        L.orc_ricker.argtypes = [C.c_double, C.c_double, f, C.c_int]
+        L.orc_ricker.restype = C.c_int
+        L.orc_coef_taylor.argtypes = [C.c_int, P(C.c_double)]
+        L.orc_coef_reference12.argtypes = [P(C.c_double)]
+        L.orc_sponge_profile.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                         P(C.c_double)]
+        L.orc_cpml_profile.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_int,
+                                       P(C.c_double), P(C.c_double)]
+        L.orc_run_pass.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, C.c_int, f,
+                                   P(Excitation), f, f, f, f]
+        L.orc_run_pass.restype = C.c_int
+        L.orc_divcurl.argtypes = [P(Grid), f, f, f, f, f, f, f, f, f]
+        L.orc_divcurl.restype = C.c_int
+        L.orc_state_create.argtypes = [P(Grid), f, f, f]
+        L.orc_state_create.restype = C.c_void_p
+        L.orc_state_step.argtypes = [C.c_void_p, P(Shot), C.c_int, C.c_int, C.c_int, f,
+                                     P(Excitation), f, f, f]
+        L.orc_state_destroy.argtypes = [C.c_void_p]
+        L.orc_threads.restype = C.c_int
+        L.orc_real_size.restype = C.c_int
+        _libs[bits] = L
+    return _libs[bits]
+
+
+def _fp(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def ricker(freq_hz: float, dt_s: float, bits: int = 64) -> np.ndarray:
+    L = lib(bits)
+    n = L.orc_ricker(freq_hz, dt_s, None, 0)
+    out = np.zeros(n, np.float32)
+    L.orc_ricker(freq_hz, dt_s, _fp(out), n)
+    return out
+
+
+def coef_taylor(R: int) -> np.ndarray:
+    c = (C.c_double * 8)()
+    lib().orc_coef_taylor(R, c)
+    return np.array(c[:R + 1])
+
+
+def coef_reference12() -> np.ndarray:
+    c = (C.c_double * 8)()
+    lib().orc_coef_reference12(c)
+    return np.array(c[:7])
+
+
+def sponge_profile(kind: int, n: int, w0: int, w1: int, coe: float) -> np.ndarray:
+    out = (C.c_double * n)()
+    lib().orc_sponge_profile(kind, n, w0, w1, coe, out)
+    return np.array(out[:])
+
+
+def cpml_profile(n, w0, w1, h, dt_s, vmax, rc, f0, stagger):
+    a = (C.c_double * n)()
+    b = (C.c_double * n)()
+    lib().orc_cpml_profile(n, w0, w1, h, dt_s, vmax, rc, f0, stagger, a, b)
+    return np.array(a[:]), np.array(b[:])
+
+
+def make_grid(nx, ny, nz, dx, dy, dz, dt_ms, R=4, coef=None, boundary=CPML, pml=(0,) * 6,
+              pml_r=1e-3, pml_f0=10.0, pml_vmax=4000.0, sponge_coef=0.0) -> Grid:
+    g = Grid()
+    g.nx, g.ny, g.nz = nx, ny, nz
+    g.dx, g.dy, g.dz = dx, dy, dz
+    g.dt_ms = dt_ms
+    g.R = R
+    c = coef_taylor(R) if coef is None else np.asarray(coef, np.float64)
+    for i in range(8):
+        g.coef[i] = float(c[i]) if i < len(c) else 0.0
+    g.boundary = boundary
+    for i in range(6):
+        g.pml[i] = int(pml[i])
+    g.pml_r, g.pml_f0, g.pml_vmax, g.sponge_coef = pml_r, pml_f0, pml_vmax, sponge_coef
+    return g
+
+
+def make_shot(sx, sy, sz, wavelet, rx0=0, nrx=1, drx=1, ry0=0, nry=1, dry=1, rz=0,
+              inject_mode=1):
+    s = Shot()
+    s.sx, s.sy, s.sz = sx, sy, sz
+    w = np.ascontiguousarray(wavelet, np.float32)
+    s.nw = len(w)
+    s.wavelet = _fp(w)
+    s.rx0, s.nrx, s.drx, s.ry0, s.nry, s.dry, s.rz = rx0, nrx, drx, ry0, nry, dry, rz
+    s.inject_mode = inject_mode
+    s._keep = w  # keep the wavelet buffer alive
+    return s
+
+
+class ExcitationArrays:
+    def __init__(self, shape):
+        self.amp2 = np.zeros(shape, np.float32)
+        self.second2 = np.zeros(shape, np.float32)
+        self.time = np.zeros(shape, np.int32)
+        self.evx = np.zeros(shape, np.float32)
+        self.evy = np.zeros(shape, np.float32)
+        self.evz = np.zeros(shape, np.float32)
+        self.etp = np.zeros(shape, np.float32)
+
+    def struct(self) -> Excitation:
+        e = Excitation()
+        e.amp2, e.second2 = _fp(self.amp2), _fp(self.second2)
+        e.time = self.time.ctypes.data_as(C.POINTER(C.c_int))
+        e.evx, e.evy, e.evz, e.etp = _fp(self.evx), _fp(self.evy), _fp(self.evz), _fp(self.etp)
+        return e
+
+
+def run_pass(g: Grid, vp, vs, rho, shot: Shot, mode: int, nsteps: int, data=None,
+             ex: ExcitationArrays | None = None, want_fields=False, bits=64):
+    """Run one pass; returns dict with 'data', 'ex', 'pp', 'ps', 'tp', 'fields'."""
+    shape = (g.nz, g.ny, g.nx)
+    nrec = shot.nrx * shot.nry
+    out = {}
+    if mode == MODEL:
+        data = np.zeros((3, nsteps, nrec), np.float32)
+    if mode == SOURCE and ex is None:
+        ex = ExcitationArrays(shape)
+    pp = ps = tp = None
+    if mode == RECEIVER:
+        pp, ps, tp = (np.zeros(shape, np.float32) for _ in range(3))
+        data = np.ascontiguousarray(data, np.float32)
+    fields = np.zeros((13,) + shape, np.float32) if want_fields else None
+    exs = ex.struct() if ex is not None else None
+    rc = lib(bits).orc_run_pass(C.byref(g), _fp(vp), _fp(vs), _fp(rho), C.byref(shot), mode,
+                                nsteps, _fp(data) if data is not None else None,
+                                C.byref(exs) if exs is not None else None,
+                                _fp(pp), _fp(ps), _fp(tp), _fp(fields))
+    if rc != 0:
+        raise RuntimeError(f"orc_run_pass failed: {rc}")
+    out.update(data=data, ex=ex, pp=pp, ps=ps, tp=tp)
+    if want_fields:
+        out["fields"] = {n: fields[i] for i, n in enumerate(FIELD_NAMES)}
+    return out
+
+
+def divcurl(g: Grid, vp, vs, vx, vy, vz):
+    shape = (g.nz, g.ny, g.nx)
+    p, sx, sy, sz = (np.zeros(shape, np.float32) for _ in range(4))
+    two_d = g.ny == 1
+    rc = lib().orc_divcurl(C.byref(g), _fp(vp), _fp(vs), _fp(vx),
+                           None if two_d else _fp(vy), _fp(vz), _fp(p),
+                           None if two_d else _fp(sx), _fp(sy), None if two_d else _fp(sz))
+    if rc != 0:
+        raise RuntimeError(f"orc_divcurl failed: {rc}")
+    return p, sx, sy, sz

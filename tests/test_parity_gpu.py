@@ -1,0 +1,157 @@
+"""CUDA library against the CPU oracle through the C ABI (needs a B200).
+
+Tolerances (the CUDA path computes in FP32; the oracle in FP64 and FP32):
+  * wavefields / traces: relative L2 against the FP64 oracle within
+    max(1e-5, 3 x the FP32 oracle's own relative L2 against FP64) — the CUDA
+    path must be as accurate as a plain FP32 restatement of the same scheme;
+  * excitation time: bit-exact on every cell whose excitation is not tied
+    (runner-up |v_P|^2 more than TIE below the maximum, maximum above FLOOR x
+    the grid maximum);
+  * images: relative L2 <= 1e-4 over the cells whose excitation time agrees.
+"""
+import numpy as np
+import pytest
+
+from _cases import CASES, FREQ, DT_MS, geometry, model, oracle_grid, product_config, rel
+
+pytestmark = pytest.mark.gpu
+
+TIE = 2e-3
+FLOOR = 1e-6
+FIELDS3 = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")
+FIELDS2 = ("vx", "vz", "txx", "tzz", "txz")
+
+
+def _setup(ertm, orc, case, nt, src_steps=0, seed=7):
+    c = CASES[case]
+    vp, vs, rho = model(c["shape"], seed=seed)
+    g = oracle_grid(orc, case, vp)
+    src, rec = geometry(c["shape"], c["pml"])
+    w = orc.ricker(FREQ, DT_MS / 1000.0)
+    oshot = orc.make_shot(*src, w, **rec)
+    ctx = ertm.Context(product_config(ertm, case, nt, src_steps))
+    ctx.set_model(ertm.TRUE_MODEL, vp, vs, rho)
+    ctx.set_model(ertm.MIGRATION_MODEL, vp, vs, rho)
+    pshot = ertm.Shot(*src, wavelet=w, **rec)
+    return ctx, g, (vp, vs, rho), oshot, pshot
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_wavefields_after_steps(ertm, orc, case):
+    nsteps = 300
+    ctx, g, (vp, vs, rho), oshot, pshot = _setup(ertm, orc, case, nt=nsteps)
+    ref = orc.run_pass(g, vp, vs, rho, oshot, orc.MODEL, nsteps, want_fields=True, bits=64)["fields"]
+    r32 = orc.run_pass(g, vp, vs, rho, oshot, orc.MODEL, nsteps, want_fields=True, bits=32)["fields"]
+    ctx.propagate(ertm.TRUE_MODEL, pshot, nsteps)
+    names = FIELDS3 if CASES[case]["shape"][1] > 1 else FIELDS2
+    for name in names:
+        gpu = ctx.get_wavefield(name)
+        e_gpu, e_32 = rel(gpu, ref[name]), rel(r32[name], ref[name])
+        tol = max(1e-5, 3 * e_32)
+        assert e_gpu <= tol, f"{case} {name}: gpu {e_gpu:.2e} > tol {tol:.2e} (fp32 oracle {e_32:.2e})"
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_modelling_traces(ertm, orc, case):
+    nt = 240
+    ctx, g, (vp, vs, rho), oshot, pshot = _setup(ertm, orc, case, nt=nt)
+    ref = orc.run_pass(g, vp, vs, rho, oshot, orc.MODEL, nt, bits=64)["data"]
+    r32 = orc.run_pass(g, vp, vs, rho, oshot, orc.MODEL, nt, bits=32)["data"]
+    gpu = ctx.forward_together_using_real_model(pshot)
+    assert gpu.shape == ref.shape
+    comps = (0, 1, 2) if CASES[case]["shape"][1] > 1 else (0, 2)
+    for q in comps:
+        e_gpu, e_32 = rel(gpu[q], ref[q]), rel(r32[q], ref[q])
+        assert e_gpu <= max(1e-5, 3 * e_32), f"{case} comp {q}: {e_gpu:.2e} vs fp32 {e_32:.2e}"
+    if CASES[case]["shape"][1] == 1:
+        assert not gpu[1].any()
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_excitation_and_imaging(ertm, orc, case):
+    nt, nsrc = 240, 160
+    ctx, g, (vp, vs, rho), oshot, pshot = _setup(ertm, orc, case, nt=nt, src_steps=nsrc)
+    data = orc.run_pass(g, vp, vs, rho, oshot, orc.MODEL, nt, bits=64)["data"]
+    src = orc.run_pass(g, vp, vs, rho, oshot, orc.SOURCE, nsrc, bits=64)
+    ex = src["ex"]
+    ctx.forward_together_using_smoothed_model(pshot)
+    gx = ctx.get_excitation()
+    clear = (ex.amp2 - ex.second2 > TIE * ex.amp2) & (ex.amp2 > FLOOR * ex.amp2.max())
+    assert clear.mean() > 0.5, f"only {clear.mean():.2f} of the cells are tie-free"
+    mism = (gx["time"] != ex.time) & clear
+    assert not mism.any(), f"{case}: {int(mism.sum())} tie-free cells with a different excitation time"
+    amp_ref = np.sqrt(ex.amp2.astype(np.float64))
+    assert rel(gx["amp"][clear], amp_ref[clear]) < 1e-4
+    for k in ("evx", "evz"):
+        assert rel(gx[k][clear], getattr(ex, k)[clear]) < 1e-4, k
+
+    rec = orc.run_pass(g, vp, vs, rho, oshot, orc.RECEIVER, nt, data=data, ex=ex, bits=64)
+    pp, ps, tp = ctx.backward_together_using_smoothed_model(pshot, data)
+    for name, gpu, ref in (("pp", pp, rec["pp"]), ("ps", ps, rec["ps"]), ("tp", tp, rec["tp"])):
+        assert np.isfinite(gpu).all(), name
+        e = rel(gpu[clear], ref[clear])
+        assert e <= 1e-4, f"{case} image {name}: relative L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("case", ["3d_r4_cpml", "2d_r6_sponge"])
+def test_divcurl(ertm, orc, case):
+    nsteps = 150
+    ctx, g, (vp, vs, rho), oshot, pshot = _setup(ertm, orc, case, nt=nsteps)
+    ctx.propagate(ertm.TRUE_MODEL, pshot, nsteps)
+    v = {n: ctx.get_wavefield(n) for n in ("vx", "vy", "vz")}
+    ref = orc.divcurl(g, vp, vs, v["vx"], v["vy"], v["vz"])
+    gpu = ctx.divcurl(ertm.TRUE_MODEL)
+    idx = (0, 1, 2, 3) if CASES[case]["shape"][1] > 1 else (0, 2)
+    for q in idx:
+        assert rel(gpu[q], ref[q]) < 1e-5, q
+
+
+def test_wavefields_after_1000_steps(ertm, orc):
+    """Larger 3D grid so the wavefield is still inside after 1000 steps."""
+    shape, pml = (72, 76, 80), (10,) * 6
+    vp, vs, rho = model(shape, seed=11, vmin=1800.0, vmax=2400.0)
+    nz, ny, nx = shape
+    dt = 0.3
+    g = orc.make_grid(nx, ny, nz, 10.0, 10.0, 10.0, dt, R=4, boundary=0, pml=pml,
+                      pml_vmax=float(vp.max()))
+    w = orc.ricker(12.0, dt / 1000.0)
+    src = (nx // 2, ny // 2, nz // 2)
+    ref = orc.run_pass(g, vp, vs, rho, orc.make_shot(*src, w), orc.MODEL, 1000, want_fields=True,
+                       bits=64)["fields"]
+    r32 = orc.run_pass(g, vp, vs, rho, orc.make_shot(*src, w), orc.MODEL, 1000, want_fields=True,
+                       bits=32)["fields"]
+    ctx = ertm.Context(ertm.Config(nx=nx, ny=ny, nz=nz, dx=10, dy=10, dz=10, dt_ms=dt, nt=1000,
+                                   order=8, boundary=0, pml=pml))
+    ctx.set_model(ertm.TRUE_MODEL, vp, vs, rho)
+    ctx.propagate(ertm.TRUE_MODEL, ertm.Shot(*src, wavelet=w), 1000)
+    report = {}
+    for name in FIELDS3:
+        e_gpu, e_32 = rel(ctx.get_wavefield(name), ref[name]), rel(r32[name], ref[name])
+        report[name] = (e_gpu, e_32)
+        assert e_gpu <= max(1e-5, 3 * e_32), (name, e_gpu, e_32)
+    print("1000-step relative L2 (gpu, fp32 oracle):", report)
+
+
+def test_call_order_and_argument_errors(ertm, orc):
+    ctx, g, _, oshot, pshot = _setup(ertm, orc, "2d_r4_cpml", nt=20)
+    with pytest.raises(ertm.ErtmError) as ei:
+        ctx.backward_together_using_smoothed_model(pshot, np.zeros((3, 20, pshot.nrec), np.float32))
+    assert ei.value.code == -4
+    bad = ertm.Shot(10_000, 0, 5, wavelet=pshot.wavelet)
+    with pytest.raises(ertm.ErtmError) as ei:
+        ctx.forward_together_using_smoothed_model(bad)
+    assert ei.value.code == -1 and "outside" in str(ei.value)
+
+
+def test_device_pointers_match_host_pointers(ertm, orc):
+    import torch
+    ctx, g, (vp, vs, rho), oshot, pshot = _setup(ertm, orc, "3d_r4_cpml", nt=120, src_steps=80)
+    host = ctx.forward_together_using_real_model(pshot)
+    dev = torch.zeros((3, 120, pshot.nrec), dtype=torch.float32, device="cuda")
+    ctx.forward_together_using_real_model(pshot, out=dev)
+    assert np.array_equal(dev.cpu().numpy(), host)
+    pp_h, ps_h, tp_h = ctx.rtm_shot(pshot, host)
+    outs = [torch.zeros(CASES["3d_r4_cpml"]["shape"], device="cuda") for _ in range(3)]
+    ctx.rtm_shot(pshot, dev, *outs)
+    for a, b in zip(outs, (pp_h, ps_h, tp_h)):
+        assert np.array_equal(a.cpu().numpy(), b)
