@@ -60,20 +60,53 @@ __device__ __forceinline__ int receiver_index(const KArgs& a, int i, int j)
     return iy * a.nrx + ix;
 }
 
+// cp.async (sm_80+ async copy, global -> shared, 4 bytes): every input of
+// plane k+1 is requested while plane k is computed.
+__device__ __forceinline__ void cpa4(void* sdst, const void* gsrc)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared-memory stage of one z plane: NV halo tiles [SH][SW], NC per-cell
+// arrays [TYB][TX], NP C-PML memory variables [TYB][TX].  Two stages alternate.
+template <int R, bool Y, int NV, int NC, int NP>
+struct Stage {
+    static constexpr int TYB = Y ? TY3 : TY2;
+    static constexpr int SW = TX + 2 * R;
+    static constexpr int SH = Y ? TYB + 2 * R : TYB;
+    static constexpr int TILE = SH * SW;
+    static constexpr int CELL = TYB * TX;
+    static constexpr int FLOATS = NV * TILE + (NC + NP) * CELL;
+    static constexpr size_t BYTES = 2 * sizeof(float) * FLOATS;
+};
+
 // ---------------------------------------------------------------------------
 // Stress kernel
 // ---------------------------------------------------------------------------
 template <int R, bool Y, bool CPML, bool PS>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2))
+struct StressShape {
+    static constexpr int NV = Y ? 3 : 2;                          // vx, vz, (vy)
+    static constexpr int NSIG = Y ? 6 : 3;                        // txx tzz txz (tyy txy tyz)
+    static constexpr int NC = NSIG + (PS ? 1 : 0) + 2;            // + tp + M + MU
+    static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
+    using S = Stage<R, Y, NV, NC, NP>;
+};
+
+template <int R, bool Y, bool CPML, bool PS>
+__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), 1)
 k_stress(const KArgs a)
 {
-    constexpr int TYB = Y ? TY3 : TY2;
-    constexpr int SW = TX + 2 * R;
-    constexpr int SH = Y ? TYB + 2 * R : TYB;
+    using SS = StressShape<R, Y, CPML, PS>;
+    using S = typename SS::S;
+    constexpr int TYB = S::TYB, SW = S::SW, TILE = S::TILE, CELL = S::CELL;
+    constexpr int NV = SS::NV, NC = SS::NC, NSIG = SS::NSIG;
     constexpr int YO = Y ? R : 0;
-    __shared__ float s_vx[SH][SW];
-    __shared__ float s_vz[SH][SW];
-    __shared__ float s_vy[Y ? SH : 1][Y ? SW : 1];
+    // per-cell slots
+    constexpr int C_TP = NSIG, C_M = NSIG + (PS ? 1 : 0), C_MU = C_M + 1;
+    extern __shared__ __align__(16) float sm[];
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i = blockIdx.x * TX + tx;
@@ -85,153 +118,205 @@ k_stress(const KArgs a)
     const int it = __ldg(a.it_ptr);
     const bool src_here = (it < a.nw) && (i == a.ssx) && (j == a.ssy);
     const float wsrc = (it < a.nw) ? __ldg(a.wavelet + it) : 0.f;
+    const int r = ty + YO, s = tx + R, cell = ty * TX + tx;
 
-    const float* __restrict__ vx = a.f[F_VX];
-    const float* __restrict__ vy = a.f[F_VY];
-    const float* __restrict__ vz = a.f[F_VZ];
-    float* __restrict__ txx = a.f[F_TXX];
-    float* __restrict__ tyy = a.f[F_TYY];
-    float* __restrict__ tzz = a.f[F_TZZ];
-    float* __restrict__ txy = a.f[F_TXY];
-    float* __restrict__ txz = a.f[F_TXZ];
-    float* __restrict__ tyz = a.f[F_TYZ];
-    float* __restrict__ tp = a.f[F_TP];
+    const float* vsrc[3] = {a.f[F_VX], a.f[F_VZ], a.f[F_VY]};
+    float* sig[6] = {a.f[F_TXX], a.f[F_TZZ], a.f[F_TXZ], a.f[F_TYY], a.f[F_TXY], a.f[F_TYZ]};
+    float* tp = a.f[F_TP];
+    const long long cj = (long long)j * sy + i;       // column offset of (i, j)
+    const long long mj = (long long)j * a.msy + i;
 
-    long long c = (long long)k0 * sz + (long long)j * sy + i;
-    long long cm = (long long)k0 * a.msz + (long long)j * a.msy + i;
+    // C-PML: slab membership and profile coefficients of this column
+    const int WX = a.w[0] + a.w[1], WY = a.w[2] + a.w[3];
+    const bool inx = CPML && act && (i < a.w[0] || i >= a.nx - a.w[1]);
+    const bool iny = CPML && Y && act && (j < a.w[2] || j >= a.ny - a.w[3]);
+    const int slx = i < a.w[0] ? i : i - a.nx + WX;
+    const int sly = j < a.w[2] ? j : j - a.ny + WY;
+    float axf = 0.f, bxf = 1.f, axh = 0.f, bxh = 1.f, ayf = 0.f, byf = 1.f, ayh = 0.f, byh = 1.f;
+    if (inx) {
+        axf = __ldg(a.pa[0][0] + i); bxf = __ldg(a.pb[0][0] + i);
+        axh = __ldg(a.pa[0][1] + i); bxh = __ldg(a.pb[0][1] + i);
+    }
+    if (iny) {
+        ayf = __ldg(a.pa[1][0] + j); byf = __ldg(a.pb[1][0] + j);
+        ayh = __ldg(a.pa[1][1] + j); byh = __ldg(a.pb[1][1] + j);
+    }
+    // psi slots in the stage: x: EXX DXVZ (DXVY), y: EYY DYVX DYVZ, z: EZZ DZVX (DZVY)
+    constexpr int PX = 0, PY = Y ? 3 : 2, PZ = Y ? 6 : 2;
 
+    auto issue = [&](int p, int st, float cvx, float cvz, float cvy) {
+        float* T = sm + st * S::FLOATS;
+        float* Cc = T + NV * TILE;
+        float* Ps = Cc + NC * CELL;
+        const long long cp = (long long)p * sz + cj;
+        T[0 * TILE + r * SW + s] = cvx;
+        T[1 * TILE + r * SW + s] = cvz;
+        if (Y) T[2 * TILE + r * SW + s] = cvy;
+#pragma unroll
+        for (int f = 0; f < NV; f++) {
+            if (tx < R) {
+                cpa4(&T[f * TILE + r * SW + tx], vsrc[f] + cp - R);
+                cpa4(&T[f * TILE + r * SW + tx + TX + R], vsrc[f] + cp + TX);
+            }
+            if (Y && ty < R) {
+                cpa4(&T[f * TILE + ty * SW + s], vsrc[f] + cp - R * sy);
+                cpa4(&T[f * TILE + (ty + TYB + R) * SW + s], vsrc[f] + cp + TYB * sy);
+            }
+        }
+        if (act) {
+#pragma unroll
+            for (int q = 0; q < NSIG; q++) cpa4(&Cc[q * CELL + cell], sig[q] + cp);
+            if (PS) cpa4(&Cc[C_TP * CELL + cell], tp + cp);
+            const long long mp = (long long)p * a.msz + mj;
+            cpa4(&Cc[C_M * CELL + cell], a.M + mp);
+            cpa4(&Cc[C_MU * CELL + cell], a.MU + mp);
+            if (CPML) {
+                if (inx) {
+                    const long long x = ((long long)p * a.ny + j) * WX + slx;
+                    cpa4(&Ps[(PX + 0) * CELL + cell], a.psi[P_EXX] + x);
+                    cpa4(&Ps[(PX + 1) * CELL + cell], a.psi[P_DXVZ] + x);
+                    if (Y) cpa4(&Ps[(PX + 2) * CELL + cell], a.psi[P_DXVY] + x);
+                }
+                if (iny) {
+                    const long long y = ((long long)p * WY + sly) * a.nx + i;
+                    cpa4(&Ps[(PY + 0) * CELL + cell], a.psi[P_EYY] + y);
+                    cpa4(&Ps[(PY + 1) * CELL + cell], a.psi[P_DYVX] + y);
+                    cpa4(&Ps[(PY + 2) * CELL + cell], a.psi[P_DYVZ] + y);
+                }
+                if (p < a.w[4] || p >= a.nz - a.w[5]) {
+                    const int sl = p < a.w[4] ? p : p - a.nz + a.w[4] + a.w[5];
+                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    cpa4(&Ps[(PZ + 0) * CELL + cell], a.psi[P_EZZ] + z);
+                    cpa4(&Ps[(PZ + 1) * CELL + cell], a.psi[P_DZVX] + z);
+                    if (Y) cpa4(&Ps[(PZ + 2) * CELL + cell], a.psi[P_DZVY] + z);
+                }
+            }
+        }
+        cpa_commit();
+    };
+
+    // register queues of planes k-R .. k+R
     float qx[2 * R + 1], qy[2 * R + 1], qz[2 * R + 1];
 #pragma unroll
     for (int q = 0; q <= 2 * R; q++) {
-        long long cc = c + (long long)(q - R) * sz;
-        qx[q] = vx[cc];
-        qz[q] = vz[cc];
-        if (Y) qy[q] = vy[cc];
+        const long long cc = (long long)(k0 + q - R) * sz + cj;
+        qx[q] = vsrc[0][cc];
+        qz[q] = vsrc[1][cc];
+        if (Y) qy[q] = vsrc[2][cc];
     }
+    issue(k0, 0, qx[R], qz[R], Y ? qy[R] : 0.f);
+    cpa_wait_all();
+    __syncthreads();
 
-    const int r = ty + YO, s = tx + R;
     for (int k = k0; k < k1; ++k) {
-        // prefetch: queue fronts of the next plane, this plane's old stresses and model
+        const int st = (k - k0) & 1;
         const bool more = (k + 1 < k1);
-        float nx_ = 0.f, ny_ = 0.f, nz_ = 0.f;
+        float fx = 0.f, fy = 0.f, fz = 0.f;
         if (more) {
-            long long cn = c + (long long)(R + 1) * sz;
-            nx_ = vx[cn];
-            nz_ = vz[cn];
-            if (Y) ny_ = vy[cn];
+            const long long cn = (long long)(k + 1 + R) * sz + cj;
+            fx = vsrc[0][cn];
+            fz = vsrc[1][cn];
+            if (Y) fy = vsrc[2][cn];
+            issue(k + 1, st ^ 1, qx[R + 1], qz[R + 1], Y ? qy[R + 1] : 0.f);
         }
-        float oxx = 0.f, oyy = 0.f, ozz = 0.f, oxy = 0.f, oxz = 0.f, oyz = 0.f, otp = 0.f;
-        float M = 0.f, U = 0.f;
-        if (act) {
-            oxx = txx[c];
-            ozz = tzz[c];
-            oxz = txz[c];
-            if (Y) {
-                oyy = tyy[c];
-                oxy = txy[c];
-                oyz = tyz[c];
-            }
-            if (PS) otp = tp[c];
-            M = __ldg(a.M + cm);
-            U = __ldg(a.MU + cm);
-        }
-
-        // stage plane k
-        s_vx[r][s] = qx[R];
-        s_vz[r][s] = qz[R];
-        if (Y) s_vy[r][s] = qy[R];
-        if (tx < R) {
-            s_vx[r][tx] = vx[c - R];
-            s_vx[r][tx + TX + R] = vx[c + TX];
-            s_vz[r][tx] = vz[c - R];
-            s_vz[r][tx + TX + R] = vz[c + TX];
-            if (Y) {
-                s_vy[r][tx] = vy[c - R];
-                s_vy[r][tx + TX + R] = vy[c + TX];
-            }
-        }
-        if (Y && ty < R) {
-            s_vx[ty][s] = vx[c - R * sy];
-            s_vx[ty + TYB + R][s] = vx[c + TYB * sy];
-            s_vy[ty][s] = vy[c - R * sy];
-            s_vy[ty + TYB + R][s] = vy[c + TYB * sy];
-            s_vz[ty][s] = vz[c - R * sy];
-            s_vz[ty + TYB + R][s] = vz[c + TYB * sy];
-        }
-        __syncthreads();
+        const float* T = sm + st * S::FLOATS;
+        const float* Cc = T + NV * TILE;
+        const float* Ps = Cc + NC * CELL;
+        const float* Tx = T;
+        const float* Tz = T + TILE;
+        const float* Ty = T + 2 * TILE;
 
         float exx = 0.f, dxvz = 0.f, dxvy = 0.f, eyy = 0.f, dyvx = 0.f, dyvz = 0.f;
         float ezz = 0.f, dzvx = 0.f, dzvy = 0.f;
 #pragma unroll
         for (int n = 1; n <= R; n++) {
-            exx = fmaf(a.cx[n], s_vx[r][s + n] - s_vx[r][s - n + 1], exx);
-            dxvz = fmaf(a.cx[n], s_vz[r][s + n - 1] - s_vz[r][s - n], dxvz);
+            exx = fmaf(a.cx[n], Tx[r * SW + s + n] - Tx[r * SW + s - n + 1], exx);
+            dxvz = fmaf(a.cx[n], Tz[r * SW + s + n - 1] - Tz[r * SW + s - n], dxvz);
             ezz = fmaf(a.cz[n], qz[R + n - 1] - qz[R - n], ezz);
             dzvx = fmaf(a.cz[n], qx[R + n] - qx[R - n + 1], dzvx);
             if (Y) {
-                dxvy = fmaf(a.cx[n], s_vy[r][s + n - 1] - s_vy[r][s - n], dxvy);
-                eyy = fmaf(a.cy[n], s_vy[r + n][s] - s_vy[r - n + 1][s], eyy);
-                dyvx = fmaf(a.cy[n], s_vx[r + n - 1][s] - s_vx[r - n][s], dyvx);
-                dyvz = fmaf(a.cy[n], s_vz[r + n - 1][s] - s_vz[r - n][s], dyvz);
+                dxvy = fmaf(a.cx[n], Ty[r * SW + s + n - 1] - Ty[r * SW + s - n], dxvy);
+                eyy = fmaf(a.cy[n], Ty[(r + n) * SW + s] - Ty[(r - n + 1) * SW + s], eyy);
+                dyvx = fmaf(a.cy[n], Tx[(r + n - 1) * SW + s] - Tx[(r - n) * SW + s], dyvx);
+                dyvz = fmaf(a.cy[n], Tz[(r + n - 1) * SW + s] - Tz[(r - n) * SW + s], dyvz);
                 dzvy = fmaf(a.cz[n], qy[R + n] - qy[R - n + 1], dzvy);
             }
         }
 
         if (act) {
+            const long long c = (long long)k * sz + cj;
             if (CPML) {
-                const int w0 = a.w[0], w1 = a.w[1];
-                if (i < w0 || i >= a.nx - w1) {
-                    int sl = i < w0 ? i : i - a.nx + w0 + w1;
-                    long long p = ((long long)k * a.ny + j) * (w0 + w1) + sl;
-                    exx = cpml_upd(a.psi[P_EXX], p, __ldg(a.pa[0][0] + i), __ldg(a.pb[0][0] + i), exx);
-                    dxvz = cpml_upd(a.psi[P_DXVZ], p, __ldg(a.pa[0][1] + i), __ldg(a.pb[0][1] + i), dxvz);
-                    if (Y)
-                        dxvy = cpml_upd(a.psi[P_DXVY], p, __ldg(a.pa[0][1] + i), __ldg(a.pb[0][1] + i),
-                                        dxvy);
-                }
-                if (Y) {
-                    const int w2 = a.w[2], w3 = a.w[3];
-                    if (j < w2 || j >= a.ny - w3) {
-                        int sl = j < w2 ? j : j - a.ny + w2 + w3;
-                        long long p = ((long long)k * (w2 + w3) + sl) * a.nx + i;
-                        eyy = cpml_upd(a.psi[P_EYY], p, __ldg(a.pa[1][0] + j), __ldg(a.pb[1][0] + j), eyy);
-                        dyvx = cpml_upd(a.psi[P_DYVX], p, __ldg(a.pa[1][1] + j), __ldg(a.pb[1][1] + j),
-                                        dyvx);
-                        dyvz = cpml_upd(a.psi[P_DYVZ], p, __ldg(a.pa[1][1] + j), __ldg(a.pb[1][1] + j),
-                                        dyvz);
+                if (inx) {
+                    const long long x = ((long long)k * a.ny + j) * WX + slx;
+                    float p0 = fmaf(bxf, Ps[(PX + 0) * CELL + cell], axf * exx);
+                    float p1 = fmaf(bxh, Ps[(PX + 1) * CELL + cell], axh * dxvz);
+                    a.psi[P_EXX][x] = p0;
+                    a.psi[P_DXVZ][x] = p1;
+                    exx += p0;
+                    dxvz += p1;
+                    if (Y) {
+                        float p2 = fmaf(bxh, Ps[(PX + 2) * CELL + cell], axh * dxvy);
+                        a.psi[P_DXVY][x] = p2;
+                        dxvy += p2;
                     }
                 }
-                const int w4 = a.w[4], w5 = a.w[5];
-                if (k < w4 || k >= a.nz - w5) {
-                    int sl = k < w4 ? k : k - a.nz + w4 + w5;
-                    long long p = ((long long)sl * a.ny + j) * a.nx + i;
-                    ezz = cpml_upd(a.psi[P_EZZ], p, __ldg(a.pa[2][0] + k), __ldg(a.pb[2][0] + k), ezz);
-                    dzvx = cpml_upd(a.psi[P_DZVX], p, __ldg(a.pa[2][1] + k), __ldg(a.pb[2][1] + k), dzvx);
-                    if (Y)
-                        dzvy = cpml_upd(a.psi[P_DZVY], p, __ldg(a.pa[2][1] + k), __ldg(a.pb[2][1] + k),
-                                        dzvy);
+                if (iny) {
+                    const long long y = ((long long)k * WY + sly) * a.nx + i;
+                    float p0 = fmaf(byf, Ps[(PY + 0) * CELL + cell], ayf * eyy);
+                    float p1 = fmaf(byh, Ps[(PY + 1) * CELL + cell], ayh * dyvx);
+                    float p2 = fmaf(byh, Ps[(PY + 2) * CELL + cell], ayh * dyvz);
+                    a.psi[P_EYY][y] = p0;
+                    a.psi[P_DYVX][y] = p1;
+                    a.psi[P_DYVZ][y] = p2;
+                    eyy += p0;
+                    dyvx += p1;
+                    dyvz += p2;
+                }
+                if (k < a.w[4] || k >= a.nz - a.w[5]) {
+                    const int sl = k < a.w[4] ? k : k - a.nz + a.w[4] + a.w[5];
+                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    const float azf = __ldg(a.pa[2][0] + k), bzf = __ldg(a.pb[2][0] + k);
+                    const float azh = __ldg(a.pa[2][1] + k), bzh = __ldg(a.pb[2][1] + k);
+                    float p0 = fmaf(bzf, Ps[(PZ + 0) * CELL + cell], azf * ezz);
+                    float p1 = fmaf(bzh, Ps[(PZ + 1) * CELL + cell], azh * dzvx);
+                    a.psi[P_EZZ][z] = p0;
+                    a.psi[P_DZVX][z] = p1;
+                    ezz += p0;
+                    dzvx += p1;
+                    if (Y) {
+                        float p2 = fmaf(bzh, Ps[(PZ + 2) * CELL + cell], azh * dzvy);
+                        a.psi[P_DZVY][z] = p2;
+                        dzvy += p2;
+                    }
                 }
             }
             float g1, g2;
             damping<Y>(a, CPML, i, j, k, g1, g2);
+            const float M = Cc[C_M * CELL + cell], U = Cc[C_MU * CELL + cell];
             const float L = M - 2.f * U;
             const float dt = a.dt;
+            float oxx = Cc[0 * CELL + cell], ozz = Cc[1 * CELL + cell], oxz = Cc[2 * CELL + cell];
+            float oyy = 0.f, oxy = 0.f, oyz = 0.f;
+            if (Y) {
+                oyy = Cc[3 * CELL + cell];
+                oxy = Cc[4 * CELL + cell];
+                oyz = Cc[5 * CELL + cell];
+            }
             if (src_here && k == a.ssz) {     // add_source_3D into txx, tyy, tzz
                 oxx += wsrc;
                 ozz += wsrc;
                 if (Y) oyy += wsrc;
             }
-            txx[c] = g1 * (g2 * oxx + dt * (M * exx + L * (eyy + ezz)));
-            tzz[c] = g1 * (g2 * ozz + dt * (M * ezz + L * (exx + eyy)));
-            txz[c] = g1 * (g2 * oxz + dt * U * (dzvx + dxvz));
+            sig[0][c] = g1 * (g2 * oxx + dt * (M * exx + L * (eyy + ezz)));
+            sig[1][c] = g1 * (g2 * ozz + dt * (M * ezz + L * (exx + eyy)));
+            sig[2][c] = g1 * (g2 * oxz + dt * U * (dzvx + dxvz));
             if (Y) {
-                tyy[c] = g1 * (g2 * oyy + dt * (M * eyy + L * (exx + ezz)));
-                txy[c] = g1 * (g2 * oxy + dt * U * (dyvx + dxvy));
-                tyz[c] = g1 * (g2 * oyz + dt * U * (dzvy + dyvz));
+                sig[3][c] = g1 * (g2 * oyy + dt * (M * eyy + L * (exx + ezz)));
+                sig[4][c] = g1 * (g2 * oxy + dt * U * (dyvx + dxvy));
+                sig[5][c] = g1 * (g2 * oyz + dt * U * (dzvy + dyvz));
             }
-            if (PS) tp[c] = g1 * (g2 * otp + dt * M * (exx + eyy + ezz));
+            if (PS) tp[c] = g1 * (g2 * Cc[C_TP * CELL + cell] + dt * M * (exx + eyy + ezz));
         }
-        __syncthreads();
 
 #pragma unroll
         for (int q = 0; q < 2 * R; q++) {
@@ -239,32 +324,46 @@ k_stress(const KArgs a)
             qz[q] = qz[q + 1];
             if (Y) qy[q] = qy[q + 1];
         }
-        qx[2 * R] = nx_;
-        qz[2 * R] = nz_;
-        if (Y) qy[2 * R] = ny_;
-        c += sz;
-        cm += a.msz;
+        qx[2 * R] = fx;
+        qz[2 * R] = fz;
+        if (Y) qy[2 * R] = fy;
+        cpa_wait_all();
+        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
 // Velocity kernel
 // ---------------------------------------------------------------------------
+template <int R, bool Y, bool CPML, int EPI>
+struct VelShape {
+    static constexpr bool PS = (EPI != EPI_NONE);
+    // tiles: txx, txz, (txy, tyy, tyz), (tp)
+    static constexpr int T_TXX = 0, T_TXZ = 1, T_TXY = 2, T_TYY = 3, T_TYZ = 4;
+    static constexpr int T_TP = Y ? 5 : 2;
+    static constexpr int NV = (Y ? 5 : 2) + (PS ? 1 : 0);
+    // cells: vx, vz, (vy), (vxp, vzp, (vyp)), b, (excitation amp2 / time)
+    static constexpr int C_VX = 0, C_VZ = 1, C_VY = 2;
+    static constexpr int C_PX = Y ? 3 : 2;
+    static constexpr int C_PZ = C_PX + 1, C_PY = C_PX + 2;
+    static constexpr int C_B = PS ? C_PX + (Y ? 3 : 2) : C_PX;
+    static constexpr int C_EX = C_B + 1;
+    static constexpr int NC = C_B + 1 + (PS ? 1 : 0);
+    static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
+    using S = Stage<R, Y, NV, NC, NP>;
+};
+
 template <int R, bool Y, bool CPML, int EPI, bool REC>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2))
+__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), 1)
 k_velocity(const KArgs a)
 {
-    constexpr bool PS = (EPI != EPI_NONE);
-    constexpr int TYB = Y ? TY3 : TY2;
-    constexpr int SW = TX + 2 * R;
-    constexpr int SH = Y ? TYB + 2 * R : TYB;
+    using VS = VelShape<R, Y, CPML, EPI>;
+    using S = typename VS::S;
+    constexpr bool PS = VS::PS;
+    constexpr int TYB = S::TYB, SW = S::SW, TILE = S::TILE, CELL = S::CELL;
+    constexpr int NV = VS::NV, NC = VS::NC;
     constexpr int YO = Y ? R : 0;
-    __shared__ float s_txx[SH][SW];
-    __shared__ float s_txz[SH][SW];
-    __shared__ float s_txy[Y ? SH : 1][Y ? SW : 1];
-    __shared__ float s_tyy[Y ? SH : 1][Y ? SW : 1];
-    __shared__ float s_tyz[Y ? SH : 1][Y ? SW : 1];
-    __shared__ float s_tp[PS ? SH : 1][PS ? SW : 1];
+    extern __shared__ __align__(16) float sm[];
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i = blockIdx.x * TX + tx;
@@ -276,93 +375,154 @@ k_velocity(const KArgs a)
     const int it = __ldg(a.it_ptr);
     const int rec = ((REC || EPI == EPI_IMAGE) && act) ? receiver_index(a, i, j) : -1;
     const long long nrec = (long long)a.nrx * a.nry;
+    const int r = ty + YO, s = tx + R, cell = ty * TX + tx;
+    const long long cj = (long long)j * sy + i;
+    const long long mj = (long long)j * a.msy + i;
 
-    const float* __restrict__ txx = a.f[F_TXX];
-    const float* __restrict__ tyy = a.f[F_TYY];
-    const float* __restrict__ tzz = a.f[F_TZZ];
-    const float* __restrict__ txy = a.f[F_TXY];
-    const float* __restrict__ txz = a.f[F_TXZ];
-    const float* __restrict__ tyz = a.f[F_TYZ];
-    const float* __restrict__ tp = a.f[F_TP];
-    float* __restrict__ vx = a.f[F_VX];
-    float* __restrict__ vy = a.f[F_VY];
-    float* __restrict__ vz = a.f[F_VZ];
-    float* __restrict__ vxp = a.f[F_VXP];
-    float* __restrict__ vyp = a.f[F_VYP];
-    float* __restrict__ vzp = a.f[F_VZP];
+    const float* txx = a.f[F_TXX];
+    const float* tyy = a.f[F_TYY];
+    const float* tzz = a.f[F_TZZ];
+    const float* txy = a.f[F_TXY];
+    const float* txz = a.f[F_TXZ];
+    const float* tyz = a.f[F_TYZ];
+    const float* tp = a.f[F_TP];
+    float* vx = a.f[F_VX];
+    float* vy = a.f[F_VY];
+    float* vz = a.f[F_VZ];
+    float* vxp = a.f[F_VXP];
+    float* vyp = a.f[F_VYP];
+    float* vzp = a.f[F_VZP];
 
-    long long c = (long long)k0 * sz + (long long)j * sy + i;
-    long long cm = (long long)k0 * a.msz + (long long)j * a.msy + i;
+    const int WX = a.w[0] + a.w[1], WY = a.w[2] + a.w[3];
+    const bool inx = CPML && act && (i < a.w[0] || i >= a.nx - a.w[1]);
+    const bool iny = CPML && Y && act && (j < a.w[2] || j >= a.ny - a.w[3]);
+    const int slx = i < a.w[0] ? i : i - a.nx + WX;
+    const int sly = j < a.w[2] ? j : j - a.ny + WY;
+    float axf = 0.f, bxf = 1.f, axh = 0.f, bxh = 1.f, ayf = 0.f, byf = 1.f, ayh = 0.f, byh = 1.f;
+    if (inx) {
+        axf = __ldg(a.pa[0][0] + i); bxf = __ldg(a.pb[0][0] + i);
+        axh = __ldg(a.pa[0][1] + i); bxh = __ldg(a.pb[0][1] + i);
+    }
+    if (iny) {
+        ayf = __ldg(a.pa[1][0] + j); byf = __ldg(a.pb[1][0] + j);
+        ayh = __ldg(a.pa[1][1] + j); byh = __ldg(a.pb[1][1] + j);
+    }
+    // psi slots: x: DXTXX DXTXZ (DXTXY), y: DYTXY DYTYY DYTYZ, z: DZTXZ DZTZZ (DZTYZ)
+    constexpr int PX = 0, PY = Y ? 3 : 2, PZ = Y ? 6 : 2;
+
+    auto issue = [&](int p, int st, float cxz, float cyz, float ctp) {
+        float* T = sm + st * S::FLOATS;
+        float* Cc = T + NV * TILE;
+        float* Ps = Cc + NC * CELL;
+        const long long cp = (long long)p * sz + cj;
+        // centres: from the z queues where there is one, else copied
+        T[VS::T_TXZ * TILE + r * SW + s] = cxz;
+        cpa4(&T[VS::T_TXX * TILE + r * SW + s], txx + cp);
+        if (Y) {
+            T[VS::T_TYZ * TILE + r * SW + s] = cyz;
+            cpa4(&T[VS::T_TXY * TILE + r * SW + s], txy + cp);
+            cpa4(&T[VS::T_TYY * TILE + r * SW + s], tyy + cp);
+        }
+        if (PS) T[VS::T_TP * TILE + r * SW + s] = ctp;
+        if (tx < R) {   // x halos: txx, txz, (txy), (tp)
+            cpa4(&T[VS::T_TXX * TILE + r * SW + tx], txx + cp - R);
+            cpa4(&T[VS::T_TXX * TILE + r * SW + tx + TX + R], txx + cp + TX);
+            cpa4(&T[VS::T_TXZ * TILE + r * SW + tx], txz + cp - R);
+            cpa4(&T[VS::T_TXZ * TILE + r * SW + tx + TX + R], txz + cp + TX);
+            if (Y) {
+                cpa4(&T[VS::T_TXY * TILE + r * SW + tx], txy + cp - R);
+                cpa4(&T[VS::T_TXY * TILE + r * SW + tx + TX + R], txy + cp + TX);
+            }
+            if (PS) {
+                cpa4(&T[VS::T_TP * TILE + r * SW + tx], tp + cp - R);
+                cpa4(&T[VS::T_TP * TILE + r * SW + tx + TX + R], tp + cp + TX);
+            }
+        }
+        if (Y && ty < R) {   // y halos: txy, tyy, tyz, (tp)
+            const long long lo = cp - R * sy, hi = cp + TYB * sy;
+            const int rl = ty * SW + s, rh = (ty + TYB + R) * SW + s;
+            cpa4(&T[VS::T_TXY * TILE + rl], txy + lo);
+            cpa4(&T[VS::T_TXY * TILE + rh], txy + hi);
+            cpa4(&T[VS::T_TYY * TILE + rl], tyy + lo);
+            cpa4(&T[VS::T_TYY * TILE + rh], tyy + hi);
+            cpa4(&T[VS::T_TYZ * TILE + rl], tyz + lo);
+            cpa4(&T[VS::T_TYZ * TILE + rh], tyz + hi);
+            if (PS) {
+                cpa4(&T[VS::T_TP * TILE + rl], tp + lo);
+                cpa4(&T[VS::T_TP * TILE + rh], tp + hi);
+            }
+        }
+        if (act) {
+            cpa4(&Cc[VS::C_VX * CELL + cell], vx + cp);
+            cpa4(&Cc[VS::C_VZ * CELL + cell], vz + cp);
+            if (Y) cpa4(&Cc[VS::C_VY * CELL + cell], vy + cp);
+            if (PS) {
+                cpa4(&Cc[VS::C_PX * CELL + cell], vxp + cp);
+                cpa4(&Cc[VS::C_PZ * CELL + cell], vzp + cp);
+                if (Y) cpa4(&Cc[VS::C_PY * CELL + cell], vyp + cp);
+            }
+            cpa4(&Cc[VS::C_B * CELL + cell], a.B + (long long)p * a.msz + mj);
+            if (EPI == EPI_EXCITE) cpa4(&Cc[VS::C_EX * CELL + cell], a.ex_amp2 + cp);
+            if (EPI == EPI_IMAGE) cpa4(&Cc[VS::C_EX * CELL + cell], a.ex_time + cp);
+            if (CPML) {
+                if (inx) {
+                    const long long x = ((long long)p * a.ny + j) * WX + slx;
+                    cpa4(&Ps[(PX + 0) * CELL + cell], a.psi[P_DXTXX] + x);
+                    cpa4(&Ps[(PX + 1) * CELL + cell], a.psi[P_DXTXZ] + x);
+                    if (Y) cpa4(&Ps[(PX + 2) * CELL + cell], a.psi[P_DXTXY] + x);
+                }
+                if (iny) {
+                    const long long y = ((long long)p * WY + sly) * a.nx + i;
+                    cpa4(&Ps[(PY + 0) * CELL + cell], a.psi[P_DYTXY] + y);
+                    cpa4(&Ps[(PY + 1) * CELL + cell], a.psi[P_DYTYY] + y);
+                    cpa4(&Ps[(PY + 2) * CELL + cell], a.psi[P_DYTYZ] + y);
+                }
+                if (p < a.w[4] || p >= a.nz - a.w[5]) {
+                    const int sl = p < a.w[4] ? p : p - a.nz + a.w[4] + a.w[5];
+                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    cpa4(&Ps[(PZ + 0) * CELL + cell], a.psi[P_DZTXZ] + z);
+                    cpa4(&Ps[(PZ + 1) * CELL + cell], a.psi[P_DZTZZ] + z);
+                    if (Y) cpa4(&Ps[(PZ + 2) * CELL + cell], a.psi[P_DZTYZ] + z);
+                }
+            }
+        }
+        cpa_commit();
+    };
 
     float qxz[2 * R + 1], qyz[2 * R + 1], qzz[2 * R + 1], qtp[2 * R + 1];
 #pragma unroll
     for (int q = 0; q <= 2 * R; q++) {
-        long long cc = c + (long long)(q - R) * sz;
+        const long long cc = (long long)(k0 + q - R) * sz + cj;
         qxz[q] = txz[cc];
         qzz[q] = tzz[cc];
         if (Y) qyz[q] = tyz[cc];
         if (PS) qtp[q] = tp[cc];
     }
+    issue(k0, 0, qxz[R], Y ? qyz[R] : 0.f, PS ? qtp[R] : 0.f);
+    cpa_wait_all();
+    __syncthreads();
 
-    const int r = ty + YO, s = tx + R;
     for (int k = k0; k < k1; ++k) {
+        const int st = (k - k0) & 1;
         const bool more = (k + 1 < k1);
-        float n_xz = 0.f, n_yz = 0.f, n_zz = 0.f, n_tp = 0.f;
+        float f_xz = 0.f, f_yz = 0.f, f_zz = 0.f, f_tp = 0.f;
         if (more) {
-            long long cn = c + (long long)(R + 1) * sz;
-            n_xz = txz[cn];
-            n_zz = tzz[cn];
-            if (Y) n_yz = tyz[cn];
-            if (PS) n_tp = tp[cn];
+            const long long cn = (long long)(k + 1 + R) * sz + cj;
+            f_xz = txz[cn];
+            f_zz = tzz[cn];
+            if (Y) f_yz = tyz[cn];
+            if (PS) f_tp = tp[cn];
+            issue(k + 1, st ^ 1, qxz[R + 1], Y ? qyz[R + 1] : 0.f, PS ? qtp[R + 1] : 0.f);
         }
-        float ovx = 0.f, ovy = 0.f, ovz = 0.f, opx = 0.f, opy = 0.f, opz = 0.f, b = 0.f;
-        if (act) {
-            ovx = vx[c];
-            ovz = vz[c];
-            if (Y) ovy = vy[c];
-            if (PS) {
-                opx = vxp[c];
-                opz = vzp[c];
-                if (Y) opy = vyp[c];
-            }
-            b = __ldg(a.B + cm);
-        }
-
-        s_txx[r][s] = txx[c];
-        s_txz[r][s] = qxz[R];
-        if (Y) {
-            s_txy[r][s] = txy[c];
-            s_tyy[r][s] = tyy[c];
-            s_tyz[r][s] = qyz[R];
-        }
-        if (PS) s_tp[r][s] = qtp[R];
-        if (tx < R) {
-            s_txx[r][tx] = txx[c - R];
-            s_txx[r][tx + TX + R] = txx[c + TX];
-            s_txz[r][tx] = txz[c - R];
-            s_txz[r][tx + TX + R] = txz[c + TX];
-            if (Y) {
-                s_txy[r][tx] = txy[c - R];
-                s_txy[r][tx + TX + R] = txy[c + TX];
-            }
-            if (PS) {
-                s_tp[r][tx] = tp[c - R];
-                s_tp[r][tx + TX + R] = tp[c + TX];
-            }
-        }
-        if (Y && ty < R) {
-            s_txy[ty][s] = txy[c - R * sy];
-            s_txy[ty + TYB + R][s] = txy[c + TYB * sy];
-            s_tyy[ty][s] = tyy[c - R * sy];
-            s_tyy[ty + TYB + R][s] = tyy[c + TYB * sy];
-            s_tyz[ty][s] = tyz[c - R * sy];
-            s_tyz[ty + TYB + R][s] = tyz[c + TYB * sy];
-            if (PS) {
-                s_tp[ty][s] = tp[c - R * sy];
-                s_tp[ty + TYB + R][s] = tp[c + TYB * sy];
-            }
-        }
-        __syncthreads();
+        const float* T = sm + st * S::FLOATS;
+        const float* Cc = T + NV * TILE;
+        const float* Ps = Cc + NC * CELL;
+        const float* Txx = T + VS::T_TXX * TILE;
+        const float* Txz = T + VS::T_TXZ * TILE;
+        const float* Txy = T + VS::T_TXY * TILE;
+        const float* Tyy = T + VS::T_TYY * TILE;
+        const float* Tyz = T + VS::T_TYZ * TILE;
+        const float* Ttp = T + VS::T_TP * TILE;
 
         float dxtxx = 0.f, dytxy = 0.f, dztxz = 0.f;
         float dxtxy = 0.f, dytyy = 0.f, dztyz = 0.f;
@@ -370,78 +530,86 @@ k_velocity(const KArgs a)
         float dxtp = 0.f, dytp = 0.f, dztp = 0.f;
 #pragma unroll
         for (int n = 1; n <= R; n++) {
-            dxtxx = fmaf(a.cx[n], s_txx[r][s + n - 1] - s_txx[r][s - n], dxtxx);
-            dxtxz = fmaf(a.cx[n], s_txz[r][s + n] - s_txz[r][s - n + 1], dxtxz);
+            dxtxx = fmaf(a.cx[n], Txx[r * SW + s + n - 1] - Txx[r * SW + s - n], dxtxx);
+            dxtxz = fmaf(a.cx[n], Txz[r * SW + s + n] - Txz[r * SW + s - n + 1], dxtxz);
             dztxz = fmaf(a.cz[n], qxz[R + n - 1] - qxz[R - n], dztxz);
             dztzz = fmaf(a.cz[n], qzz[R + n] - qzz[R - n + 1], dztzz);
             if (Y) {
-                dytxy = fmaf(a.cy[n], s_txy[r + n][s] - s_txy[r - n + 1][s], dytxy);
-                dxtxy = fmaf(a.cx[n], s_txy[r][s + n] - s_txy[r][s - n + 1], dxtxy);
-                dytyy = fmaf(a.cy[n], s_tyy[r + n - 1][s] - s_tyy[r - n][s], dytyy);
+                dytxy = fmaf(a.cy[n], Txy[(r + n) * SW + s] - Txy[(r - n + 1) * SW + s], dytxy);
+                dxtxy = fmaf(a.cx[n], Txy[r * SW + s + n] - Txy[r * SW + s - n + 1], dxtxy);
+                dytyy = fmaf(a.cy[n], Tyy[(r + n - 1) * SW + s] - Tyy[(r - n) * SW + s], dytyy);
                 dztyz = fmaf(a.cz[n], qyz[R + n - 1] - qyz[R - n], dztyz);
-                dytyz = fmaf(a.cy[n], s_tyz[r + n][s] - s_tyz[r - n + 1][s], dytyz);
+                dytyz = fmaf(a.cy[n], Tyz[(r + n) * SW + s] - Tyz[(r - n + 1) * SW + s], dytyz);
             }
             if (PS) {
-                dxtp = fmaf(a.cx[n], s_tp[r][s + n - 1] - s_tp[r][s - n], dxtp);
+                dxtp = fmaf(a.cx[n], Ttp[r * SW + s + n - 1] - Ttp[r * SW + s - n], dxtp);
                 dztp = fmaf(a.cz[n], qtp[R + n] - qtp[R - n + 1], dztp);
-                if (Y) dytp = fmaf(a.cy[n], s_tp[r + n - 1][s] - s_tp[r - n][s], dytp);
+                if (Y) dytp = fmaf(a.cy[n], Ttp[(r + n - 1) * SW + s] - Ttp[(r - n) * SW + s], dytp);
             }
         }
 
         if (act) {
+            const long long c = (long long)k * sz + cj;
             if (CPML) {
-                const int w0 = a.w[0], w1 = a.w[1];
-                if (i < w0 || i >= a.nx - w1) {
-                    int sl = i < w0 ? i : i - a.nx + w0 + w1;
-                    long long p = ((long long)k * a.ny + j) * (w0 + w1) + sl;
-                    dxtxx = cpml_upd(a.psi[P_DXTXX], p, __ldg(a.pa[0][1] + i), __ldg(a.pb[0][1] + i),
-                                     dxtxx);
-                    dxtxz = cpml_upd(a.psi[P_DXTXZ], p, __ldg(a.pa[0][0] + i), __ldg(a.pb[0][0] + i),
-                                     dxtxz);
-                    if (Y)
-                        dxtxy = cpml_upd(a.psi[P_DXTXY], p, __ldg(a.pa[0][0] + i),
-                                         __ldg(a.pb[0][0] + i), dxtxy);
-                }
-                if (Y) {
-                    const int w2 = a.w[2], w3 = a.w[3];
-                    if (j < w2 || j >= a.ny - w3) {
-                        int sl = j < w2 ? j : j - a.ny + w2 + w3;
-                        long long p = ((long long)k * (w2 + w3) + sl) * a.nx + i;
-                        dytxy = cpml_upd(a.psi[P_DYTXY], p, __ldg(a.pa[1][0] + j),
-                                         __ldg(a.pb[1][0] + j), dytxy);
-                        dytyy = cpml_upd(a.psi[P_DYTYY], p, __ldg(a.pa[1][1] + j),
-                                         __ldg(a.pb[1][1] + j), dytyy);
-                        dytyz = cpml_upd(a.psi[P_DYTYZ], p, __ldg(a.pa[1][0] + j),
-                                         __ldg(a.pb[1][0] + j), dytyz);
+                if (inx) {
+                    const long long x = ((long long)k * a.ny + j) * WX + slx;
+                    float p0 = fmaf(bxh, Ps[(PX + 0) * CELL + cell], axh * dxtxx);
+                    float p1 = fmaf(bxf, Ps[(PX + 1) * CELL + cell], axf * dxtxz);
+                    a.psi[P_DXTXX][x] = p0;
+                    a.psi[P_DXTXZ][x] = p1;
+                    dxtxx += p0;
+                    dxtxz += p1;
+                    if (Y) {
+                        float p2 = fmaf(bxf, Ps[(PX + 2) * CELL + cell], axf * dxtxy);
+                        a.psi[P_DXTXY][x] = p2;
+                        dxtxy += p2;
                     }
                 }
-                const int w4 = a.w[4], w5 = a.w[5];
-                if (k < w4 || k >= a.nz - w5) {
-                    int sl = k < w4 ? k : k - a.nz + w4 + w5;
-                    long long p = ((long long)sl * a.ny + j) * a.nx + i;
-                    dztxz = cpml_upd(a.psi[P_DZTXZ], p, __ldg(a.pa[2][0] + k), __ldg(a.pb[2][0] + k),
-                                     dztxz);
-                    dztzz = cpml_upd(a.psi[P_DZTZZ], p, __ldg(a.pa[2][1] + k), __ldg(a.pb[2][1] + k),
-                                     dztzz);
-                    if (Y)
-                        dztyz = cpml_upd(a.psi[P_DZTYZ], p, __ldg(a.pa[2][0] + k),
-                                         __ldg(a.pb[2][0] + k), dztyz);
+                if (iny) {
+                    const long long y = ((long long)k * WY + sly) * a.nx + i;
+                    float p0 = fmaf(byf, Ps[(PY + 0) * CELL + cell], ayf * dytxy);
+                    float p1 = fmaf(byh, Ps[(PY + 1) * CELL + cell], ayh * dytyy);
+                    float p2 = fmaf(byf, Ps[(PY + 2) * CELL + cell], ayf * dytyz);
+                    a.psi[P_DYTXY][y] = p0;
+                    a.psi[P_DYTYY][y] = p1;
+                    a.psi[P_DYTYZ][y] = p2;
+                    dytxy += p0;
+                    dytyy += p1;
+                    dytyz += p2;
+                }
+                if (k < a.w[4] || k >= a.nz - a.w[5]) {
+                    const int sl = k < a.w[4] ? k : k - a.nz + a.w[4] + a.w[5];
+                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    const float azf = __ldg(a.pa[2][0] + k), bzf = __ldg(a.pb[2][0] + k);
+                    const float azh = __ldg(a.pa[2][1] + k), bzh = __ldg(a.pb[2][1] + k);
+                    float p0 = fmaf(bzf, Ps[(PZ + 0) * CELL + cell], azf * dztxz);
+                    float p1 = fmaf(bzh, Ps[(PZ + 1) * CELL + cell], azh * dztzz);
+                    a.psi[P_DZTXZ][z] = p0;
+                    a.psi[P_DZTZZ][z] = p1;
+                    dztxz += p0;
+                    dztzz += p1;
+                    if (Y) {
+                        float p2 = fmaf(bzf, Ps[(PZ + 2) * CELL + cell], azf * dztyz);
+                        a.psi[P_DZTYZ][z] = p2;
+                        dztyz += p2;
+                    }
                 }
             }
             float g1, g2;
             damping<Y>(a, CPML, i, j, k, g1, g2);
+            const float b = Cc[VS::C_B * CELL + cell];
             const float db = a.dt * b;
-            float nvx = g1 * (g2 * ovx + db * (dxtxx + dytxy + dztxz));
-            float nvz = g1 * (g2 * ovz + db * (dxtxz + dytyz + dztzz));
+            float nvx = g1 * (g2 * Cc[VS::C_VX * CELL + cell] + db * (dxtxx + dytxy + dztxz));
+            float nvz = g1 * (g2 * Cc[VS::C_VZ * CELL + cell] + db * (dxtxz + dytyz + dztzz));
             float nvy = 0.f;
-            if (Y) nvy = g1 * (g2 * ovy + db * (dxtxy + dytyy + dztyz));
+            if (Y) nvy = g1 * (g2 * Cc[VS::C_VY * CELL + cell] + db * (dxtxy + dytyy + dztyz));
             float npx = 0.f, npy = 0.f, npz = 0.f;
             if (PS) {
                 // decoupled P velocity from the P-stress gradient (role of fwd_vxp_vzp_3D,
                 // 3D_forward_or_back_together.cu:118); S velocity = v - v_P
-                npx = g1 * (g2 * opx + db * dxtp);
-                npz = g1 * (g2 * opz + db * dztp);
-                if (Y) npy = g1 * (g2 * opy + db * dytp);
+                npx = g1 * (g2 * Cc[VS::C_PX * CELL + cell] + db * dxtp);
+                npz = g1 * (g2 * Cc[VS::C_PZ * CELL + cell] + db * dztp);
+                if (Y) npy = g1 * (g2 * Cc[VS::C_PY * CELL + cell] + db * dytp);
                 vxp[c] = npx;
                 vzp[c] = npz;
                 if (Y) vyp[c] = npy;
@@ -450,7 +618,7 @@ k_velocity(const KArgs a)
                 // caculate_ex_amp_time_new (2D_elastic_RTM/elastic_2D_kernel_3.cu:30-48):
                 // strict '>' keeps the earliest maximum of |v_P|
                 float a2 = npx * npx + npy * npy + npz * npz;
-                if (a2 > a.ex_amp2[c]) {
+                if (a2 > Cc[VS::C_EX * CELL + cell]) {
                     a.ex_amp2[c] = a2;
                     a.ex_time[c] = it;
                     a.ex_v[0][c] = npx;
@@ -462,14 +630,13 @@ k_velocity(const KArgs a)
             if (EPI == EPI_IMAGE) {
                 // imaging_inner_product_ex / imaging_correlation_ex
                 // (2D_elastic_RTM/elastic_2D_kernel_3.cu:542-576) at it == excitation time
-                if (a.ex_time[c] == it) {
+                if (__float_as_int(Cc[VS::C_EX * CELL + cell]) == it) {
                     float ex = a.ex_v[0][c], ey = Y ? a.ex_v[1][c] : 0.f, ez = a.ex_v[2][c];
                     float den = ex * ex + ey * ey + ez * ez;
-                    if (den > 0.f) {
-                        float inv = 1.f / den;
-                        if (a.img[0]) a.img[0][c] = (ex * npx + ey * npy + ez * npz) * inv;
+                    if (den > 0.f) {   // a true division: 1/den overflows for denormal den
+                        if (a.img[0]) a.img[0][c] = (ex * npx + ey * npy + ez * npz) / den;
                         if (a.img[1])
-                            a.img[1][c] = (ex * (nvx - npx) + ey * (nvy - npy) + ez * (nvz - npz)) * inv;
+                            a.img[1][c] = (ex * (nvx - npx) + ey * (nvy - npy) + ez * (nvz - npz)) / den;
                     }
                     float et = a.ex_tp[c];
                     if (a.img[2] && et != 0.f) a.img[2][c] = qtp[R] / et;
@@ -501,7 +668,6 @@ k_velocity(const KArgs a)
                 d[2 * cs] = nvz;
             }
         }
-        __syncthreads();
 
 #pragma unroll
         for (int q = 0; q < 2 * R; q++) {
@@ -510,18 +676,37 @@ k_velocity(const KArgs a)
             if (Y) qyz[q] = qyz[q + 1];
             if (PS) qtp[q] = qtp[q + 1];
         }
-        qxz[2 * R] = n_xz;
-        qzz[2 * R] = n_zz;
-        if (Y) qyz[2 * R] = n_yz;
-        if (PS) qtp[2 * R] = n_tp;
-        c += sz;
-        cm += a.msz;
+        qxz[2 * R] = f_xz;
+        qzz[2 * R] = f_zz;
+        if (Y) qyz[2 * R] = f_yz;
+        if (PS) qtp[2 * R] = f_tp;
+        cpa_wait_all();
+        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
 // Launch helpers (instantiated per R in launch_r4.cu / launch_r6.cu)
 // ---------------------------------------------------------------------------
+// One instantiation per kernel, so the shared-memory opt-in below is made for
+// each kernel separately (the kernels all share one function type).
+template <void (*K)(KArgs)>
+static cudaError_t launch_dyn(dim3 grid, dim3 block, size_t smem, const KArgs& a, cudaStream_t st)
+{
+    // opt in to more than 48 KB of dynamic shared memory (once per kernel)
+    static cudaError_t attr = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+    if (attr != cudaSuccess) return attr;
+    K<<<grid, block, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, bool Y, bool C, bool P>
+static cudaError_t launch_stress_y(dim3 grid, dim3 block, const KArgs& a, cudaStream_t st)
+{
+    return launch_dyn<k_stress<R, Y, C, P>>(grid, block, StressShape<R, Y, C, P>::S::BYTES, a, st);
+}
+
 template <int R>
 cudaError_t launch_stress_t(const Geom& g, const KArgs& a, bool cpml, bool ps, cudaStream_t st)
 {
@@ -529,27 +714,33 @@ cudaError_t launch_stress_t(const Geom& g, const KArgs& a, bool cpml, bool ps, c
     const int tyb = Y ? TY3 : TY2;
     dim3 block(TX, tyb);
     dim3 grid((g.nx + TX - 1) / TX, (g.ny + tyb - 1) / tyb, (g.nz + a.kchunk - 1) / a.kchunk);
-#define ERTM_S(YY, CC, PP) k_stress<R, YY, CC, PP><<<grid, block, 0, st>>>(a)
     if (Y) {
-        if (cpml) { if (ps) ERTM_S(true, true, true); else ERTM_S(true, true, false); }
-        else { if (ps) ERTM_S(true, false, true); else ERTM_S(true, false, false); }
-    } else {
-        if (cpml) { if (ps) ERTM_S(false, true, true); else ERTM_S(false, true, false); }
-        else { if (ps) ERTM_S(false, false, true); else ERTM_S(false, false, false); }
+        if (cpml) return ps ? launch_stress_y<R, true, true, true>(grid, block, a, st)
+                            : launch_stress_y<R, true, true, false>(grid, block, a, st);
+        return ps ? launch_stress_y<R, true, false, true>(grid, block, a, st)
+                  : launch_stress_y<R, true, false, false>(grid, block, a, st);
     }
-#undef ERTM_S
-    return cudaGetLastError();
+    if (cpml) return ps ? launch_stress_y<R, false, true, true>(grid, block, a, st)
+                        : launch_stress_y<R, false, true, false>(grid, block, a, st);
+    return ps ? launch_stress_y<R, false, false, true>(grid, block, a, st)
+              : launch_stress_y<R, false, false, false>(grid, block, a, st);
 }
 
 template <int R, bool Y, bool C>
 static cudaError_t launch_velocity_y(dim3 grid, dim3 block, const KArgs& a, int epi, bool rec,
                                      cudaStream_t st)
 {
-    if (epi == EPI_EXCITE) k_velocity<R, Y, C, EPI_EXCITE, false><<<grid, block, 0, st>>>(a);
-    else if (epi == EPI_IMAGE) k_velocity<R, Y, C, EPI_IMAGE, false><<<grid, block, 0, st>>>(a);
-    else if (rec) k_velocity<R, Y, C, EPI_NONE, true><<<grid, block, 0, st>>>(a);
-    else k_velocity<R, Y, C, EPI_NONE, false><<<grid, block, 0, st>>>(a);
-    return cudaGetLastError();
+    if (epi == EPI_EXCITE)
+        return launch_dyn<k_velocity<R, Y, C, EPI_EXCITE, false>>(
+            grid, block, VelShape<R, Y, C, EPI_EXCITE>::S::BYTES, a, st);
+    if (epi == EPI_IMAGE)
+        return launch_dyn<k_velocity<R, Y, C, EPI_IMAGE, false>>(
+            grid, block, VelShape<R, Y, C, EPI_IMAGE>::S::BYTES, a, st);
+    if (rec)
+        return launch_dyn<k_velocity<R, Y, C, EPI_NONE, true>>(
+            grid, block, VelShape<R, Y, C, EPI_NONE>::S::BYTES, a, st);
+    return launch_dyn<k_velocity<R, Y, C, EPI_NONE, false>>(
+        grid, block, VelShape<R, Y, C, EPI_NONE>::S::BYTES, a, st);
 }
 
 template <int R>

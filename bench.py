@@ -49,11 +49,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-steps", type=int, default=60)
+    ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only time the step kernels (profiling cases)")
     return ap.parse_args()
 
 
-def workload(small: bool):
+def workload(small: bool, grid: str = ""):
     synth = importlib.import_module(PKG + ".synthetic")
+    if grid:
+        nx, ny, nz = (int(v) for v in grid.split(","))
+        return synth.layered_3d(n_interior=(nz, ny, nx), nt=400, smooth_sigma=0)
     if small:
         return synth.layered_3d(n_interior=(60, 80, 80), pml=20, nt=400, smooth_sigma=4.0)
     return synth.layered_3d()
@@ -195,9 +201,20 @@ def main():
 
     ertm = importlib.import_module(PKG)
     synth = importlib.import_module(PKG + ".synthetic")
-    wl = workload(args.small)
+    wl = workload(args.small, args.grid)
     nz, ny, nx = wl.shape
     cells = nx * ny * nz
+    if args.kernels_only:
+        ctx = ertm.Context(ertm.Config(nx=nx, ny=ny, nz=nz, dx=wl.dx, dy=wl.dy, dz=wl.dz,
+                                       dt_ms=wl.dt_ms, nt=wl.nt, order=8, pml=(wl.pml,) * 6,
+                                       device=local))
+        ctx.set_model(ertm.MIGRATION_MODEL, wl.svp, wl.svs, wl.srho)
+        ms = ctx.time_kernels(_shot(ertm, wl, synth, 0), args.kernel_steps)
+        print(json.dumps({"workload": wl.name, "cells": cells, "steps": args.kernel_steps,
+                          "ms_per_launch": [m / args.kernel_steps for m in ms],
+                          "gcells": [cells / (m / args.kernel_steps) / 1e6 for m in ms]}))
+        ctx.close()
+        return
     cfg = ertm.Config(nx=nx, ny=ny, nz=nz, dx=wl.dx, dy=wl.dy, dz=wl.dz, dt_ms=wl.dt_ms,
                       nt=wl.nt, order=8, boundary=ertm.BOUNDARY_CPML, pml=(wl.pml,) * 6,
                       device=local)
