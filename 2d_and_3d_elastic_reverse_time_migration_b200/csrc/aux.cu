@@ -211,17 +211,18 @@ cudaError_t launch_divcurl(int R, const Geom& g, const KArgs& a, const float* vp
     return cudaGetLastError();
 }
 
-cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, bool cpml, bool psplit,
-                          cudaStream_t s)
+cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,
+                          bool psplit, cudaStream_t s)
 {
-    return R == 4 ? launch_stress_r4(g, a, cpml, psplit, s) : launch_stress_r6(g, a, cpml, psplit, s);
+    return R == 4 ? launch_stress_r4(g, a, m, cpml, psplit, s)
+                  : launch_stress_r6(g, a, m, cpml, psplit, s);
 }
 
-cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
-                            cudaStream_t s)
+cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, const VelMaps& m, bool cpml,
+                            int epi, bool record, cudaStream_t s)
 {
-    return R == 4 ? launch_velocity_r4(g, a, cpml, epi, record, s)
-                  : launch_velocity_r6(g, a, cpml, epi, record, s);
+    return R == 4 ? launch_velocity_r4(g, a, m, cpml, epi, record, s)
+                  : launch_velocity_r6(g, a, m, cpml, epi, record, s);
 }
 
 }  // namespace ertm

@@ -6,6 +6,8 @@
 // buffer; passes are stream-ordered on the context stream and each public call
 // synchronises that stream before returning.  The whole grid lives on one GPU
 // (no z-slab decomposition, unlike the reference's exchange_device_nz_kernel_*).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -77,6 +79,12 @@ struct ertm_ctx {
     int wavelet_cap = 0;
     int* it_d = nullptr;
     float* vmax_d = nullptr;
+    int* err_d = nullptr;
+
+    // TMA tensor maps (box shapes C, X, Y, XY; see StressMaps / VelMaps)
+    CUtensorMap mC[NFIELD], mX[NFIELD], mY[NFIELD], mXY[NFIELD];
+    CUtensorMap mModel[2][3];
+    CUtensorMap mExAmp, mExTime;
 
     std::string err;
     long long launches = 0;
@@ -280,6 +288,117 @@ int validate_shot(ertm_ctx* c, const ertm_shot* s, bool need_source)
     return ERTM_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                             &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }();
+    return fn;
+}
+
+// One tensor map over a whole padded volume (allocation base, [pz][py][px]) with a
+// bx x by x 1 box.  TMA requires 16-byte aligned bases and strides: cudaMalloc bases
+// are 256-byte aligned and the row pitch is a multiple of 128 bytes.
+int encode_map(ertm_ctx* c, CUtensorMap* m, const void* base, bool is_int, int bx, int by)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return fail(c, ERTM_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    const Geom& g = c->g;
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
+    cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)(g.px * g.py) * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(m, is_int ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                     const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, ERTM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return ERTM_OK;
+}
+
+struct BoxDims {
+    int c_x, c_y, x_x, y_y;
+};
+BoxDims box_dims(const ertm_ctx* c)
+{
+    const int tyb = c->g.tyb;
+    const int xw = TX + 2 * xb_of(c->R);
+    const int yh = tyb + (c->g.two_d ? 0 : 2 * c->R);
+    return {TX, tyb, xw, yh};
+}
+
+// tensor maps of every field: centre boxes for all, halo boxes where a kernel
+// differentiates along x / y: vx vy vz tp txy (XY), txx txz (X), tyy tyz (Y)
+int build_field_maps(ertm_ctx* c)
+{
+    BoxDims b = box_dims(c);
+    int rc;
+    for (int q = 0; q < NFIELD; q++) {
+        if (!c->f_base[q]) continue;
+        if ((rc = encode_map(c, &c->mC[q], c->f_base[q], false, b.c_x, b.c_y))) return rc;
+        if ((rc = encode_map(c, &c->mX[q], c->f_base[q], false, b.x_x, b.c_y))) return rc;
+        if ((rc = encode_map(c, &c->mXY[q], c->f_base[q], false, b.x_x, b.y_y))) return rc;
+        if ((rc = encode_map(c, &c->mY[q], c->f_base[q], false, b.c_x, b.y_y))) return rc;
+    }
+    return ERTM_OK;
+}
+
+StressMaps stress_maps(const ertm_ctx* c, int which)
+{
+    StressMaps m;
+    std::memset(&m, 0, sizeof m);
+    const int v[3] = {F_VX, F_VZ, F_VY};
+    for (int q = 0; q < 3; q++) {
+        m.v[q] = c->mXY[v[q]];
+        m.vc[q] = c->mC[v[q]];
+    }
+    const int sg[6] = {F_TXX, F_TZZ, F_TXZ, F_TYY, F_TXY, F_TYZ};
+    for (int q = 0; q < 6; q++) m.sig[q] = c->mC[sg[q]];
+    m.tp = c->mC[F_TP];
+    m.M = c->mModel[which][0];
+    m.MU = c->mModel[which][1];
+    return m;
+}
+
+VelMaps vel_maps(const ertm_ctx* c, int which, int epi)
+{
+    VelMaps m;
+    std::memset(&m, 0, sizeof m);
+    const bool Y = !c->g.two_d, ps = (epi != EPI_NONE);
+    m.txx = c->mX[F_TXX];
+    m.txz = c->mX[F_TXZ];
+    m.txy = c->mXY[F_TXY];
+    m.tp = c->mXY[F_TP];
+    m.tyy = c->mY[F_TYY];
+    m.tyz = c->mY[F_TYZ];
+    int n = 0;
+    m.c[n++] = c->mC[F_VX];
+    m.c[n++] = c->mC[F_VZ];
+    if (Y) m.c[n++] = c->mC[F_VY];
+    if (ps) {
+        m.c[n++] = c->mC[F_VXP];
+        m.c[n++] = c->mC[F_VZP];
+        if (Y) m.c[n++] = c->mC[F_VYP];
+    }
+    m.c[n++] = c->mModel[which][2];
+    if (epi == EPI_EXCITE) m.c[n++] = c->mExAmp;
+    if (epi == EPI_IMAGE) m.c[n++] = c->mExTime;
+    n = 0;
+    m.fr[n++] = c->mC[F_TXZ];
+    m.fr[n++] = c->mC[F_TZZ];
+    if (Y) m.fr[n++] = c->mC[F_TYZ];
+    if (ps) m.fr[n++] = c->mC[F_TP];
+    return m;
+}
+
 int ensure_traces(ertm_ctx* c, size_t n)
 {
     if (c->traces_cap >= n) return ERTM_OK;
@@ -303,6 +422,9 @@ int ensure_excitation(ertm_ctx* c)
         if ((rc = alloc_volume(c, &c->ex_v_base[q], &dummy))) return rc;
     }
     if ((rc = alloc_volume(c, &c->ex_tp_base, &dummy))) return rc;
+    const int tyb = c->g.tyb;
+    if ((rc = encode_map(c, &c->mExAmp, c->ex_amp2_base, false, TX, tyb))) return rc;
+    if ((rc = encode_map(c, &c->mExTime, c->ex_time_base, true, TX, tyb))) return rc;
     return ERTM_OK;
 }
 
@@ -378,21 +500,44 @@ void fill_args(ertm_ctx* c, int which, const ertm_shot* s, KArgs& a)
         a.img[q] = c->img_base[q] ? c->img_base[q] + g.off0 : nullptr;
     }
     a.ex_tp = c->ex_tp_base ? c->ex_tp_base + g.off0 : nullptr;
+    a.err = c->err_d;
 }
 
-// z planes per CTA: enough CTAs to fill the GPU at least twice.
+int check_device_error(ertm_ctx* c)
+{
+    int e = 0;
+    CK(c, cudaMemcpyAsync(&e, c->err_d, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (e) {
+        CK(c, cudaMemsetAsync(c->err_d, 0, sizeof(int), c->stream));
+        return fail(c, ERTM_EDEVICE, "a step kernel's bounded wait for its staged planes expired (code %d)", e);
+    }
+    return ERTM_OK;
+}
+
+// z planes per CTA.  The step kernels run one CTA per SM (3D) or a few (2D);
+// the chunk count minimises (waves of CTAs) x (planes per chunk + start-up cost),
+// the start-up being the z-queue fill and the TMA pipeline ramp (~2R planes).
 int choose_kchunk(const ertm_ctx* c)
 {
     const Geom& g = c->g;
     long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    long long want = 4LL * sms;
-    int chunks = (int)std::max(1LL, std::min((long long)g.nz, (want + cols - 1) / cols));
-    // keep at least 8R planes per chunk so the 2R-plane queue warm-up stays small
-    int kc = (g.nz + chunks - 1) / chunks;
-    kc = std::max(kc, std::min(g.nz, 8 * c->R));
-    return kc;
+    const long long slots = (long long)sms * (g.two_d ? 8 : 1);
+    const double startup = 2.0 * c->R;
+    int best = g.nz;
+    double best_cost = 1e300;
+    for (int kc = g.nz; kc >= std::min(g.nz, 16); kc--) {
+        long long chunks = (g.nz + kc - 1) / kc;
+        long long waves = (cols * chunks + slots - 1) / slots;
+        double cost = (double)waves * (kc + startup);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = kc;
+        }
+    }
+    return best;
 }
 
 int reset_state(ertm_ctx* c)
@@ -448,13 +593,15 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
         CK(c, launch_inject(a, nsteps - 1, c->stream));
         c->launches++;
     }
+    const StressMaps sm = stress_maps(c, which);
+    const VelMaps vm = vel_maps(c, which, epi);
     for (int step = 0; step < nsteps; step++) {
-        CK(c, launch_stress(R, c->g, a, cpml, psplit, c->stream));
-        CK(c, launch_velocity(R, c->g, a, cpml, epi, record, c->stream));
+        CK(c, launch_stress(R, c->g, a, sm, cpml, psplit, c->stream));
+        CK(c, launch_velocity(R, c->g, a, vm, cpml, epi, record, c->stream));
         CK(c, launch_advance(c->it_d, dir, c->stream));
         c->launches += 3;
     }
-    return ERTM_OK;
+    return check_device_error(c);
 }
 
 int copy_out_volume(ertm_ctx* c, const float* padded_origin, float* out)
@@ -592,11 +739,15 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
             }
         }
     }
-    if (cudaMalloc(&x->it_d, sizeof(int)) != cudaSuccess || cudaMalloc(&x->vmax_d, sizeof(float)) != cudaSuccess) {
+    if (cudaMalloc(&x->it_d, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&x->vmax_d, sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&x->err_d, sizeof(int)) != cudaSuccess ||
+        cudaMemsetAsync(x->err_d, 0, sizeof(int), x->stream) != cudaSuccess) {
         cudaGetLastError();
         fail(x, ERTM_ENOMEM, "counters");
         return bail(ERTM_ENOMEM);
     }
+    if ((rc = build_field_maps(x))) return bail(rc);
     if (cudaStreamSynchronize(x->stream) != cudaSuccess) {
         fail(x, ERTM_ECUDA, "%s", cudaGetErrorString(cudaGetLastError()));
         return bail(ERTM_ECUDA);
@@ -633,6 +784,7 @@ int ertm_destroy(ertm_ctx* c)
     cudaFree(c->wavelet);
     cudaFree(c->it_d);
     cudaFree(c->vmax_d);
+    cudaFree(c->err_d);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return ERTM_OK;
@@ -663,9 +815,13 @@ int ertm_set_model(ertm_ctx* c, int which, const float* vp, const float* vs, con
     if (!vp || !vs || !rho) return fail(c, ERTM_EINVAL, "NULL model array");
     CK(c, cudaSetDevice(c->device));
     int rc;
-    for (int q = 0; q < 5; q++)
-        if (!c->m_base[which][q] && (rc = alloc_volume(c, &c->m_base[which][q], &c->m[which][q])))
+    for (int q = 0; q < 5; q++) {
+        if (c->m_base[which][q]) continue;
+        if ((rc = alloc_volume(c, &c->m_base[which][q], &c->m[which][q]))) return rc;
+        if (q < 3 && (rc = encode_map(c, &c->mModel[which][q], c->m_base[which][q], false, TX,
+                                      c->g.tyb)))
             return rc;
+    }
     if ((rc = ensure_stage(c))) return rc;
     const long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
     const float* src[3] = {vp, vs, rho};
@@ -890,11 +1046,13 @@ int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
     for (int q = 0; q < 3; q++) CK(c, cudaEventCreate(&ev[q]));
     CK(c, launch_set_int(c->it_d, 0, c->stream));
     float tot[2] = {0.f, 0.f};
+    const StressMaps sm = stress_maps(c, 1);
+    const VelMaps vm = vel_maps(c, 1, EPI_EXCITE);
     for (int step = 0; step < nsteps; step++) {
         CK(c, cudaEventRecord(ev[0], c->stream));
-        CK(c, launch_stress(c->R, c->g, a, cpml, true, c->stream));
+        CK(c, launch_stress(c->R, c->g, a, sm, cpml, true, c->stream));
         CK(c, cudaEventRecord(ev[1], c->stream));
-        CK(c, launch_velocity(c->R, c->g, a, cpml, EPI_EXCITE, false, c->stream));
+        CK(c, launch_velocity(c->R, c->g, a, vm, cpml, EPI_EXCITE, false, c->stream));
         CK(c, cudaEventRecord(ev[2], c->stream));
         CK(c, launch_advance(c->it_d, 1, c->stream));
         c->launches += 3;
@@ -909,7 +1067,7 @@ int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
     c->have_excitation = false;
     ms[0] = tot[0];
     ms[1] = tot[1];
-    return ERTM_OK;
+    return check_device_error(c);
 }
 
 int64_t ertm_kernel_launches(const ertm_ctx* c) { return c ? c->launches : 0; }

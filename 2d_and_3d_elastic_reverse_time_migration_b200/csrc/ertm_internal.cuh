@@ -10,6 +10,7 @@
 // tile size are allocated too and stay zero.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -77,19 +78,48 @@ struct KArgs {
     float* ex_v[3];
     float* ex_tp;
     float* img[3];
+    int* err;                        // device error word (0 = ok)
 };
 
+// Device error codes written to KArgs::err
+enum DeviceError { DEV_OK = 0, DEV_WAIT_TIMEOUT = 1 };
+
+// TMA tensor maps of one step kernel, passed as a __grid_constant__ parameter.
+// Every map covers a whole padded volume [pz][py][px]; the box shape is fixed
+// per map: C = TX x TYB (centre), X = (TX+2XB) x TYB, Y = TX x (TYB+2R),
+// XY = (TX+2XB) x (TYB+2R), one plane deep.
+struct StressMaps {
+    CUtensorMap v[3];      // vx, vz, vy      (XY boxes; X in 2D)
+    CUtensorMap vc[3];     // vx, vz, vy      (C boxes: z-queue fronts)
+    CUtensorMap sig[6];    // txx tzz txz tyy txy tyz (C)
+    CUtensorMap tp;        // (C)
+    CUtensorMap M, MU;     // (C)
+};
+
+struct VelMaps {
+    CUtensorMap txx, txz;  // X boxes
+    CUtensorMap txy, tp;   // XY boxes (X in 2D)
+    CUtensorMap tyy, tyz;  // Y boxes
+    CUtensorMap c[8];      // C boxes: vx vz vy vxp vzp vyp b excitation(amp2 or time)
+    CUtensorMap fr[4];     // C boxes of txz tzz tyz tp: z-queue fronts
+};
+
+// x halo of the staged tiles: >= R and a multiple of 4 floats (16-byte TMA x start)
+constexpr int xb_of(int R) { return R <= 4 ? 4 : 8; }
+
 // Launchers (one translation unit per stencil radius).
-cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, bool cpml, bool psplit,
-                          cudaStream_t s);
-cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, bool cpml, int epi,
-                            bool record, cudaStream_t s);
-cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s);
-cudaError_t launch_stress_r6(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s);
-cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
-                               cudaStream_t s);
-cudaError_t launch_velocity_r6(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
-                               cudaStream_t s);
+cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,
+                          bool psplit, cudaStream_t s);
+cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, const VelMaps& m, bool cpml,
+                            int epi, bool record, cudaStream_t s);
+cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,
+                             bool psplit, cudaStream_t s);
+cudaError_t launch_stress_r6(const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,
+                             bool psplit, cudaStream_t s);
+cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, const VelMaps& m, bool cpml, int epi,
+                               bool record, cudaStream_t s);
+cudaError_t launch_velocity_r6(const Geom& g, const KArgs& a, const VelMaps& m, bool cpml, int epi,
+                               bool record, cudaStream_t s);
 
 // Small kernels (aux.cu)
 cudaError_t launch_scatter(const Geom& g, const float* src, float* dst, cudaStream_t s);

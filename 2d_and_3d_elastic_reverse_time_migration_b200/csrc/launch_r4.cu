@@ -3,15 +3,16 @@
 
 namespace ertm {
 
-cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, bool cpml, bool psplit, cudaStream_t s)
+cudaError_t launch_stress_r4(const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,
+                             bool psplit, cudaStream_t s)
 {
-    return launch_stress_t<4>(g, a, cpml, psplit, s);
+    return launch_stress_t<4>(g, a, m, cpml, psplit, s);
 }
 
-cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, bool cpml, int epi, bool record,
-                               cudaStream_t s)
+cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, const VelMaps& m, bool cpml, int epi,
+                               bool record, cudaStream_t s)
 {
-    return launch_velocity_t<4>(g, a, cpml, epi, record, s);
+    return launch_velocity_t<4>(g, a, m, cpml, epi, record, s);
 }
 
 }  // namespace ertm
