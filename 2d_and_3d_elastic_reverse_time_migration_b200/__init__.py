@@ -79,6 +79,8 @@ SIGNATURES = {
     "ertm_propagate": (C.c_int, [_P, C.c_int, C.POINTER(_Shot), C.c_int]),
     "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
     "ertm_kernel_launches": (C.c_int64, [_P]),
+    "ertm_forward_together_using_real_model_noalloc": (
+        C.c_int, [C.POINTER(_Config), _P, _P, _P, C.POINTER(_Shot), _P, _P, C.c_char_p, C.c_size_t]),
 }
 
 _lib_handle: C.CDLL | None = None
@@ -323,3 +325,23 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self._L.ertm_kernel_launches(self._h))
+
+
+def forward_together_using_real_model_noalloc(cfg: Config, vp, vs, rho, shot: Shot, out,
+                                              stream_ptr: int | None = None):
+    """Modelling pass that allocates no GPU memory (see include/ertm.h).
+
+    For callers that may not allocate device memory when they call in: every
+    array (vp, vs, rho, shot.wavelet, out of shape (3, nt, nrec)) must already be
+    a CUDA tensor; the library's wavefields live in a fixed 64 MiB device array.
+    Calls share that array, so calls that overlap on the GPU race."""
+    L = lib()
+    n = cfg.nx * cfg.ny * cfg.nz
+    cs, ss = cfg.struct(), shot.struct()
+    buf = C.create_string_buffer(512)
+    rc = L.ertm_forward_together_using_real_model_noalloc(
+        C.byref(cs), _ptr(vp, n), _ptr(vs, n), _ptr(rho, n), C.byref(ss),
+        _ptr(out, 3 * cfg.nt * shot.nrec), stream_ptr, buf, len(buf))
+    if rc != 0:
+        raise ErtmError(rc, buf.value.decode(errors="replace"))
+    return out

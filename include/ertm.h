@@ -175,6 +175,29 @@ int ertm_time_kernels(ertm_ctx *ctx, const ertm_shot *shot, int nsteps, float *m
 /* Number of kernels this context has launched (for launch accounting). */
 int64_t ertm_kernel_launches(const ertm_ctx *ctx);
 
+/* ---- modelling without device allocation ------------------------------
+ * No counterpart in the reference: an addition of this library.
+ *
+ * The same modelling pass as ertm_forward_together_using_real_model, for
+ * callers that must not allocate GPU memory when they call in (a plugin host
+ * whose execute step forbids it, a real-time pipeline whose memory is fixed at
+ * start-up, a framework whose own allocator owns the device).  No context is
+ * created and nothing is allocated: the caller passes device pointers for vp,
+ * vs, rho (nz*ny*nx), shot->wavelet and data_out ([3][nt][nrec]), and the
+ * wavefields live in one fixed 64 MiB device array inside the library, held by
+ * every GPU that loads it until the process exits.  A grid whose state does
+ * not fit returns ERTM_EINVAL with the needed size in errbuf.  The first call
+ * on a device looks up that array's address (make it before any stream capture
+ * on that device).  Calls share the array: calls that overlap on the GPU race,
+ * so serialise them; each call clears the state it uses.  Work is ordered on
+ * `cuda_stream` (NULL: the legacy default stream) and is complete on return.
+ * errbuf (may be NULL) receives a message on failure. */
+int ertm_forward_together_using_real_model_noalloc(const ertm_config *cfg, const float *vp,
+                                                   const float *vs, const float *rho,
+                                                   const ertm_shot *shot, float *data_out,
+                                                   void *cuda_stream, char *errbuf,
+                                                   size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
