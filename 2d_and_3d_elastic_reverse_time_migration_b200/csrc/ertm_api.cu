@@ -524,7 +524,7 @@ int choose_kchunk(const ertm_ctx* c)
     long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const long long slots = (long long)sms * (g.two_d ? 8 : 1);
+    const long long slots = (long long)sms * (g.two_d ? 8 : CTAS3);
     const double startup = 2.0 * c->R;
     int best = g.nz;
     double best_cost = 1e300;
@@ -595,12 +595,40 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
     }
     const StressMaps sm = stress_maps(c, which);
     const VelMaps vm = vel_maps(c, which, epi);
-    for (int step = 0; step < nsteps; step++) {
-        CK(c, launch_stress(R, c->g, a, sm, cpml, psplit, c->stream));
-        CK(c, launch_velocity(R, c->g, a, vm, cpml, epi, record, c->stream));
-        CK(c, launch_advance(c->it_d, dir, c->stream));
-        c->launches += 3;
+    auto one_step = [&]() -> cudaError_t {
+        cudaError_t e = launch_stress(R, c->g, a, sm, cpml, psplit, c->stream);
+        if (e == cudaSuccess) e = launch_velocity(R, c->g, a, vm, cpml, epi, record, c->stream);
+        if (e == cudaSuccess) e = launch_advance(c->it_d, dir, c->stream);
+        return e;
+    };
+    // The time loop runs as a CUDA graph of kGraphSteps steps replayed back to back
+    // (the kernels read the step index from device memory, so one graph serves every
+    // chunk); the first step and the remainder are launched directly.
+    constexpr int kGraphSteps = 32;
+    int done = 0;
+    if (nsteps > 0) {
+        CK(c, one_step());
+        done = 1;
     }
+    if (nsteps - done >= 2 * kGraphSteps) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int q = 0; q < kGraphSteps && e == cudaSuccess; q++) e = one_step();
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        while (e == cudaSuccess && nsteps - done >= kGraphSteps) {
+            e = cudaGraphLaunch(exec, c->stream);
+            done += kGraphSteps;
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "graph time loop: %s", cudaGetErrorString(e));
+    }
+    for (; done < nsteps; done++) CK(c, one_step());
+    c->launches += 3LL * nsteps;
     return check_device_error(c);
 }
 

@@ -404,7 +404,7 @@ int run_noalloc(const ertm_config* cfg, const float* vp, const float* vs, const 
         long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-        const long long slots = (long long)sms * (two_d ? 8 : 1);
+        const long long slots = (long long)sms * (two_d ? 8 : CTAS3);
         int best = g.nz;
         double best_cost = 1e300;
         for (int kc = g.nz; kc >= (g.nz < 16 ? g.nz : 16); kc--) {

@@ -163,7 +163,7 @@ struct StressShape {
 };
 
 template <int R, bool Y, bool CPML, bool PS>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), 1)
+__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), Y ? CTAS3 : 1)
 k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
 {
     using SS = StressShape<R, Y, CPML, PS>;
@@ -435,7 +435,7 @@ struct VelShape {
 };
 
 template <int R, bool Y, bool CPML, int EPI, bool REC>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), 1)
+__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), Y ? CTAS3 : 1)
 k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
 {
     using VS = VelShape<R, Y, CPML, EPI>;
