@@ -49,7 +49,7 @@ class _Config(C.Structure):
                 ("order", C.c_int), ("coef_kind", C.c_int), ("coef", C.c_float * 8),
                 ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_float),
                 ("pml_f0", C.c_float), ("pml_vmax", C.c_float), ("sponge_coef", C.c_float),
-                ("device", C.c_int), ("reserved", C.c_int * 7)]
+                ("device", C.c_int), ("checkpoint_every", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class _Shot(C.Structure):
@@ -79,6 +79,8 @@ SIGNATURES = {
     "ertm_propagate": (C.c_int, [_P, C.c_int, C.POINTER(_Shot), C.c_int]),
     "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
     "ertm_kernel_launches": (C.c_int64, [_P]),
+    "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_forward_together_using_real_model_noalloc": (
         C.c_int, [C.POINTER(_Config), _P, _P, _P, C.POINTER(_Shot), _P, _P, C.c_char_p, C.c_size_t]),
 }
@@ -123,11 +125,13 @@ class Config:
     pml_vmax: float = 0.0
     sponge_coef: float = 0.0
     device: int = 0
+    checkpoint_every: int = 0
 
     def struct(self) -> _Config:
         c = _Config()
         for f in ("nx", "ny", "nz", "dx", "dy", "dz", "dt_ms", "nt", "src_steps", "order",
-                  "coef_kind", "boundary", "pml_r", "pml_f0", "pml_vmax", "sponge_coef", "device"):
+                  "coef_kind", "boundary", "pml_r", "pml_f0", "pml_vmax", "sponge_coef", "device",
+                  "checkpoint_every"):
             setattr(c, f, getattr(self, f))
         for i, v in enumerate(self.coef[:8]):
             c.coef[i] = v
@@ -321,6 +325,27 @@ class Context:
         s = shot.struct()
         self._ck(self._L.ertm_time_kernels(self._h, C.byref(s), nsteps, ms))
         return float(ms[0]), float(ms[1])
+
+    def born_forward(self, shot: Shot, r_vp, r_vs, r_rho, out=None):
+        """Linearised data (3, nt, nrec) for relative perturbations of the migration model."""
+        n = self.ncell
+        if out is None:
+            out = np.zeros((3, self.cfg.nt, shot.nrec), np.float32)
+        args = [a if _is_torch(a) else np.ascontiguousarray(a, np.float32) for a in (r_vp, r_vs, r_rho)]
+        s = shot.struct()
+        self._ck(self._L.ertm_born_forward(self._h, C.byref(s), *[_ptr(a, n) for a in args],
+                                           _ptr(out, 3 * self.cfg.nt * shot.nrec, True)))
+        return out
+
+    def born_adjoint(self, shot: Shot, residual, g_vp=None, g_vs=None, g_rho=None):
+        """Transpose of born_forward applied to residual (3, nt, nrec): (g_vp, g_vs, g_rho)."""
+        n = self.ncell
+        outs = [self._vol(o) for o in (g_vp, g_vs, g_rho)]
+        r = residual if _is_torch(residual) else np.ascontiguousarray(residual, np.float32)
+        s = shot.struct()
+        self._ck(self._L.ertm_born_adjoint(self._h, C.byref(s), _ptr(r, 3 * self.cfg.nt * shot.nrec),
+                                           *[_ptr(o, n, True) for o in outs]))
+        return tuple(outs)
 
     @property
     def kernel_launches(self) -> int:

@@ -1,0 +1,40 @@
+// Born modelling / adjoint kernels (2D, sponge boundaries): argument block and launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ertm {
+
+constexpr int BXH = 8;   // x halo of the compact 2D layout (floats)
+
+struct BornArgs {
+    int nx, nz, R;
+    long long px;                          // row pitch; cell (i,k) at (k+R)*px + i + BXH
+    float cx[8], cz[8];                    // c_n / h
+    float dt;
+    const float *M, *U, *L, *B, *g1, *g2;  // model products and damping factors
+    float *v0x, *v0z, *s0xx, *s0zz, *s0xz; // background state
+    float *vx, *vz, *sxx, *szz, *sxz;      // scattered state
+    const float *dM, *dU, *rr;             // perturbation products
+    float *ax, *az, *hxx, *hzz, *hxz;      // adjoint state
+    float *gM, *gL, *gU, *gR;              // gradient accumulators
+    const float *hv0x, *hv0z, *ha0x, *ha0z;// background history read by the adjoint step
+    float *kv0x, *kv0z, *ka0x, *ka0z;      // history slot written by a recording step
+    int ssx, ssz, nw;
+    const float* wavelet;
+    int rx0, nrx, drx, rz;
+    float* traces;                         // [3][nt][nrx]: recorded (forward) or residual (adjoint)
+    int nt;
+};
+
+cudaError_t born_launch_model(const BornArgs& a, const float* Mc, const float* Uc, const float* Bc,
+                              long long csz, const float* att_x, const float* att_z, float* M,
+                              float* U, float* L, float* B, float* g1, float* g2, cudaStream_t s);
+cudaError_t born_launch_pert(const BornArgs& a, const float* rvp, const float* rvs,
+                             const float* rrho, float* dM, float* dU, float* rr, cudaStream_t s);
+cudaError_t born_launch_step(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s);
+cudaError_t born_launch_adjoint_step(const BornArgs& a, int it, cudaStream_t s);
+cudaError_t born_launch_inject(const BornArgs& a, int it, cudaStream_t s);
+cudaError_t born_launch_final(const BornArgs& a, float* gvp, float* gvs, float* grho, cudaStream_t s);
+
+}  // namespace ertm

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "ertm.h"
+#include "born.cuh"
 #include "ertm_internal.cuh"
 
 using namespace ertm;
@@ -88,6 +89,18 @@ struct ertm_ctx {
 
     std::string err;
     long long launches = 0;
+
+    // Born / adjoint state (2D, compact layout; allocated on first use)
+    struct BornState {
+        bool ready = false;
+        long long px = 0, n = 0;          // pitch and floats per compact volume
+        float* block = nullptr;           // one allocation holding every compact volume
+        float* vol[30] = {nullptr};       // M U L B g1 g2 | bg 5 | sc 5 | dM dU rr | adj 5 | grad 4
+        float* ckpt = nullptr;            // checkpoints: nck x 5 volumes
+        int nck = 0;
+        float* hist = nullptr;            // history: K x 4 volumes
+        int K = 0;
+    } born;
 };
 
 namespace {
@@ -687,8 +700,9 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     }
     if (c.src_steps < 0 || c.src_steps > c.nt)
         return fail(nullptr, ERTM_EINVAL, "src_steps %d outside [0, nt]", c.src_steps);
-    for (int q = 0; q < 7; q++)
+    for (int q = 0; q < 6; q++)
         if (c.reserved[q]) return fail(nullptr, ERTM_EINVAL, "reserved fields must be zero");
+    if (c.checkpoint_every < 0) return fail(nullptr, ERTM_EINVAL, "checkpoint_every < 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -813,6 +827,9 @@ int ertm_destroy(ertm_ctx* c)
     cudaFree(c->it_d);
     cudaFree(c->vmax_d);
     cudaFree(c->err_d);
+    cudaFree(c->born.block);
+    cudaFree(c->born.ckpt);
+    cudaFree(c->born.hist);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return ERTM_OK;
@@ -1099,5 +1116,231 @@ int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
 }
 
 int64_t ertm_kernel_launches(const ertm_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Born modelling and adjoint (2D, sponge boundaries)
+// ---------------------------------------------------------------------------
+namespace {
+
+enum { BV_M, BV_U, BV_L, BV_B, BV_G1, BV_G2, BV_BG, BV_SC = BV_BG + 5, BV_DM = BV_SC + 5, BV_DU,
+       BV_RR, BV_ADJ, BV_GRAD = BV_ADJ + 5, BV_N = BV_GRAD + 4 };
+
+int born_check(ertm_ctx* c, const ertm_shot* s)
+{
+    if (!c->g.two_d) return fail(c, ERTM_ENOTSUP, "Born operators: 2D grids only in this build");
+    if (c->cfg.boundary == ERTM_BOUNDARY_CPML)
+        return fail(c, ERTM_ENOTSUP, "Born operators: sponge boundaries only in this build");
+    if (!c->model_set[1]) return fail(c, ERTM_ESTATE, "migration model not set");
+    int rc = validate_shot(c, s, true);
+    if (rc) return rc;
+    return ERTM_OK;
+}
+
+// arguments over the compact layout; model products copied from the migration model
+int born_prepare(ertm_ctx* c, BornArgs& a)
+{
+    auto& B = c->born;
+    const Geom& g = c->g;
+    int rc;
+    if (!B.ready) {
+        B.px = round_up(2LL * BXH + round_up(g.nx, 32), 32);
+        B.n = B.px * (g.nz + 2LL * c->R);
+        // one block so that consecutive volumes (the 5 background fields of a
+        // checkpoint) are contiguous
+        CK(c, cudaMalloc(&B.block, sizeof(float) * B.n * BV_N));
+        CK(c, cudaMemsetAsync(B.block, 0, sizeof(float) * B.n * BV_N, c->stream));
+        for (int q = 0; q < BV_N; q++) B.vol[q] = B.block + (size_t)q * B.n;
+        B.ready = true;
+    }
+    if ((rc = upload_profiles(c, 0.f))) return rc;
+    std::memset(&a, 0, sizeof a);
+    a.nx = g.nx;
+    a.nz = g.nz;
+    a.R = c->R;
+    a.px = B.px;
+    for (int q = 0; q < 8; q++) {
+        a.cx[q] = (float)(c->coef[q] / c->cfg.dx);
+        a.cz[q] = (float)(c->coef[q] / c->cfg.dz);
+    }
+    a.dt = c->cfg.dt_ms / 1000.f;
+    a.M = B.vol[BV_M]; a.U = B.vol[BV_U]; a.L = B.vol[BV_L]; a.B = B.vol[BV_B];
+    a.g1 = B.vol[BV_G1]; a.g2 = B.vol[BV_G2];
+    float** bg[5] = {&a.v0x, &a.v0z, &a.s0xx, &a.s0zz, &a.s0xz};
+    float** sc[5] = {&a.vx, &a.vz, &a.sxx, &a.szz, &a.sxz};
+    float** ad[5] = {&a.ax, &a.az, &a.hxx, &a.hzz, &a.hxz};
+    for (int q = 0; q < 5; q++) {
+        *bg[q] = B.vol[BV_BG + q];
+        *sc[q] = B.vol[BV_SC + q];
+        *ad[q] = B.vol[BV_ADJ + q];
+    }
+    a.dM = B.vol[BV_DM]; a.dU = B.vol[BV_DU]; a.rr = B.vol[BV_RR];
+    a.gM = B.vol[BV_GRAD]; a.gL = B.vol[BV_GRAD + 1]; a.gU = B.vol[BV_GRAD + 2];
+    a.gR = B.vol[BV_GRAD + 3];
+    a.nt = c->cfg.nt;
+    CK(c, born_launch_model(a, c->m[1][0], c->m[1][1], c->m[1][2], g.sz, c->att[0], c->att[2],
+                            B.vol[BV_M], B.vol[BV_U], B.vol[BV_L], B.vol[BV_B], B.vol[BV_G1],
+                            B.vol[BV_G2], c->stream));
+    c->launches++;
+    return ERTM_OK;
+}
+
+void born_shot(BornArgs& a, const ertm_shot* s, const float* wav)
+{
+    a.ssx = s->sx;
+    a.ssz = s->sz;
+    a.nw = s->nw;
+    a.wavelet = wav;
+    a.rx0 = s->rx0;
+    a.nrx = s->nrx;
+    a.drx = s->drx;
+    a.rz = s->rz;
+}
+
+int born_zero(ertm_ctx* c, int first, int count)
+{
+    for (int q = first; q < first + count; q++)
+        CK(c, cudaMemsetAsync(c->born.vol[q], 0, sizeof(float) * c->born.n, c->stream));
+    return ERTM_OK;
+}
+
+// contiguous nz*nx device copies of up to three caller arrays (stage)
+int born_stage_in(ertm_ctx* c, const float* const* src, int count, const float** out)
+{
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    const long long n = (long long)c->g.nx * c->g.nz;
+    for (int q = 0; q < count; q++) {
+        if (is_device_ptr(src[q])) {
+            out[q] = src[q];
+            continue;
+        }
+        CK(c, cudaMemcpyAsync(c->stage + q * n, src[q], sizeof(float) * n, cudaMemcpyHostToDevice,
+                              c->stream));
+        out[q] = c->stage + q * n;
+    }
+    return ERTM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ertm_born_forward(ertm_ctx* c, const ertm_shot* s, const float* r_vp, const float* r_vs,
+                      const float* r_rho, float* data_out)
+{
+    if (!c) return ERTM_EINVAL;
+    if (!r_vp || !r_vs || !r_rho || !data_out) return fail(c, ERTM_EINVAL, "NULL argument");
+    CK(c, cudaSetDevice(c->device));
+    int rc = born_check(c, s);
+    if (rc) return rc;
+    BornArgs a;
+    if ((rc = born_prepare(c, a))) return rc;
+    if ((rc = upload_wavelet(c, s))) return rc;
+    born_shot(a, s, c->wavelet);
+    const float* src[3] = {r_vp, r_vs, r_rho};
+    const float* dev[3];
+    if ((rc = born_stage_in(c, src, 3, dev))) return rc;
+    CK(c, born_launch_pert(a, dev[0], dev[1], dev[2], c->born.vol[BV_DM], c->born.vol[BV_DU],
+                           c->born.vol[BV_RR], c->stream));
+    if ((rc = born_zero(c, BV_BG, 10))) return rc;
+    const size_t nd = 3 * (size_t)c->cfg.nt * s->nrx;
+    const bool dev_out = is_device_ptr(data_out);
+    if (!dev_out && (rc = ensure_traces(c, nd))) return rc;
+    a.traces = dev_out ? data_out : c->traces;
+    CK(c, cudaMemsetAsync(a.traces, 0, sizeof(float) * nd, c->stream));
+    for (int it = 0; it < c->cfg.nt; it++) CK(c, born_launch_step(a, it, true, false, c->stream));
+    c->launches += 1 + 2LL * c->cfg.nt;
+    if (!dev_out)
+        CK(c, cudaMemcpyAsync(data_out, a.traces, sizeof(float) * nd, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
+
+int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, float* g_vp,
+                      float* g_vs, float* g_rho)
+{
+    if (!c) return ERTM_EINVAL;
+    if (!residual || !g_vp || !g_vs || !g_rho) return fail(c, ERTM_EINVAL, "NULL argument");
+    CK(c, cudaSetDevice(c->device));
+    int rc = born_check(c, s);
+    if (rc) return rc;
+    BornArgs a;
+    if ((rc = born_prepare(c, a))) return rc;
+    if ((rc = upload_wavelet(c, s))) return rc;
+    born_shot(a, s, c->wavelet);
+    auto& B = c->born;
+    const int nt = c->cfg.nt;
+    const int K = std::min(nt, c->cfg.checkpoint_every > 0 ? c->cfg.checkpoint_every : 200);
+    const int nck = (nt + K - 1) / K;
+    if (B.nck < nck) {
+        cudaFree(B.ckpt);
+        B.ckpt = nullptr;
+        CK(c, cudaMalloc(&B.ckpt, sizeof(float) * 5 * B.n * nck));
+        B.nck = nck;
+    }
+    if (B.K < K) {
+        cudaFree(B.hist);
+        B.hist = nullptr;
+        CK(c, cudaMalloc(&B.hist, sizeof(float) * 4 * B.n * K));
+        B.K = K;
+    }
+    // residual on the device
+    const size_t nd = 3 * (size_t)nt * s->nrx;
+    if (is_device_ptr(residual)) a.traces = const_cast<float*>(residual);
+    else {
+        if ((rc = ensure_traces(c, nd))) return rc;
+        CK(c, cudaMemcpyAsync(c->traces, residual, sizeof(float) * nd, cudaMemcpyHostToDevice, c->stream));
+        a.traces = c->traces;
+    }
+    // 1. background forward, checkpointing its state every K steps
+    if ((rc = born_zero(c, BV_BG, 5))) return rc;
+    for (int it = 0; it < nt; it++) {
+        if (it % K == 0)
+            CK(c, cudaMemcpyAsync(B.ckpt + (size_t)(it / K) * 5 * B.n, B.vol[BV_BG],
+                                  sizeof(float) * 5 * B.n, cudaMemcpyDeviceToDevice, c->stream));
+        CK(c, born_launch_step(a, it, false, false, c->stream));
+    }
+    // 2. reverse sweep, one checkpoint segment at a time
+    if ((rc = born_zero(c, BV_ADJ, 9))) return rc;
+    CK(c, born_launch_inject(a, nt - 1, c->stream));
+    for (int sg = nck - 1; sg >= 0; sg--) {
+        const int t0 = sg * K, t1 = std::min(nt, t0 + K);
+        CK(c, cudaMemcpyAsync(B.vol[BV_BG], B.ckpt + (size_t)sg * 5 * B.n, sizeof(float) * 5 * B.n,
+                              cudaMemcpyDeviceToDevice, c->stream));
+        for (int it = t0; it < t1; it++) {
+            float* h = B.hist + (size_t)(it - t0) * 4 * B.n;
+            a.kv0x = h;
+            a.kv0z = h + B.n;
+            a.ka0x = h + 2 * B.n;
+            a.ka0z = h + 3 * B.n;
+            CK(c, born_launch_step(a, it, false, true, c->stream));
+        }
+        for (int it = t1 - 1; it >= t0; it--) {
+            const float* h = B.hist + (size_t)(it - t0) * 4 * B.n;
+            a.hv0x = h;
+            a.hv0z = h + B.n;
+            a.ha0x = h + 2 * B.n;
+            a.ha0z = h + 3 * B.n;
+            CK(c, born_launch_adjoint_step(a, it, c->stream));
+        }
+    }
+    c->launches += 2LL * nt * 2 + 2LL * nt + 2;
+    // 3. gradients w.r.t. the relative perturbations
+    float* outs[3] = {g_vp, g_vs, g_rho};
+    const long long n = (long long)c->g.nx * c->g.nz;
+    bool dev[3];
+    for (int q = 0; q < 3; q++) dev[q] = is_device_ptr(outs[q]);
+    if (!(dev[0] && dev[1] && dev[2]) && (rc = ensure_stage(c))) return rc;
+    float* tgt[3];
+    for (int q = 0; q < 3; q++) tgt[q] = dev[q] ? outs[q] : c->stage + q * n;
+    CK(c, born_launch_final(a, tgt[0], tgt[1], tgt[2], c->stream));
+    for (int q = 0; q < 3; q++)
+        if (!dev[q])
+            CK(c, cudaMemcpyAsync(outs[q], tgt[q], sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return ERTM_OK;
+}
 
 }  // extern "C"

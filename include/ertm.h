@@ -93,7 +93,8 @@ typedef struct {
     float pml_vmax;          /* CPML velocity; 0 -> max Vp of the model */
     float sponge_coef;       /* reference coe_attenuation (sponge kinds) */
     int   device;            /* CUDA device ordinal */
-    int   reserved[7];       /* must be zero */
+    int   checkpoint_every;  /* Born adjoint: background checkpoint interval; 0 -> 200 */
+    int   reserved[6];       /* must be zero */
 } ertm_config;
 
 typedef struct {
@@ -146,6 +147,24 @@ int ertm_backward_together_using_smoothed_model(ertm_ctx *ctx, const ertm_shot *
 /* Source pass then receiver pass: one RTM shot. */
 int ertm_rtm_shot(ertm_ctx *ctx, const ertm_shot *shot, const float *data_in,
                   float *img_pp, float *img_ps, float *img_tp);
+
+/* ---- least-squares RTM operators (2D, sponge boundaries) ---------------
+ * The linearised (Born) modelling of the reference's LSRTM
+ * (demig_fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization and
+ * cuda_cal_dem_parameter_viscoelastic_media_new, 2D_elastic_RTM/viscoelastic_equation.cu
+ * :328-477, :2398-2505, inversion_para 2, elastic case) and its exact adjoint
+ * (the role of adjoint_fwd_vx/vz_viscoelastic, adjoint_fwd_memory_new and
+ * cal_gradient_in_viscoelastic_media_new, :1827-2294), in the migration model.
+ * Perturbations are relative: r_vp = dvp/vp, r_vs = dvs/vs, r_rho = drho/rho
+ * (nz*ny*nx each).  data/residual are [3][nt][nrec] (vx, 0, vz).  The adjoint
+ * returns F^T residual, i.e. the gradient of 0.5 |F r - d|^2 when the residual
+ * is F r - d; its background wavefield is rebuilt from checkpoints every
+ * cfg.checkpoint_every steps (no full wavefield history is kept).
+ * 2D grids with a sponge boundary only (ERTM_ENOTSUP otherwise). */
+int ertm_born_forward(ertm_ctx *ctx, const ertm_shot *shot, const float *r_vp,
+                      const float *r_vs, const float *r_rho, float *data_out);
+int ertm_born_adjoint(ertm_ctx *ctx, const ertm_shot *shot, const float *residual,
+                      float *g_vp, float *g_vs, float *g_rho);
 
 /* ---- inspection (the reference's output_3d_wavefiled_* / EA outputs,
  *      3D_output_file.cu:2-250) ------------------------------------------ */

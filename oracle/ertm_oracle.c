@@ -647,3 +647,254 @@ int orc_divcurl(const orc_grid *g, const float *vp, const float *vs,
     free(X); free(Y); free(Z); free(VS);
     return 0;
 }
+
+/* ----------------------------------------------------------------------
+ * Born modelling and its exact adjoint (2D, sponge boundaries)
+ * -------------------------------------------------------------------- */
+typedef struct {
+    int nx, nz, R;
+    long px, pz, n;            /* padded extents (R halo on every side) */
+    real c[8], dt, ix, iz;
+    real *M, *U, *L, *B, *g1, *g2;
+} born2d;
+
+#define B2(S, i, k) (((long)(k) + (S)->R) * (S)->px + (i) + (S)->R)
+
+static int born_setup(born2d *S, const orc_grid *g, const float *vp, const float *vs,
+                      const float *rho)
+{
+    if (g->ny != 1 || g->boundary == ORC_BOUNDARY_CPML) return -1;
+    memset(S, 0, sizeof *S);
+    S->nx = g->nx; S->nz = g->nz; S->R = g->R;
+    S->px = g->nx + 2L * g->R; S->pz = g->nz + 2L * g->R; S->n = S->px * S->pz;
+    for (int q = 0; q <= g->R; q++) S->c[q] = (real)g->coef[q];
+    S->dt = (real)(g->dt_ms / 1000.0);
+    S->ix = (real)(1.0 / g->dx); S->iz = (real)(1.0 / g->dz);
+    real **arr[6] = {&S->M, &S->U, &S->L, &S->B, &S->g1, &S->g2};
+    for (int q = 0; q < 6; q++) if (!(*arr[q] = zalloc(S->n))) return -2;
+    double *px = (double *)malloc(sizeof(double) * g->nx), *pz = (double *)malloc(sizeof(double) * g->nz);
+    if (!px || !pz) { free(px); free(pz); return -2; }
+    orc_sponge_profile(g->boundary, g->nx, g->pml[0], g->pml[1], g->sponge_coef, px);
+    orc_sponge_profile(g->boundary, g->nz, g->pml[4], g->pml[5], g->sponge_coef, pz);
+    for (int k = 0; k < g->nz; k++)
+        for (int i = 0; i < g->nx; i++) {
+            long c = B2(S, i, k), m = (long)k * g->nx + i;
+            real r = rho[m], p = vp[m], s = vs[m];
+            S->M[c] = r * p * p; S->U[c] = r * s * s; S->L[c] = S->M[c] - 2 * S->U[c]; S->B[c] = 1 / r;
+            real a = (real)((float)pz[k] + (float)px[i]) * S->dt / 2;
+            S->g1[c] = 1 / (1 + a); S->g2[c] = 1 - a;
+        }
+    free(px); free(pz);
+    return 0;
+}
+
+static void born_free(born2d *S)
+{
+    free(S->M); free(S->U); free(S->L); free(S->B); free(S->g1); free(S->g2);
+}
+
+static real b_dpx(const born2d *S, const real *f, long c) { return dplus(f, c, 1, S->c, S->R) * S->ix; }
+static real b_dmx(const born2d *S, const real *f, long c) { return dminus(f, c, 1, S->c, S->R) * S->ix; }
+static real b_dpz(const born2d *S, const real *f, long c) { return dplus(f, c, S->px, S->c, S->R) * S->iz; }
+static real b_dmz(const born2d *S, const real *f, long c) { return dminus(f, c, S->px, S->c, S->R) * S->iz; }
+
+/* one step of background (+ scattered when dM != NULL); stores v0 (start of
+ * step) and a0 into keep[4] when keep != NULL */
+static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, real *v0z, real *s0xx,
+                      real *s0zz, real *s0xz, real *vx, real *vz, real *sxx, real *szz, real *sxz,
+                      const real *dM, const real *dU, const real *rr, real **keep)
+{
+    const real dt = S->dt;
+    if (it < s->nw) {
+        long c = B2(S, s->sx, s->sz);
+        s0xx[c] += s->wavelet[it];
+        s0zz[c] += s->wavelet[it];
+    }
+    if (keep) {
+        memcpy(keep[0], v0x, sizeof(real) * S->n);
+        memcpy(keep[1], v0z, sizeof(real) * S->n);
+    }
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < S->nz; k++)
+        for (int i = 0; i < S->nx; i++) {
+            long c = B2(S, i, k);
+            real e0xx = b_dpx(S, v0x, c), e0zz = b_dmz(S, v0z, c);
+            real e0xz = b_dpz(S, v0x, c) + b_dmx(S, v0z, c);
+            real g1 = S->g1[c], g2 = S->g2[c], M = S->M[c], L = S->L[c], U = S->U[c];
+            s0xx[c] = g1 * (g2 * s0xx[c] + dt * (M * e0xx + L * e0zz));
+            s0zz[c] = g1 * (g2 * s0zz[c] + dt * (M * e0zz + L * e0xx));
+            s0xz[c] = g1 * (g2 * s0xz[c] + dt * U * e0xz);
+            if (dM) {
+                real exx = b_dpx(S, vx, c), ezz = b_dmz(S, vz, c);
+                real exz = b_dpz(S, vx, c) + b_dmx(S, vz, c);
+                real dm = dM[c], du = dU[c], dl = dm - 2 * du;
+                sxx[c] = g1 * (g2 * sxx[c] + dt * (M * exx + L * ezz + dm * e0xx + dl * e0zz));
+                szz[c] = g1 * (g2 * szz[c] + dt * (M * ezz + L * exx + dm * e0zz + dl * e0xx));
+                sxz[c] = g1 * (g2 * sxz[c] + dt * (U * exz + du * e0xz));
+            }
+        }
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < S->nz; k++)
+        for (int i = 0; i < S->nx; i++) {
+            long c = B2(S, i, k);
+            real g1 = S->g1[c], g2 = S->g2[c], b = S->B[c];
+            real a0x = b * (b_dmx(S, s0xx, c) + b_dmz(S, s0xz, c));
+            real a0z = b * (b_dpx(S, s0xz, c) + b_dpz(S, s0zz, c));
+            if (keep) { keep[2][c] = a0x; keep[3][c] = a0z; }
+            v0x[c] = g1 * (g2 * v0x[c] + dt * a0x);
+            v0z[c] = g1 * (g2 * v0z[c] + dt * a0z);
+            if (dM) {
+                real ax = b * (b_dmx(S, sxx, c) + b_dmz(S, sxz, c));
+                real az = b * (b_dpx(S, sxz, c) + b_dpz(S, szz, c));
+                vx[c] = g1 * (g2 * vx[c] + dt * (ax - rr[c] * a0x));
+                vz[c] = g1 * (g2 * vz[c] + dt * (az - rr[c] * a0z));
+            }
+        }
+}
+
+static int born_rec(const born2d *S, const orc_shot *s, int r, long *c)
+{
+    int irx = r % s->nrx, i = s->rx0 + irx * s->drx;
+    if (i < 0 || i >= S->nx || s->rz < 0 || s->rz >= S->nz) return 0;
+    *c = B2(S, i, s->rz);
+    return 1;
+}
+
+int orc_born_forward(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                     const orc_shot *s, int nt, const float *r_vp, const float *r_vs,
+                     const float *r_rho, float *data)
+{
+    born2d S;
+    if (!s || !data || nt < 1 || s->nry != 1) return -1;
+    int rc = born_setup(&S, g, vp, vs, rho);
+    if (rc) { born_free(&S); return rc; }
+    real *f[13];
+    for (int q = 0; q < 13; q++) if (!(f[q] = zalloc(S.n))) { rc = -2; }
+    if (!rc) {
+        real *dM = f[10], *dU = f[11], *rr = f[12];
+        for (int k = 0; k < S.nz; k++)
+            for (int i = 0; i < S.nx; i++) {
+                long c = B2(&S, i, k), m = (long)k * S.nx + i;
+                dM[c] = S.M[c] * ((real)r_rho[m] + 2 * (real)r_vp[m]);
+                dU[c] = S.U[c] * ((real)r_rho[m] + 2 * (real)r_vs[m]);
+                rr[c] = r_rho[m];
+            }
+        const long nrec = s->nrx;
+        memset(data, 0, sizeof(float) * 3 * (size_t)nt * nrec);
+        for (int it = 0; it < nt; it++) {
+            born_step(&S, s, it, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], dM, dU,
+                      rr, NULL);
+            for (long r = 0; r < nrec; r++) {
+                long c;
+                if (!born_rec(&S, s, (int)r, &c)) continue;
+                data[((long)0 * nt + it) * nrec + r] = (float)f[5][c];
+                data[((long)2 * nt + it) * nrec + r] = (float)f[6][c];
+            }
+        }
+    }
+    for (int q = 0; q < 13; q++) free(f[q]);
+    born_free(&S);
+    return rc;
+}
+
+int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                     const orc_shot *s, int nt, const float *residual, float *g_vp, float *g_vs,
+                     float *g_rho)
+{
+    born2d S;
+    if (!s || !residual || nt < 1 || s->nry != 1) return -1;
+    int rc = born_setup(&S, g, vp, vs, rho);
+    if (rc) { born_free(&S); return rc; }
+    const long n = S.n;
+    /* background history: v0 at the start of every step and a0 of every step */
+    real *hist = (real *)malloc(sizeof(real) * (size_t)4 * n * nt);
+    real *w[16];
+    for (int q = 0; q < 16; q++) w[q] = zalloc(n);
+    for (int q = 0; q < 16; q++) if (!w[q]) rc = -2;
+    if (!hist) rc = -2;
+    if (!rc) {
+        real *v0x = w[0], *v0z = w[1], *s0xx = w[2], *s0zz = w[3], *s0xz = w[4];
+        for (int it = 0; it < nt; it++) {
+            real *keep[4] = {hist + (4L * it + 0) * n, hist + (4L * it + 1) * n,
+                             hist + (4L * it + 2) * n, hist + (4L * it + 3) * n};
+            born_step(&S, s, it, v0x, v0z, s0xx, s0zz, s0xz, NULL, NULL, NULL, NULL, NULL, NULL,
+                      NULL, NULL, keep);
+        }
+        real *ax = w[5], *az = w[6], *hxx = w[7], *hzz = w[8], *hxz = w[9];
+        real *gM = w[10], *gL = w[11], *gU = w[12], *gR = w[13], *tx = w[14], *tz = w[15];
+        for (long q = 0; q < n; q++) ax[q] = az[q] = hxx[q] = hzz[q] = hxz[q] = 0;
+        const long nrec = s->nrx;
+        const real dt = S.dt;
+        real *Qxx = (real *)calloc(n, sizeof(real)), *Qzz = (real *)calloc(n, sizeof(real));
+        real *Qxz = (real *)calloc(n, sizeof(real));
+        for (int it = nt - 1; it >= 0; it--) {
+            const real *hv0x = hist + (4L * it + 0) * n, *hv0z = hist + (4L * it + 1) * n;
+            const real *ha0x = hist + (4L * it + 2) * n, *ha0z = hist + (4L * it + 3) * n;
+            for (long r = 0; r < nrec; r++) {          /* record^T */
+                long c;
+                if (!born_rec(&S, s, (int)r, &c)) continue;
+                ax[c] += residual[((long)0 * nt + it) * nrec + r];
+                az[c] += residual[((long)2 * nt + it) * nrec + r];
+            }
+            /* velocity update^T */
+            for (long q = 0; q < n; q++) {
+                tx[q] = S.B[q] * S.g1[q] * ax[q];
+                tz[q] = S.B[q] * S.g1[q] * az[q];
+            }
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < S.nz; k++)
+                for (int i = 0; i < S.nx; i++) {
+                    long c = B2(&S, i, k);
+                    real g1 = S.g1[c];
+                    gR[c] += -dt * (g1 * ax[c] * ha0x[c] + g1 * az[c] * ha0z[c]);
+                    hxx[c] += -dt * b_dpx(&S, tx, c);
+                    hxz[c] += -dt * (b_dpz(&S, tx, c) + b_dmx(&S, tz, c));
+                    hzz[c] += -dt * b_dmz(&S, tz, c);
+                }
+            /* stress update^T */
+            for (long q = 0; q < n; q++) {
+                real g1 = S.g1[q];
+                Qxx[q] = g1 * hxx[q]; Qzz[q] = g1 * hzz[q]; Qxz[q] = g1 * hxz[q];
+                tx[q] = S.M[q] * Qxx[q] + S.L[q] * Qzz[q];     /* reused as M Qxx + L Qzz */
+                tz[q] = S.L[q] * Qxx[q] + S.M[q] * Qzz[q];     /* L Qxx + M Qzz */
+            }
+            real *uq = hxx;                                    /* U Qxz, written after use */
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < S.nz; k++)
+                for (int i = 0; i < S.nx; i++) {
+                    long c = B2(&S, i, k);
+                    real e0xx = b_dpx(&S, hv0x, c), e0zz = b_dmz(&S, hv0z, c);
+                    real e0xz = b_dpz(&S, hv0x, c) + b_dmx(&S, hv0z, c);
+                    gM[c] += dt * (Qxx[c] * e0xx + Qzz[c] * e0zz);
+                    gL[c] += dt * (Qxx[c] * e0zz + Qzz[c] * e0xx);
+                    gU[c] += dt * Qxz[c] * e0xz;
+                }
+            for (long q = 0; q < n; q++) uq[q] = S.U[q] * Qxz[q];
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < S.nz; k++)
+                for (int i = 0; i < S.nx; i++) {
+                    long c = B2(&S, i, k);
+                    real g12 = S.g2[c] * S.g1[c];
+                    ax[c] = g12 * ax[c] - dt * (b_dmx(&S, tx, c) + b_dmz(&S, uq, c));
+                    az[c] = g12 * az[c] - dt * (b_dpz(&S, tz, c) + b_dpx(&S, uq, c));
+                }
+            for (long q = 0; q < n; q++) {
+                real g2 = S.g2[q];
+                hxx[q] = g2 * Qxx[q]; hzz[q] = g2 * Qzz[q]; hxz[q] = g2 * Qxz[q];
+            }
+        }
+        for (int k = 0; k < S.nz; k++)
+            for (int i = 0; i < S.nx; i++) {
+                long c = B2(&S, i, k), m = (long)k * S.nx + i;
+                real gm = gM[c] + gL[c], gu = gU[c] - 2 * gL[c];
+                g_vp[m] = (float)(2 * S.M[c] * gm);
+                g_vs[m] = (float)(2 * S.U[c] * gu);
+                g_rho[m] = (float)(S.M[c] * gm + S.U[c] * gu + gR[c]);
+            }
+        free(Qxx); free(Qzz); free(Qxz);
+    }
+    for (int q = 0; q < 16; q++) free(w[q]);
+    free(hist);
+    born_free(&S);
+    return rc;
+}

@@ -107,6 +107,27 @@ int orc_divcurl(const orc_grid *g, const float *vp, const float *vs,
                 const float *vx, const float *vy, const float *vz,
                 float *p, float *sx, float *sy, float *sz);
 
+/* ---- Born modelling and its adjoint (2D, sponge boundaries) ----------
+ * Linearised (first-order scattering) modelling for relative perturbations
+ * r_vp, r_vs, r_rho of the model (vp, vs, rho): the scattered field obeys the
+ * background scheme with secondary sources
+ *   stress  : dt (dM e0_xx + dL e0_zz, dL e0_xx + dM e0_zz, dU e0_xz)
+ *   velocity: -dt r_rho a0
+ * with dM = M (r_rho + 2 r_vp), dU = U (r_rho + 2 r_vs), dL = dM - 2 dU, e0 the
+ * background strain rates and a0 = b div(sigma0) the background acceleration —
+ * the reference's secondary sources (cuda_cal_dem_parameter_viscoelastic_media_new,
+ * 2D_elastic_RTM/viscoelastic_equation.cu:2398-2505, inversion_para 2) without
+ * attenuation.  This is the exact derivative of orc_run_pass's discrete scheme.
+ * born_forward records vx, vz of the scattered field into data[3][nt][nrec].
+ * born_adjoint applies the exact transpose of born_forward to `residual`
+ * ([3][nt][nrec]) and returns the gradients w.r.t. r_vp, r_vs, r_rho. */
+int orc_born_forward(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                     const orc_shot *s, int nt, const float *r_vp, const float *r_vs,
+                     const float *r_rho, float *data);
+int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                     const orc_shot *s, int nt, const float *residual, float *g_vp, float *g_vs,
+                     float *g_rho);
+
 /* Threads used by the OpenMP loops (1 if built without OpenMP). */
 int orc_threads(void);
 /* sizeof(REAL) of this build. */

@@ -82,6 +82,10 @@ def lib(bits: int = 64) -> C.CDLL:
         L.orc_state_step.argtypes = [C.c_void_p, P(Shot), C.c_int, C.c_int, C.c_int, f,
                                      P(Excitation), f, f, f]
         L.orc_state_destroy.argtypes = [C.c_void_p]
+        L.orc_born_forward.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f, f, f, f]
+        L.orc_born_forward.restype = C.c_int
+        L.orc_born_adjoint.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f, f, f, f]
+        L.orc_born_adjoint.restype = C.c_int
         L.orc_threads.restype = C.c_int
         L.orc_real_size.restype = C.c_int
         _libs[bits] = L
@@ -214,3 +218,26 @@ def divcurl(g: Grid, vp, vs, vx, vy, vz):
     if rc != 0:
         raise RuntimeError(f"orc_divcurl failed: {rc}")
     return p, sx, sy, sz
+
+
+def born_forward(g: Grid, vp, vs, rho, shot: Shot, nt: int, r_vp, r_vs, r_rho, bits=64):
+    """Born data [3][nt][nrec] for relative perturbations of (vp, vs, rho); 2D sponge only."""
+    data = np.zeros((3, nt, shot.nrx * shot.nry), np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (r_vp, r_vs, r_rho)]
+    rc = lib(bits).orc_born_forward(C.byref(g), _fp(vp), _fp(vs), _fp(rho), C.byref(shot), nt,
+                                    *[_fp(a) for a in args], _fp(data))
+    if rc != 0:
+        raise RuntimeError(f"orc_born_forward failed: {rc}")
+    return data
+
+
+def born_adjoint(g: Grid, vp, vs, rho, shot: Shot, nt: int, residual, bits=64):
+    """Exact transpose of born_forward applied to residual; returns (g_vp, g_vs, g_rho)."""
+    shape = (g.nz, g.ny, g.nx)
+    out = [np.zeros(shape, np.float32) for _ in range(3)]
+    res = np.ascontiguousarray(residual, np.float32)
+    rc = lib(bits).orc_born_adjoint(C.byref(g), _fp(vp), _fp(vs), _fp(rho), C.byref(shot), nt,
+                                    _fp(res), *[_fp(o) for o in out])
+    if rc != 0:
+        raise RuntimeError(f"orc_born_adjoint failed: {rc}")
+    return tuple(out)

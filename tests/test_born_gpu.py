@@ -1,0 +1,69 @@
+"""CUDA Born operators against the oracle, adjointness in FP32, checkpoint independence."""
+import numpy as np
+import pytest
+
+from _born_case import born_case, oracle_shot
+from _cases import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(ertm, c, K=0):
+    nz, _, nx = c["shape"]
+    cfg = ertm.Config(nx=nx, ny=1, nz=nz, dx=10, dy=10, dz=10, dt_ms=1.0, nt=c["nt"],
+                      order=2 * c["R"], boundary=ertm.BOUNDARY_SPONGE_CUBIC, pml=c["pml"],
+                      sponge_coef=150.0, checkpoint_every=K)
+    ctx = ertm.Context(cfg)
+    ctx.set_model(ertm.MIGRATION_MODEL, c["vp"], c["vs"], c["rho"])
+    shot = ertm.Shot(*c["geo"]["src"], wavelet=c["w"], **c["geo"]["rec"])
+    return ctx, shot
+
+
+@pytest.mark.parametrize("R", [4, 6])
+def test_born_forward_and_adjoint_match_oracle(ertm, orc, R):
+    c = born_case(orc, R=R)
+    s = oracle_shot(orc, c)
+    rng = c["rng"]
+    m = [(0.05 * rng.standard_normal(c["shape"])).astype(np.float32) for _ in range(3)]
+    ref = orc.born_forward(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], *m)
+    r32 = orc.born_forward(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], *m, bits=32)
+    ctx, shot = _ctx(ertm, c, K=40)
+    gpu = ctx.born_forward(shot, *m)
+    for q in (0, 2):
+        assert rel(gpu[q], ref[q]) <= max(1e-5, 3 * rel(r32[q], ref[q])), q
+    dh = rng.standard_normal(ref.shape).astype(np.float32)
+    dh[1] = 0
+    gref = orc.born_adjoint(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], dh)
+    g32 = orc.born_adjoint(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], dh, bits=32)
+    ggpu = ctx.born_adjoint(shot, dh)
+    for a, b, f in zip(ggpu, gref, g32):
+        assert rel(a, b) <= max(1e-5, 3 * rel(f, b))
+
+
+def test_gpu_dot_product_and_checkpoint_independence(ertm, orc):
+    c = born_case(orc, nz=64, nx=80, nt=400)
+    rng = c["rng"]
+    m = [(0.05 * rng.standard_normal(c["shape"])).astype(np.float32) for _ in range(3)]
+    ctx, shot = _ctx(ertm, c, K=0)
+    d = ctx.born_forward(shot, *m)
+    dh = rng.standard_normal(d.shape).astype(np.float32)
+    dh[1] = 0
+    g_default = ctx.born_adjoint(shot, dh)
+    lhs = float(np.sum(d.astype(np.float64) * dh))
+    rhs = sum(float(np.sum(a.astype(np.float64) * b)) for a, b in zip(m, g_default))
+    assert abs(lhs - rhs) <= 1e-4 * abs(lhs), (lhs, rhs)
+    ctx7, shot7 = _ctx(ertm, c, K=7)
+    g7 = ctx7.born_adjoint(shot7, dh)
+    for a, b in zip(g7, g_default):
+        assert np.array_equal(a, b)       # the rebuilt background is bit-identical
+
+
+def test_born_rejects_cpml_and_3d(ertm):
+    cfg = ertm.Config(nx=40, ny=1, nz=40, dx=5, dy=5, dz=5, dt_ms=0.5, nt=10, pml=(8, 8, 0, 0, 8, 8))
+    ctx = ertm.Context(cfg)
+    z = np.zeros((40, 1, 40), np.float32) + 2000
+    ctx.set_model(ertm.MIGRATION_MODEL, z, z / 2, z / 2)
+    shot = ertm.Shot(20, 0, 10, wavelet=np.ones(3, np.float32), rx0=0, nrx=4, rz=10)
+    with pytest.raises(ertm.ErtmError) as ei:
+        ctx.born_forward(shot, z * 0, z * 0, z * 0)
+    assert ei.value.code == -5
