@@ -73,6 +73,7 @@ SIGNATURES = {
     "ertm_forward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot)]),
     "ertm_backward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_rtm_shot": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_rtm_batch": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(_P), _P, _P, _P]),
     "ertm_get_wavefield": (C.c_int, [_P, C.c_int, _P]),
     "ertm_get_excitation": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "ertm_divcurl": (C.c_int, [_P, C.c_int, _P, _P, _P, _P]),
@@ -293,6 +294,24 @@ class Context:
         s = shot.struct()
         self._ck(self._L.ertm_rtm_shot(self._h, C.byref(s), _ptr(d, 3 * self.cfg.nt * shot.nrec),
                                        _ptr(pp, n, True), _ptr(ps, n, True), _ptr(tp, n, True)))
+        return pp, ps, tp
+
+    def rtm_batch(self, shots: list, data: list, pp=None, ps=None, tp=None):
+        """RTM of several shots with the images stacked on the device."""
+        n = self.ncell
+        pp, ps, tp = self._vol(pp), self._vol(ps), self._vol(tp)
+        arr = (_Shot * max(1, len(shots)))()
+        keep = []
+        for q, sh in enumerate(shots):
+            arr[q] = sh.struct()
+        ptrs = (C.c_void_p * max(1, len(data)))()
+        for q, (sh, d) in enumerate(zip(shots, data)):
+            d = d if _is_torch(d) else np.ascontiguousarray(d, np.float32)
+            keep.append(d)
+            ptrs[q] = _ptr(d, 3 * self.cfg.nt * sh.nrec)
+        self._ck(self._L.ertm_rtm_batch(self._h, arr, len(shots), ptrs, _ptr(pp, n, True),
+                                        _ptr(ps, n, True), _ptr(tp, n, True)))
+        del keep
         return pp, ps, tp
 
     def get_wavefield(self, name_or_id, out=None):

@@ -88,6 +88,13 @@ __global__ void k_inject(KArgs a, int it)
 }
 
 __global__ void k_advance(int* it, int delta) { *it += delta; }
+
+__global__ void k_axpy(long long n, const float* __restrict__ x, float* __restrict__ y)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        y[i] += x[i];
+}
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
 template <int R>
@@ -187,6 +194,12 @@ cudaError_t launch_inject(const KArgs& a, int it, cudaStream_t s)
     long long nrec = (long long)a.nrx * a.nry;
     if (nrec <= 0) return cudaSuccess;
     k_inject<<<(unsigned)((nrec + 255) / 256), 256, 0, s>>>(a, it);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(long long n, const float* x, float* y, cudaStream_t s)
+{
+    k_axpy<<<grid_for(n), 256, 0, s>>>(n, x, y);
     return cudaGetLastError();
 }
 

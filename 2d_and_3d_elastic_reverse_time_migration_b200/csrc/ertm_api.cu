@@ -974,6 +974,39 @@ int ertm_rtm_shot(ertm_ctx* c, const ertm_shot* s, const float* data_in, float* 
     return ertm_backward_together_using_smoothed_model(c, s, data_in, img_pp, img_ps, img_tp);
 }
 
+int ertm_rtm_batch(ertm_ctx* c, const ertm_shot* shots, int nshots, const float* const* data,
+                   float* stack_pp, float* stack_ps, float* stack_tp)
+{
+    if (!c) return ERTM_EINVAL;
+    if (nshots < 0 || (nshots > 0 && (!shots || !data))) return fail(c, ERTM_EINVAL, "bad shot list");
+    CK(c, cudaSetDevice(c->device));
+    const Geom& g = c->g;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    float* outs[3] = {stack_pp, stack_ps, stack_tp};
+    // running sums in the padded layout, gathered once at the end
+    float* acc = nullptr;
+    CK(c, cudaMalloc(&acc, sizeof(float) * 3 * g.total));
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(float) * 3 * g.total, c->stream);
+    int rc = e == cudaSuccess ? ERTM_OK : fail(c, ERTM_ECUDA, "%s", cudaGetErrorString(e));
+    for (int q = 0; q < nshots && rc == ERTM_OK; q++) {
+        // one RTM shot (no per-shot image download), then stack its images
+        rc = ertm_forward_together_using_smoothed_model(c, &shots[q]);
+        if (rc == ERTM_OK)
+            rc = ertm_backward_together_using_smoothed_model(c, &shots[q], data[q], nullptr, nullptr,
+                                                             nullptr);
+        for (int k = 0; rc == ERTM_OK && k < 3; k++) {
+            e = launch_axpy(g.total, c->img_base[k], acc + k * g.total, c->stream);
+            if (e != cudaSuccess) rc = fail(c, ERTM_ECUDA, "stack: %s", cudaGetErrorString(e));
+            c->launches++;
+        }
+    }
+    for (int k = 0; rc == ERTM_OK && k < 3; k++) rc = copy_out_volume(c, acc + k * g.total + g.off0, outs[k]);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(acc);
+    (void)n;
+    return rc;
+}
+
 int ertm_get_wavefield(ertm_ctx* c, int field, float* out)
 {
     if (!c) return ERTM_EINVAL;

@@ -1,0 +1,96 @@
+"""Least-squares RTM: conjugate gradients on the Born normal equations.
+
+Solves  min_m 0.5 sum_shots |F_s m - d_s|^2  for the relative perturbations
+m = (r_vp, r_vs, r_rho) of the migration model, with F_s the Born operator of
+shot s (`Context.born_forward`) and F_s^T its exact adjoint
+(`Context.born_adjoint`).  The reference's LSRTM driver loop is absent from its
+tree; its kernels (Born "demig", adjoint, gradient) are what these operators
+restate.
+
+`precond` (optional) maps a gradient (3 volumes) to a search direction; it is
+used as in preconditioned CGLS, and a preconditioned step is accepted only if
+the Born-modelled data misfit falls, otherwise the plain CG step of the same
+iteration is taken instead (plain CG is the fallback).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, Sequence
+
+import numpy as np
+
+
+@dataclass
+class CGResult:
+    m: tuple                      # (r_vp, r_vs, r_rho) numpy arrays
+    misfit: list = field(default_factory=list)   # relative data misfit |r|^2/|d|^2 per iteration
+    accepted: list = field(default_factory=list)  # per iteration: "precond" or "plain"
+
+
+def _dot(a: Sequence[np.ndarray], b: Sequence[np.ndarray]) -> float:
+    return float(sum(np.sum(x.astype(np.float64) * y) for x, y in zip(a, b)))
+
+
+def _axpy(alpha: float, x, y):
+    return tuple((yy + alpha * xx).astype(np.float32) for xx, yy in zip(x, y))
+
+
+def born_all(ctx, shots, m):
+    return [ctx.born_forward(s, *m) for s in shots]
+
+
+def adjoint_all(ctx, shots, res):
+    g = None
+    for s, r in zip(shots, res):
+        gs = ctx.born_adjoint(s, r)
+        g = gs if g is None else tuple(a + b for a, b in zip(g, gs))
+    return tuple(x.astype(np.float32) for x in g)
+
+
+def cgls(ctx, shots: list, data: list, niter: int,
+         precond: Callable[[tuple], tuple] | None = None,
+         callback: Callable[[int, float], None] | None = None) -> CGResult:
+    shape = ctx.cfg.shape
+    m = tuple(np.zeros(shape, np.float32) for _ in range(3))
+    r = [d.astype(np.float32).copy() for d in data]            # r = d - F m
+    dnorm = sum(float(np.sum(d.astype(np.float64) ** 2)) for d in data)
+    s = adjoint_all(ctx, shots, r)
+    z = precond(s) if precond else s
+    p = z
+    gamma = _dot(s, z)
+    out = CGResult(m=m)
+    rnorm = dnorm
+    for it in range(niter):
+        q = born_all(ctx, shots, p)
+        qq = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q)
+        if qq == 0.0 or gamma == 0.0:
+            break
+        alpha = gamma / qq
+        r_new = [(rr - alpha * qq_).astype(np.float32) for rr, qq_ in zip(r, q)]
+        rn = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new)
+        kind = "precond" if precond else "plain"
+        if precond and rn >= rnorm:
+            # safeguard: the preconditioned direction did not lower the misfit;
+            # restart from the plain gradient direction
+            p = s
+            gamma = _dot(s, s)
+            q = born_all(ctx, shots, p)
+            qq = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q)
+            alpha = gamma / qq
+            r_new = [(rr - alpha * qq_).astype(np.float32) for rr, qq_ in zip(r, q)]
+            rn = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new)
+            kind = "plain"
+        m = _axpy(alpha, p, m)
+        r, rnorm = r_new, rn
+        s = adjoint_all(ctx, shots, r)
+        z = precond(s) if (precond and kind == "precond") else s
+        gamma_new = _dot(s, z)
+        beta = gamma_new / gamma if gamma else 0.0
+        p = _axpy(beta, p, z)
+        gamma = gamma_new
+        out.misfit.append(rnorm / dnorm)
+        out.accepted.append(kind)
+        if callback:
+            callback(it, rnorm / dnorm)
+    out.m = m
+    return out

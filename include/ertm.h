@@ -148,6 +148,14 @@ int ertm_backward_together_using_smoothed_model(ertm_ctx *ctx, const ertm_shot *
 int ertm_rtm_shot(ertm_ctx *ctx, const ertm_shot *shot, const float *data_in,
                   float *img_pp, float *img_ps, float *img_tp);
 
+/* RTM of `nshots` shots on this context's GPU with the images stacked on the
+ * device (the reference's shot loop and per-shot image files,
+ * 3D_output_file.cu:339-365, become one sum); data[q] is shot q's
+ * [3][nt][nrec] record.  Outputs are nz*ny*nx (any may be NULL).  Several GPUs
+ * split a shot list between contexts and add their stacks (one reduce). */
+int ertm_rtm_batch(ertm_ctx *ctx, const ertm_shot *shots, int nshots, const float *const *data,
+                   float *stack_pp, float *stack_ps, float *stack_tp);
+
 /* ---- least-squares RTM operators (2D, sponge boundaries) ---------------
  * The linearised (Born) modelling of the reference's LSRTM
  * (demig_fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization and
