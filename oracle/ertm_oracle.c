@@ -436,6 +436,9 @@ static long rec_cell(const orc_state *S, const orc_shot *s, int r, int *ok)
     return AT(S, i, j, s->rz);
 }
 
+static int image_pp_ps(real ex, real ey, real ez, real px, real py, real pz, real sx, real sy,
+                       real sz, real *pp, real *ps);
+
 /* One time step `it` of a pass, in the order of
  * 3D_elastic_RTM/3D_forward_or_back_together.cu:25-154 (model), :173-289 (source),
  * :310-452 (receiver). */
@@ -516,18 +519,30 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                     long m = ((long)k * g->ny + j) * g->nx + i;
                     if (ex->time[m] != it) continue;
                     long c = AT(S, i, j, k);
-                    real ex_ = ex->evx[m], ey = ex->evy[m], ez = ex->evz[m];
-                    real den = ex_ * ex_ + ey * ey + ez * ez;
                     real px = S->f[F_VXP][c], py = S->f[F_VYP][c], pz = S->f[F_VZP][c];
-                    real sx = S->f[F_VX][c] - px, sy2 = S->f[F_VY][c] - py, sz2 = S->f[F_VZ][c] - pz;
-                    if (den > 0) {
-                        if (pp) pp[m] = (float)((ex_ * px + ey * py + ez * pz) / den);
-                        if (ps) ps[m] = (float)((ex_ * sx + ey * sy2 + ez * sz2) / den);
+                    real vpp, vps;
+                    if (image_pp_ps(ex->evx[m], ex->evy[m], ex->evz[m], px, py, pz,
+                                    S->f[F_VX][c] - px, S->f[F_VY][c] - py, S->f[F_VZ][c] - pz,
+                                    &vpp, &vps)) {
+                        if (pp) pp[m] = (float)vpp;
+                        if (ps) ps[m] = (float)vps;
                     }
                     real et = ex->etp[m];
                     if (ptp && et != 0) ptp[m] = (float)(S->f[F_TP][c] / et);
                 }
     }
+}
+
+/* PP and PS of one cell (imaging_inner_product_ex_2D, elastic_2D_kernel_3.cu:559-580):
+ * (e . r_P)/|e|^2 and (e . r_S)/|e|^2; returns 0 where |e|^2 == 0 */
+static int image_pp_ps(real ex, real ey, real ez, real px, real py, real pz, real sx, real sy,
+                       real sz, real *pp, real *ps)
+{
+    real den = ex * ex + ey * ey + ez * ez;
+    if (!(den > 0)) return 0;
+    *pp = (ex * px + ey * py + ez * pz) / den;
+    *ps = (ex * sx + ey * sy + ez * sz) / den;
+    return 1;
 }
 
 static void state_export(const orc_state *S, float *out)
@@ -698,6 +713,9 @@ static real b_dmx(const born2d *S, const real *f, long c) { return dminus(f, c, 
 static real b_dpz(const born2d *S, const real *f, long c) { return dplus(f, c, S->px, S->c, S->R) * S->iz; }
 static real b_dmz(const born2d *S, const real *f, long c) { return dminus(f, c, S->px, S->c, S->R) * S->iz; }
 
+static void born_sources(real dm, real du, real rr, real e0xx, real e0zz, real e0xz, real a0x,
+                         real a0z, real dt, real *sxx, real *szz, real *sxz, real *svx, real *svz);
+
 /* one step of background (+ scattered when dM != NULL); stores v0 (start of
  * step) and a0 into keep[4] when keep != NULL */
 static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, real *v0z, real *s0xx,
@@ -727,10 +745,12 @@ static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, rea
             if (dM) {
                 real exx = b_dpx(S, vx, c), ezz = b_dmz(S, vz, c);
                 real exz = b_dpz(S, vx, c) + b_dmx(S, vz, c);
-                real dm = dM[c], du = dU[c], dl = dm - 2 * du;
-                sxx[c] = g1 * (g2 * sxx[c] + dt * (M * exx + L * ezz + dm * e0xx + dl * e0zz));
-                szz[c] = g1 * (g2 * szz[c] + dt * (M * ezz + L * exx + dm * e0zz + dl * e0xx));
-                sxz[c] = g1 * (g2 * sxz[c] + dt * (U * exz + du * e0xz));
+                real qxx, qzz, qxz, unused0, unused1;
+                born_sources(dM[c], dU[c], 0, e0xx, e0zz, e0xz, 0, 0, dt, &qxx, &qzz, &qxz, &unused0,
+                             &unused1);
+                sxx[c] = g1 * (g2 * sxx[c] + dt * (M * exx + L * ezz) + qxx);
+                szz[c] = g1 * (g2 * szz[c] + dt * (M * ezz + L * exx) + qzz);
+                sxz[c] = g1 * (g2 * sxz[c] + dt * U * exz + qxz);
             }
         }
 #pragma omp parallel for schedule(static)
@@ -746,10 +766,27 @@ static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, rea
             if (dM) {
                 real ax = b * (b_dmx(S, sxx, c) + b_dmz(S, sxz, c));
                 real az = b * (b_dpx(S, sxz, c) + b_dpz(S, szz, c));
-                vx[c] = g1 * (g2 * vx[c] + dt * (ax - rr[c] * a0x));
-                vz[c] = g1 * (g2 * vz[c] + dt * (az - rr[c] * a0z));
+                real q0, q1, q2, svx, svz;
+                born_sources(0, 0, rr[c], 0, 0, 0, a0x, a0z, dt, &q0, &q1, &q2, &svx, &svz);
+                vx[c] = g1 * (g2 * vx[c] + dt * ax + svx);
+                vz[c] = g1 * (g2 * vz[c] + dt * az + svz);
             }
         }
+}
+
+/* Born secondary sources of one cell (the reference's dem_p terms,
+ * cuda_cal_dem_parameter_viscoelastic_media_new, viscoelastic_equation.cu:2398-2505,
+ * inversion_para 2, no attenuation): stress sources dt (dM exx + dL ezz,
+ * dM ezz + dL exx, dU exz) and velocity sources -dt r_rho (ax, az) */
+static void born_sources(real dm, real du, real rr, real e0xx, real e0zz, real e0xz, real a0x,
+                         real a0z, real dt, real *sxx, real *szz, real *sxz, real *svx, real *svz)
+{
+    real dl = dm - 2 * du;
+    *sxx = dt * (dm * e0xx + dl * e0zz);
+    *szz = dt * (dm * e0zz + dl * e0xx);
+    *sxz = dt * du * e0xz;
+    *svx = -dt * rr * a0x;
+    *svz = -dt * rr * a0z;
 }
 
 static int born_rec(const born2d *S, const orc_shot *s, int r, long *c)
@@ -897,4 +934,66 @@ int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const 
     free(hist);
     born_free(&S);
     return rc;
+}
+
+/* ----------------------------------------------------------------------
+ * Entry points used only to compare single pieces of the scheme with the
+ * reference's own 2D kernels (tests/golden/ref_kernels_2d.npz)
+ * -------------------------------------------------------------------- */
+
+/* One stress half-step of the 2D scheme from given fields (nz*nx arrays):
+ * the code of stress_step, without the P stress. */
+int orc_stress_step_given(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                          const float *vx, const float *vz, const float *txx, const float *tzz,
+                          const float *txz, float *otxx, float *otzz, float *otxz)
+{
+    if (!g || g->ny != 1) return -1;
+    orc_state *S = state_new(g, vp, vs, rho);
+    if (!S) return -2;
+    const float *in[5] = {vx, vz, txx, tzz, txz};
+    const int fid[5] = {F_VX, F_VZ, F_TXX, F_TZZ, F_TXZ};
+    for (int q = 0; q < 5; q++)
+        for (int k = 0; k < g->nz; k++)
+            for (int i = 0; i < g->nx; i++)
+                S->f[fid[q]][AT(S, i, 0, k)] = in[q][(long)k * g->nx + i];
+    stress_step(S, 0);
+    float *out[3] = {otxx, otzz, otxz};
+    const int oid[3] = {F_TXX, F_TZZ, F_TXZ};
+    for (int q = 0; q < 3; q++)
+        for (int k = 0; k < g->nz; k++)
+            for (int i = 0; i < g->nx; i++)
+                out[q][(long)k * g->nx + i] = (float)S->f[oid[q]][AT(S, i, 0, k)];
+    state_free(S);
+    return 0;
+}
+
+/* Born secondary sources for n cells (see born_sources): inputs per cell */
+int orc_born_sources_given(long n, double dt_ms, const float *vp, const float *vs, const float *rho,
+                           const float *rvp, const float *rvs, const float *rrho, const float *exx,
+                           const float *ezz, const float *exz, const float *ax, const float *az,
+                           float *osxx, float *oszz, float *osxz, float *osvx, float *osvz)
+{
+    real dt = (real)(dt_ms / 1000.0);
+    for (long c = 0; c < n; c++) {
+        real r = rho[c], p = vp[c], q = vs[c];
+        real M = r * p * p, U = r * q * q;
+        real dm = M * ((real)rrho[c] + 2 * (real)rvp[c]), du = U * ((real)rrho[c] + 2 * (real)rvs[c]);
+        real a, b, d, e, f;
+        born_sources(dm, du, rrho[c], exx[c], ezz[c], exz[c], ax[c], az[c], dt, &a, &b, &d, &e, &f);
+        osxx[c] = (float)a; oszz[c] = (float)b; osxz[c] = (float)d; osvx[c] = (float)e; osvz[c] = (float)f;
+    }
+    return 0;
+}
+
+/* PP / PS of n cells with the oracle's imaging rule (2D: y components zero) */
+int orc_image_given(long n, const float *ex, const float *ez, const float *rpx, const float *rpz,
+                    const float *rsx, const float *rsz, float *pp, float *ps)
+{
+    for (long c = 0; c < n; c++) {
+        real a = 0, b = 0;
+        if (!image_pp_ps(ex[c], 0, ez[c], rpx[c], 0, rpz[c], rsx[c], 0, rsz[c], &a, &b)) a = b = 0;
+        pp[c] = (float)a;
+        ps[c] = (float)b;
+    }
+    return 0;
 }

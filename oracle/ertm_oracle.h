@@ -128,6 +128,18 @@ int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const 
                      const orc_shot *s, int nt, const float *residual, float *g_vp, float *g_vs,
                      float *g_rho);
 
+/* Single pieces of the scheme on given inputs, for comparison with the
+ * reference's own 2D kernels (see ertm_oracle.c). */
+int orc_stress_step_given(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                          const float *vx, const float *vz, const float *txx, const float *tzz,
+                          const float *txz, float *otxx, float *otzz, float *otxz);
+int orc_born_sources_given(long n, double dt_ms, const float *vp, const float *vs, const float *rho,
+                           const float *rvp, const float *rvs, const float *rrho, const float *exx,
+                           const float *ezz, const float *exz, const float *ax, const float *az,
+                           float *osxx, float *oszz, float *osxz, float *osvx, float *osvz);
+int orc_image_given(long n, const float *ex, const float *ez, const float *rpx, const float *rpz,
+                    const float *rsx, const float *rsz, float *pp, float *ps);
+
 /* Threads used by the OpenMP loops (1 if built without OpenMP). */
 int orc_threads(void);
 /* sizeof(REAL) of this build. */

@@ -86,6 +86,12 @@ def lib(bits: int = 64) -> C.CDLL:
         L.orc_born_forward.restype = C.c_int
         L.orc_born_adjoint.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f, f, f, f]
         L.orc_born_adjoint.restype = C.c_int
+        L.orc_stress_step_given.argtypes = [P(Grid)] + [f] * 11
+        L.orc_stress_step_given.restype = C.c_int
+        L.orc_born_sources_given.argtypes = [C.c_long, C.c_double] + [f] * 16
+        L.orc_born_sources_given.restype = C.c_int
+        L.orc_image_given.argtypes = [C.c_long] + [f] * 8
+        L.orc_image_given.restype = C.c_int
         L.orc_threads.restype = C.c_int
         L.orc_real_size.restype = C.c_int
         _libs[bits] = L
@@ -241,3 +247,36 @@ def born_adjoint(g: Grid, vp, vs, rho, shot: Shot, nt: int, residual, bits=64):
     if rc != 0:
         raise RuntimeError(f"orc_born_adjoint failed: {rc}")
     return tuple(out)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def stress_step_given(g: Grid, vp, vs, rho, vx, vz, txx, tzz, txz):
+    """One 2D stress half-step from given [nz][nx] fields -> (txx, tzz, txz)."""
+    shape = (g.nz, g.nx)
+    out = [np.zeros(shape, np.float32) for _ in range(3)]
+    ins = [_f32(a) for a in (vp, vs, rho, vx, vz, txx, tzz, txz)]
+    rc = lib().orc_stress_step_given(C.byref(g), *[_fp(a) for a in ins], *[_fp(o) for o in out])
+    if rc != 0:
+        raise RuntimeError(f"orc_stress_step_given failed: {rc}")
+    return tuple(out)
+
+
+def born_sources_given(dt_ms, vp, vs, rho, rvp, rvs, rrho, exx, ezz, exz, ax, az):
+    """Per-cell Born secondary sources -> (sxx, szz, sxz, svx, svz) increments."""
+    ins = [_f32(a).ravel() for a in (vp, vs, rho, rvp, rvs, rrho, exx, ezz, exz, ax, az)]
+    n = ins[0].size
+    out = [np.zeros(n, np.float32) for _ in range(5)]
+    lib().orc_born_sources_given(n, dt_ms, *[_fp(a) for a in ins], *[_fp(o) for o in out])
+    return tuple(out)
+
+
+def image_given(ex, ez, rpx, rpz, rsx, rsz):
+    """Per-cell PP and PS excitation-amplitude images (0 where e == 0)."""
+    ins = [_f32(a).ravel() for a in (ex, ez, rpx, rpz, rsx, rsz)]
+    n = ins[0].size
+    pp, ps = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    lib().orc_image_given(n, *[_fp(a) for a in ins], _fp(pp), _fp(ps))
+    return pp, ps

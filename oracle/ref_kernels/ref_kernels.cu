@@ -1,0 +1,127 @@
+// Golden-vector harness over the reference's own 2D CUDA kernels, compiled from
+// the reference tree (paths passed by the Makefile).  Host wrappers copy small
+// arrays in the reference's 2D layout (ix * (nz + 2 radius) + iz, radius-padded)
+// to the device, launch one reference kernel and copy the result back.  Only
+// tests/golden/make_golden_kernels.py calls it, to record fixtures.
+#include "ref_shim.cuh"
+#include REF_K2
+#include REF_K3
+#include REF_VISCO
+
+#include <vector>
+
+namespace {
+struct Dev {
+    std::vector<float*> p;
+    float* put(const float* h, size_t n)
+    {
+        float* d = nullptr;
+        cudaMalloc(&d, n * sizeof(float));
+        if (h) cudaMemcpy(d, h, n * sizeof(float), cudaMemcpyHostToDevice);
+        else cudaMemset(d, 0, n * sizeof(float));
+        p.push_back(d);
+        return d;
+    }
+    float* fill(float v, size_t n)
+    {
+        std::vector<float> h(n, v);
+        return put(h.data(), n);
+    }
+    ~Dev() { for (float* d : p) cudaFree(d); }
+};
+int get(float* h, const float* d, size_t n)
+{
+    cudaDeviceSynchronize();
+    cudaMemcpy(h, d, n * sizeof(float), cudaMemcpyDeviceToHost);
+    return (int)cudaGetLastError();
+}
+}  // namespace
+
+// fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization (viscoelastic_equation.cu:184-325)
+// with tao = strain = 1 (no attenuation: memory variables stay zero) and
+// modul_p = vp^2, modul_s = vs^2: one elastic stress half-step with damping.
+// nx % 32 == 0, nz % 16 == 0.  coe_x = dt/1000/dx (the driver that sets it is absent).
+extern "C" int ref_stress_step(int nx, int nz, float dt_ms, float dx, float dz, const float* coe7,
+                               const float* vp, const float* vs, const float* rho, const float* att,
+                               const float* vx, const float* vz, const float* txx, const float* tzz,
+                               const float* txz, float* otxx, float* otzz, float* otxz)
+{
+    const size_t n = (size_t)(nx + 2 * radius) * (nz + 2 * radius);
+    Dev D;
+    std::vector<float> mp(n), ms(n);
+    for (size_t i = 0; i < n; i++) { mp[i] = vp[i] * vp[i]; ms[i] = vs[i] * vs[i]; }
+    float *dvx = D.put(vx, n), *dvz = D.put(vz, n);
+    float *t1xx = D.put(txx, n), *t1zz = D.put(tzz, n), *t1xz = D.put(txz, n);
+    float *t2xx = D.put(nullptr, n), *t2zz = D.put(nullptr, n), *t2xz = D.put(nullptr, n);
+    float *tp1 = D.put(nullptr, n), *tp2 = D.put(nullptr, n);
+    float *mpd = D.put(mp.data(), n), *msd = D.put(ms.data(), n), *attd = D.put(att, n);
+    float *rhod = D.put(rho, n), *vpd = D.put(vp, n), *vsd = D.put(vs, n);
+    float* mem[8];
+    for (int q = 0; q < 8; q++) mem[q] = D.put(nullptr, n);
+    float *tao = D.fill(1.f, n), *sp = D.fill(1.f, n), *ss = D.fill(1.f, n);
+    float* coe = D.put(coe7, 7);
+    const float coe_x = dt_ms / 1000.f / dx, coe_z = dt_ms / 1000.f / dz;
+    fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization<<<dim3(nx / 32, nz / 16), dim3(32, 16)>>>(
+        tp2, tp1, t2xx, t1xx, t2zz, t1zz, t2xz, t1xz, dvx, dvz, mpd, msd, attd, dt_ms, coe, coe_x,
+        coe_z, nx, nz, rhod, mem[0], mem[1], mem[2], mem[3], mem[4], mem[5], mem[6], mem[7], vpd, vsd,
+        tao, sp, ss);
+    int e = get(otxx, t2xx, n);
+    e |= get(otzz, t2zz, n);
+    e |= get(otxz, t2xz, n);
+    return e;
+}
+
+// decom_new (elastic_2D_kernel_2.cu:671-791): P = vp div v, S = vs curl v
+extern "C" int ref_decom_new(int nx, int nz, float dx, float dz, const float* coe7, const float* vx,
+                             const float* vz, const float* vp, const float* vs, float* p, float* s)
+{
+    const size_t n = (size_t)(nx + 2 * radius) * (nz + 2 * radius);
+    Dev D;
+    float *dvx = D.put(vx, n), *dvz = D.put(vz, n), *dp = D.put(nullptr, n), *ds = D.put(nullptr, n);
+    float *vpd = D.put(vp, n), *vsd = D.put(vs, n), *coe = D.put(coe7, 7);
+    decom_new<<<dim3(nx / 32, nz / 16), dim3(32, 16)>>>(dvx, dvz, dp, ds, vpd, vsd, coe, nx, nz, dx, dz);
+    int e = get(p, dp, n);
+    e |= get(s, ds, n);
+    return e;
+}
+
+// imaging_inner_product_ex_2D (elastic_2D_kernel_3.cu:559-580) with every cell's
+// excitation time equal to `it`; plain nx*nz arrays (no padding, no offsets)
+extern "C" int ref_imaging(int nx, int nz, const float* ex, const float* ez, const float* rx,
+                           const float* rz, float* out)
+{
+    const size_t n = (size_t)nx * nz;
+    Dev D;
+    float *dex = D.put(ex, n), *dez = D.put(ez, n), *drx = D.put(rx, n), *drz = D.put(rz, n);
+    float *dt = D.put(nullptr, n), *amp = D.put(nullptr, n), *dout = D.put(nullptr, n);
+    float* mx = D.fill(1.f, 1);
+    imaging_inner_product_ex_2D<<<dim3((nx + 31) / 32, (nz + 15) / 16), dim3(32, 16)>>>(
+        dout, amp, dex, dez, dt, drx, drz, nx, nz, nz, 0, 0, mx, 0);
+    return get(out, dout, n);
+}
+
+// cuda_cal_dem_parameter_viscoelastic_media_new (viscoelastic_equation.cu:2398-2505),
+// inversion_para 2 (relative vp, vs, rho perturbations), no attenuation.
+// out: dem_p1, dem_p2, then dem_p[2..4] (stress sources), each padded n.
+extern "C" int ref_dem_sources(int nx, int nz, float dt_ms, const float* vp, const float* vs,
+                               const float* rho, const float* rvp, const float* rvs, const float* rrho,
+                               const float* vx_x, const float* vx_z, const float* vz_x,
+                               const float* vz_z, const float* vx_t, const float* vz_t, float* out)
+{
+    const size_t n = (size_t)(nx + 2 * radius2) * (nz + 2 * radius2);
+    Dev D;
+    float *d1 = D.put(nullptr, n), *d2 = D.put(nullptr, n), *dall = D.put(nullptr, 8 * n);
+    float *a = D.put(vx_x, n), *b = D.put(vx_z, n), *c = D.put(vz_x, n), *d = D.put(vz_z, n);
+    float *e = D.put(vx_t, n), *f = D.put(vz_t, n);
+    float *z0 = D.put(nullptr, n), *z1 = D.put(nullptr, n), *z2 = D.put(nullptr, n);
+    float *pvp = D.put(rvp, n), *pvs = D.put(rvs, n), *pr = D.put(rrho, n);
+    float *vpd = D.put(vp, n), *vsd = D.put(vs, n), *rhod = D.put(rho, n);
+    float *tao = D.fill(1.f, n), *sp = D.fill(1.f, n), *ss = D.fill(1.f, n);
+    cuda_cal_dem_parameter_viscoelastic_media_new<<<dim3(nx / 32, nz / 16), dim3(32, 16)>>>(
+        d1, d2, dall, a, b, c, d, e, f, z0, z1, z2, pvp, pvs, pr, nx, nz, vpd, vsd, rhod, tao, sp, ss,
+        dt_ms, 2);
+    int err = get(out, d1, n);
+    err |= get(out + n, d2, n);
+    err |= get(out + 2 * n, dall + 2 * n, 3 * n);
+    return err;
+}
