@@ -3,9 +3,12 @@
 // One time step is two z-streaming kernels:
 //   k_stress   : sigma(n+1) = f(sigma(n), v(n)) [+ P stress tp]      (+ source)
 //   k_velocity : v(n+1) = f(v(n), sigma(n+1))   [+ P velocity v_P]   (+ epilogue)
-// Each CTA owns a TX x TYB column of the x–y plane and a chunk of z planes.
-// One elected thread streams every input plane into a ring of shared-memory
-// stages with TMA (cp.async.bulk.tensor, mbarrier completion, S planes ahead);
+// Each CTA owns a TX x TYB column of the x–y plane and a chunk of z planes:
+// TYB consumer warps (one cell per thread) plus one producer warp.  One lane of
+// the producer warp streams every input plane into a ring of shared-memory
+// stages with TMA (cp.async.bulk.tensor, mbarrier completion, S planes ahead),
+// refilling a stage right after the per-plane barrier that frees it, so the
+// issue cost stays off the consumers' critical path;
 // C-PML memory variables, which live only in the absorbing slabs, come by
 // 4-byte cp.async into a double buffer.
 // The current plane of the fields that need x or y derivatives is staged in
@@ -163,7 +166,7 @@ struct StressShape {
 };
 
 template <int R, bool Y, bool CPML, bool PS>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), Y ? CTAS3 : 1)
+__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
 k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
 {
     using SS = StressShape<R, Y, CPML, PS>;
@@ -176,7 +179,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * SS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const bool leader = (tx == 0 && ty == 0);
+    const bool leader = (tx == 0 && ty == TYB);
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TYB;
     const int i = i0 + tx, j = j0 + ty;
     const int k0 = blockIdx.z * a.kchunk;
@@ -260,8 +263,21 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         mbar_fence_init();
     }
     __syncthreads();
-    if (leader)
-        for (int t = 0; t < kStages && t < nk; t++) issue(t);
+    if (ty == TYB) {   // producer warp: mirrors the consumers' per-plane barrier
+        if (leader)
+            for (int t = 0; t < kStages && t < nk; t++) issue(t);
+        __syncthreads();
+        for (int t = 0; t < nk; ++t) {
+            __syncthreads();
+            if (leader && t + kStages < nk) issue(t + kStages);
+        }
+        if (leader) {
+            for (int u = (nk > kStages ? nk - kStages : 0); u < nk; ++u)
+                if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1) && a.err)
+                    atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        }
+        return;
+    }
 
     // register queues of planes k-R .. k+R; the front (k+R) arrives with each stage
     const float* vsrc[3] = {a.f[F_VX], a.f[F_VZ], a.f[F_VY]};
@@ -396,7 +412,6 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         }
         cpa_wait_all();
         __syncthreads();
-        if (leader && ok && t + kStages < nk) issue(t + kStages);
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
@@ -435,7 +450,7 @@ struct VelShape {
 };
 
 template <int R, bool Y, bool CPML, int EPI, bool REC>
-__global__ void __launch_bounds__(TX * (Y ? TY3 : TY2), Y ? CTAS3 : 1)
+__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
 k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
 {
     using VS = VelShape<R, Y, CPML, EPI>;
@@ -447,7 +462,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * VS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const bool leader = (tx == 0 && ty == 0);
+    const bool leader = (tx == 0 && ty == TYB);
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TYB;
     const int i = i0 + tx, j = j0 + ty;
     const int k0 = blockIdx.z * a.kchunk;
@@ -535,8 +550,21 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         mbar_fence_init();
     }
     __syncthreads();
-    if (leader)
-        for (int t = 0; t < kStages && t < nk; t++) issue(t);
+    if (ty == TYB) {   // producer warp: mirrors the consumers' per-plane barrier
+        if (leader)
+            for (int t = 0; t < kStages && t < nk; t++) issue(t);
+        __syncthreads();
+        for (int t = 0; t < nk; ++t) {
+            __syncthreads();
+            if (leader && t + kStages < nk) issue(t + kStages);
+        }
+        if (leader) {
+            for (int u = (nk > kStages ? nk - kStages : 0); u < nk; ++u)
+                if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1) && a.err)
+                    atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        }
+        return;
+    }
 
     const float* txz = a.f[F_TXZ];
     const float* tyz = a.f[F_TYZ];
@@ -733,7 +761,6 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         }
         cpa_wait_all();
         __syncthreads();
-        if (leader && ok && t + kStages < nk) issue(t + kStages);
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
@@ -773,7 +800,7 @@ cudaError_t launch_stress_t(const Geom& g, const KArgs& a, const StressMaps& m, 
 {
     const bool Y = !g.two_d;
     const int tyb = Y ? TY3 : TY2;
-    dim3 block(TX, tyb), grid = step_grid(g, a, tyb);
+    dim3 block(TX, tyb + 1), grid = step_grid(g, a, tyb);
     if (Y) {
         if (cpml) return ps ? launch_stress_y<R, true, true, true>(grid, block, m, a, st)
                             : launch_stress_y<R, true, true, false>(grid, block, m, a, st);
@@ -809,7 +836,7 @@ cudaError_t launch_velocity_t(const Geom& g, const KArgs& a, const VelMaps& m, b
 {
     const bool Y = !g.two_d;
     const int tyb = Y ? TY3 : TY2;
-    dim3 block(TX, tyb), grid = step_grid(g, a, tyb);
+    dim3 block(TX, tyb + 1), grid = step_grid(g, a, tyb);
     if (Y) return cpml ? launch_velocity_y<R, true, true>(grid, block, m, a, epi, rec, st)
                        : launch_velocity_y<R, true, false>(grid, block, m, a, epi, rec, st);
     return cpml ? launch_velocity_y<R, false, true>(grid, block, m, a, epi, rec, st)
