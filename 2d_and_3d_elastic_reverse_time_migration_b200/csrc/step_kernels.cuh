@@ -7,8 +7,9 @@
 // TYB consumer warps (one cell per thread) plus one producer warp.  One lane of
 // the producer warp streams every input plane into a ring of shared-memory
 // stages with TMA (cp.async.bulk.tensor, mbarrier completion, S planes ahead),
-// refilling a stage right after the per-plane barrier that frees it, so the
-// issue cost stays off the consumers' critical path;
+// refilling a stage as soon as every consumer warp has arrived on the stage's
+// `empty` mbarrier.  There is no block-wide barrier in the z loop (warps drift
+// apart by up to S-1 planes) and the issue cost stays off the consumers' path;
 // C-PML memory variables, which live only in the absorbing slabs, come by
 // 4-byte cp.async into a double buffer.
 // The current plane of the fields that need x or y derivatives is staged in
@@ -119,6 +120,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
 // one plane of a 3D tiled tensor (coordinates in the padded volume)
 __device__ __forceinline__ void tma3(float* dst, const CUtensorMap* map, int x, int y, int z,
                                      uint64_t* bar)
@@ -144,7 +150,31 @@ struct Boxes {
     static constexpr int XY = XW * YH;
 };
 
+// Stage ring: plane t goes to stage t % kStages.  bars[s] ("full") completes
+// when the TMA bytes of the stage's plane have landed; bars[kStages + s]
+// ("empty") when all TYB consumer warps have arrived after using the stage.
 constexpr int kStages = 3;
+
+// Producer lane: issue planes 0 .. nk-1, refilling a stage as soon as its
+// previous plane is released.  Every wait is bounded; before returning it
+// waits (bounded) for the copies still in flight, so the block never exits
+// with a TMA write into its shared memory pending.  False if a wait gave up.
+template <class Issue>
+__device__ __forceinline__ bool produce_planes(uint64_t* bars, int nk, Issue issue)
+{
+    bool ok = true;
+    int t = 0;
+    for (; t < nk; ++t) {
+        if (t >= kStages && !mbar_wait_bounded(&bars[kStages + t % kStages], ((t / kStages) - 1) & 1)) {
+            ok = false;
+            break;
+        }
+        issue(t);
+    }
+    for (int u = (t > kStages ? t - kStages : 0); u < t; ++u)
+        if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1)) ok = false;
+    return ok;
+}
 
 // ---------------------------------------------------------------------------
 // Stress kernel
@@ -162,7 +192,7 @@ struct StressShape {
     static constexpr int STAGE = OFF_C + NC * B::C;             // floats
     static constexpr unsigned TX_BYTES = 4u * STAGE;
     static constexpr int PSI = NP * B::C;                       // floats per psi buffer
-    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 8 * kStages;
+    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 16 * kStages;
 };
 
 template <int R, bool Y, bool CPML, bool PS>
@@ -259,23 +289,15 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     };
 
     if (leader) {
-        for (int s = 0; s < kStages; s++) mbar_init(&bars[s], 1);
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&bars[s], 1);
+            mbar_init(&bars[kStages + s], TYB);
+        }
         mbar_fence_init();
     }
     __syncthreads();
-    if (ty == TYB) {   // producer warp: mirrors the consumers' per-plane barrier
-        if (leader)
-            for (int t = 0; t < kStages && t < nk; t++) issue(t);
-        __syncthreads();
-        for (int t = 0; t < nk; ++t) {
-            __syncthreads();
-            if (leader && t + kStages < nk) issue(t + kStages);
-        }
-        if (leader) {
-            for (int u = (nk > kStages ? nk - kStages : 0); u < nk; ++u)
-                if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1) && a.err)
-                    atomicExch(a.err, DEV_WAIT_TIMEOUT);
-        }
+    if (ty == TYB) {   // producer warp
+        if (leader && !produce_planes(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -291,7 +313,6 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     }
     issue_psi(k0, 0);
     cpa_wait_all();
-    __syncthreads();
 
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
@@ -411,7 +432,8 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
             if (Y) qy[q] = qy[q + 1];
         }
         cpa_wait_all();
-        __syncthreads();
+        __syncwarp();
+        if (tx == 0) mbar_arrive(&bars[kStages + st]);   // release the stage
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
@@ -446,7 +468,7 @@ struct VelShape {
     static constexpr unsigned TX_BYTES = 4u * STAGE;
     static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
     static constexpr int PSI = NP * B::C;
-    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 8 * kStages;
+    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 16 * kStages;
 };
 
 template <int R, bool Y, bool CPML, int EPI, bool REC>
@@ -546,23 +568,15 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     };
 
     if (leader) {
-        for (int s = 0; s < kStages; s++) mbar_init(&bars[s], 1);
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&bars[s], 1);
+            mbar_init(&bars[kStages + s], TYB);
+        }
         mbar_fence_init();
     }
     __syncthreads();
-    if (ty == TYB) {   // producer warp: mirrors the consumers' per-plane barrier
-        if (leader)
-            for (int t = 0; t < kStages && t < nk; t++) issue(t);
-        __syncthreads();
-        for (int t = 0; t < nk; ++t) {
-            __syncthreads();
-            if (leader && t + kStages < nk) issue(t + kStages);
-        }
-        if (leader) {
-            for (int u = (nk > kStages ? nk - kStages : 0); u < nk; ++u)
-                if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1) && a.err)
-                    atomicExch(a.err, DEV_WAIT_TIMEOUT);
-        }
+    if (ty == TYB) {   // producer warp
+        if (leader && !produce_planes(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -581,7 +595,6 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     }
     issue_psi(k0, 0);
     cpa_wait_all();
-    __syncthreads();
 
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
@@ -760,7 +773,8 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
             if (PS) qtp[q] = qtp[q + 1];
         }
         cpa_wait_all();
-        __syncthreads();
+        __syncwarp();
+        if (tx == 0) mbar_arrive(&bars[kStages + st]);   // release the stage
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
