@@ -528,16 +528,25 @@ int check_device_error(ertm_ctx* c)
     return ERTM_OK;
 }
 
-// z planes per CTA.  The step kernels run one CTA per SM (3D) or a few (2D);
-// the chunk count minimises (waves of CTAs) x (planes per chunk + start-up cost),
-// the start-up being the z-queue fill and the TMA pipeline ramp (~2R planes).
+// z planes per CTA.  3D: chunks of about 32 planes, balanced over nz.  Timed on
+// B200 at 480 x 480 x 380 (R = 4, C-PML), the step kernels get faster as the
+// chunk shrinks from the whole column (380 planes) down to 32-48 planes
+// (stress 1.92 -> 1.51 ms, velocity 1.98 -> 1.61 ms per launch), while below
+// ~24 planes the z-queue fill of each chunk starts to cost more than the finer
+// load balance gains.  2D: the chunk count minimises (waves of CTAs) x
+// (planes per chunk + start-up of ~2R planes).
 int choose_kchunk(const ertm_ctx* c)
 {
     const Geom& g = c->g;
+    if (!g.two_d) {
+        const int target = 32;
+        const int chunks = std::max(1, (g.nz + target / 2) / target);
+        return (g.nz + chunks - 1) / chunks;
+    }
     long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const long long slots = (long long)sms * (g.two_d ? 8 : CTAS3);
+    const long long slots = (long long)sms * 8;
     const double startup = 2.0 * c->R;
     int best = g.nz;
     double best_cost = 1e300;

@@ -150,29 +150,28 @@ struct Boxes {
     static constexpr int XY = XW * YH;
 };
 
-// Stage ring: plane t goes to stage t % kStages.  bars[s] ("full") completes
-// when the TMA bytes of the stage's plane have landed; bars[kStages + s]
+// Stage ring of NS stages: plane t goes to stage t % NS.  bars[s] ("full")
+// completes when the TMA bytes of the stage's plane have landed; bars[NS + s]
 // ("empty") when all TYB consumer warps have arrived after using the stage.
-constexpr int kStages = 3;
 
 // Producer lane: issue planes 0 .. nk-1, refilling a stage as soon as its
 // previous plane is released.  Every wait is bounded; before returning it
 // waits (bounded) for the copies still in flight, so the block never exits
 // with a TMA write into its shared memory pending.  False if a wait gave up.
-template <class Issue>
+template <int NS, class Issue>
 __device__ __forceinline__ bool produce_planes(uint64_t* bars, int nk, Issue issue)
 {
     bool ok = true;
     int t = 0;
     for (; t < nk; ++t) {
-        if (t >= kStages && !mbar_wait_bounded(&bars[kStages + t % kStages], ((t / kStages) - 1) & 1)) {
+        if (t >= NS && !mbar_wait_bounded(&bars[NS + t % NS], ((t / NS) - 1) & 1)) {
             ok = false;
             break;
         }
         issue(t);
     }
-    for (int u = (t > kStages ? t - kStages : 0); u < t; ++u)
-        if (!mbar_wait_bounded(&bars[u % kStages], (u / kStages) & 1)) ok = false;
+    for (int u = (t > NS ? t - NS : 0); u < t; ++u)
+        if (!mbar_wait_bounded(&bars[u % NS], (u / NS) & 1)) ok = false;
     return ok;
 }
 
@@ -192,7 +191,8 @@ struct StressShape {
     static constexpr int STAGE = OFF_C + NC * B::C;             // floats
     static constexpr unsigned TX_BYTES = 4u * STAGE;
     static constexpr int PSI = NP * B::C;                       // floats per psi buffer
-    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 16 * kStages;
+    static constexpr int NS = 4;                                // ring stages
+    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 2 * PSI) + 16 * NS;
 };
 
 template <int R, bool Y, bool CPML, bool PS>
@@ -201,11 +201,12 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
 {
     using SS = StressShape<R, Y, CPML, PS>;
     using B = typename SS::B;
+    constexpr int NS = SS::NS;
     constexpr int TYB = B::TYB, XB = B::XB, XW = B::XW, CB = B::C;
     constexpr int NV = SS::NV, NSIG = SS::NSIG;
     constexpr int C_TP = NSIG, C_M = NSIG + (PS ? 1 : 0), C_MU = C_M + 1;
     extern __shared__ __align__(128) float sm[];
-    float* psibuf = sm + kStages * SS::STAGE;
+    float* psibuf = sm + NS * SS::STAGE;
     uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * SS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -229,7 +230,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     const long long cj = (long long)j * sy + i;
 
     auto issue = [&](int t) {   // leader only: all boxes of iteration t into stage t % S
-        const int st = t % kStages;
+        const int st = t % NS;
         float* S = sm + st * SS::STAGE;
         uint64_t* bar = &bars[st];
         const int z = gz0 + t;
@@ -289,15 +290,15 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     };
 
     if (leader) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < NS; s++) {
             mbar_init(&bars[s], 1);
-            mbar_init(&bars[kStages + s], TYB);
+            mbar_init(&bars[NS + s], TYB);
         }
         mbar_fence_init();
     }
     __syncthreads();
     if (ty == TYB) {   // producer warp
-        if (leader && !produce_planes(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        if (leader && !produce_planes<NS>(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -317,8 +318,8 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
-        const int st = t % kStages;
-        if (ok) ok = mbar_wait_bounded(&bars[st], (t / kStages) & 1);
+        const int st = t % NS;
+        if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
         if (t + 1 < nk) issue_psi(k + 1, (t + 1) & 1);
         const float* S = sm + st * SS::STAGE;
         const float* Cc = S + SS::OFF_C;
@@ -433,7 +434,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         }
         cpa_wait_all();
         __syncwarp();
-        if (tx == 0) mbar_arrive(&bars[kStages + st]);   // release the stage
+        if (tx == 0) mbar_arrive(&bars[NS + st]);   // release the stage
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
@@ -468,7 +469,8 @@ struct VelShape {
     static constexpr unsigned TX_BYTES = 4u * STAGE;
     static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
     static constexpr int PSI = NP * B::C;
-    static constexpr size_t BYTES = 4 * (size_t)(kStages * STAGE + 2 * PSI) + 16 * kStages;
+    static constexpr int NS = 3;   // ring stages (4 would not leave room for 2 CTAs per SM)
+    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 2 * PSI) + 16 * NS;
 };
 
 template <int R, bool Y, bool CPML, int EPI, bool REC>
@@ -477,10 +479,11 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
 {
     using VS = VelShape<R, Y, CPML, EPI>;
     using B = typename VS::B;
+    constexpr int NS = VS::NS;
     constexpr bool PS = VS::PS;
     constexpr int TYB = B::TYB, XB = B::XB, XW = B::XW, CB = B::C;
     extern __shared__ __align__(128) float sm[];
-    float* psibuf = sm + kStages * VS::STAGE;
+    float* psibuf = sm + NS * VS::STAGE;
     uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * VS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -507,7 +510,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     float* vzp = a.f[F_VZP];
 
     auto issue = [&](int t) {
-        const int st = t % kStages;
+        const int st = t % NS;
         float* S = sm + st * VS::STAGE;
         uint64_t* bar = &bars[st];
         const int z = gz0 + t;
@@ -568,15 +571,15 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     };
 
     if (leader) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < NS; s++) {
             mbar_init(&bars[s], 1);
-            mbar_init(&bars[kStages + s], TYB);
+            mbar_init(&bars[NS + s], TYB);
         }
         mbar_fence_init();
     }
     __syncthreads();
     if (ty == TYB) {   // producer warp
-        if (leader && !produce_planes(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        if (leader && !produce_planes<NS>(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -599,8 +602,8 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
-        const int st = t % kStages;
-        if (ok) ok = mbar_wait_bounded(&bars[st], (t / kStages) & 1);
+        const int st = t % NS;
+        if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
         if (t + 1 < nk) issue_psi(k + 1, (t + 1) & 1);
         const float* S = sm + st * VS::STAGE;
         const float* Cc = S + VS::O_C;
@@ -774,7 +777,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         }
         cpa_wait_all();
         __syncwarp();
-        if (tx == 0) mbar_arrive(&bars[kStages + st]);   // release the stage
+        if (tx == 0) mbar_arrive(&bars[NS + st]);   // release the stage
     }
     if (!ok && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
 }
