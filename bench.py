@@ -301,6 +301,11 @@ def main():
     t_k = {"stress": ms_stress / ks, "velocity": ms_vel / ks}
     dom = max(t_k, key=t_k.get)
     achieved = bytes_k[dom] / (t_k[dom] / 1e3) / 1e9
+    # DRAM bytes per launch from one ncu capture (dram__bytes_read.sum +
+    # dram__bytes_write.sum, 1-pass metrics) of `bench.py --kernels-only
+    # --kernel-steps 4` at the default workload; profiles/traffic_rtm_480x480x380.md
+    traffic = {"stress": 5364710144 + 2976416000, "velocity": 6583469824 + 2632403968}
+    traffic_ok = (not args.grid and not args.small)
     step_ms = (ms_stress + ms_vel) / ks
     step_gbs = (bytes_k["stress"] + bytes_k["velocity"]) / (step_ms / 1e3) / 1e9
 
@@ -332,7 +337,8 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": f"k_{dom} (source pass)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "frac": round(achieved / peak, 4),
+                         "traffic": traffic[dom] if traffic_ok else None,
                          "peak_source": peak_src,
                          "bytes_per_cell": bytes_k[dom] // cells,
                          "kernel_ms": {k: round(v, 4) for k, v in t_k.items()},
