@@ -49,7 +49,8 @@ class _Config(C.Structure):
                 ("order", C.c_int), ("coef_kind", C.c_int), ("coef", C.c_float * 8),
                 ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_float),
                 ("pml_f0", C.c_float), ("pml_vmax", C.c_float), ("sponge_coef", C.c_float),
-                ("device", C.c_int), ("checkpoint_every", C.c_int), ("reserved", C.c_int * 6)]
+                ("device", C.c_int), ("checkpoint_every", C.c_int), ("autotune", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class _Shot(C.Structure):
@@ -58,6 +59,11 @@ class _Shot(C.Structure):
                 ("rx0", C.c_int), ("nrx", C.c_int), ("drx", C.c_int),
                 ("ry0", C.c_int), ("nry", C.c_int), ("dry", C.c_int),
                 ("rz", C.c_int), ("inject_mode", C.c_int)]
+
+
+class _Window(C.Structure):
+    _fields_ = [("x0", C.c_int), ("y0", C.c_int), ("wx", C.c_int), ("wy", C.c_int),
+                ("nt", C.c_int), ("src_steps", C.c_int)]
 
 
 # every entry point of include/ertm.h: name -> (restype, argtypes)
@@ -69,6 +75,10 @@ SIGNATURES = {
     "ertm_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "ertm_set_stream": (C.c_int, [_P, _P]),
     "ertm_set_model": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "ertm_set_grid": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "ertm_rtm_windows": (C.c_int, [C.POINTER(_Config), _P, _P, _P, C.c_int, C.POINTER(_Window),
+                                   C.POINTER(_Shot), C.POINTER(_P), C.c_int, _P, _P, _P,
+                                   C.c_char_p, C.c_size_t]),
     "ertm_forward_together_using_real_model": (C.c_int, [_P, C.POINTER(_Shot), _P]),
     "ertm_forward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot)]),
     "ertm_backward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
@@ -127,12 +137,13 @@ class Config:
     sponge_coef: float = 0.0
     device: int = 0
     checkpoint_every: int = 0
+    autotune: int = 0
 
     def struct(self) -> _Config:
         c = _Config()
         for f in ("nx", "ny", "nz", "dx", "dy", "dz", "dt_ms", "nt", "src_steps", "order",
                   "coef_kind", "boundary", "pml_r", "pml_f0", "pml_vmax", "sponge_coef", "device",
-                  "checkpoint_every"):
+                  "checkpoint_every", "autotune"):
             setattr(c, f, getattr(self, f))
         for i, v in enumerate(self.coef[:8]):
             c.coef[i] = v
@@ -257,6 +268,12 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None):
         self._ck(self._L.ertm_set_stream(self._h, stream_ptr))
+
+    def set_grid(self, nx: int, ny: int, nt: int, src_steps: int = 0):
+        """Shrink (or restore) the active grid; models must be set again afterwards."""
+        self._ck(self._L.ertm_set_grid(self._h, nx, ny, nt, src_steps))
+        self.cfg = Config(**{**self.cfg.__dict__, "nx": nx, "ny": ny, "nt": nt,
+                             "src_steps": src_steps})
 
     def set_model(self, which: int, vp, vs, rho):
         n = self.ncell
@@ -389,3 +406,48 @@ def forward_together_using_real_model_noalloc(cfg: Config, vp, vs, rho, shot: Sh
     if rc != 0:
         raise ErtmError(rc, buf.value.decode(errors="replace"))
     return out
+
+
+@dataclass
+class Window:
+    """Mirror of ertm_window: aperture of one shot over a shared model (model cells)."""
+    x0: int
+    y0: int
+    wx: int
+    wy: int
+    nt: int
+    src_steps: int = 0
+
+    def struct(self) -> _Window:
+        w = _Window()
+        w.x0, w.y0, w.wx, w.wy, w.nt, w.src_steps = (self.x0, self.y0, self.wx, self.wy, self.nt,
+                                                      self.src_steps)
+        return w
+
+
+def rtm_windows(base: Config, vp, vs, rho, windows: list, shots: list, data: list, lanes: int = 2,
+                pp=None, ps=None, tp=None):
+    """Batched RTM over aperture windows of one shared migration model (model cells,
+    no absorbing layers, shape (nz, ny, nx) = base.shape); images stacked into
+    pp, ps, tp of the model's shape.  See ertm_rtm_windows in include/ertm.h."""
+    L = lib()
+    n = base.nx * base.ny * base.nz
+    outs = [np.zeros(base.shape, np.float32) if o is None else o for o in (pp, ps, tp)]
+    model = [a if _is_torch(a) else np.ascontiguousarray(a, np.float32) for a in (vp, vs, rho)]
+    k = max(1, len(shots))
+    warr, sarr, parr = (_Window * k)(), (_Shot * k)(), (C.c_void_p * k)()
+    keep = []
+    for q, (w, sh, d) in enumerate(zip(windows, shots, data)):
+        warr[q] = w.struct()
+        sarr[q] = sh.struct()
+        d = d if _is_torch(d) else np.ascontiguousarray(d, np.float32)
+        keep.append(d)
+        parr[q] = _ptr(d, 3 * w.nt * sh.nrec)
+    cs = base.struct()
+    buf = C.create_string_buffer(1024)
+    rc = L.ertm_rtm_windows(C.byref(cs), *[_ptr(a, n) for a in model], len(shots), warr, sarr, parr,
+                            lanes, *[_ptr(o, n, True) for o in outs], buf, len(buf))
+    del keep
+    if rc != 0:
+        raise ErtmError(rc, buf.value.decode(errors="replace"))
+    return tuple(outs)

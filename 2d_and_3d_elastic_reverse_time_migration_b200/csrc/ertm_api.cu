@@ -15,7 +15,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "ertm.h"
@@ -42,6 +45,7 @@ struct ertm_ctx {
     ertm_config cfg{};
     int R = 4;
     Geom g{};
+    int cap_nx = 0, cap_ny = 0;      // grid the buffers were allocated for (ertm_set_grid)
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -62,6 +66,7 @@ struct ertm_ctx {
     float* psi[NPSI] = {nullptr};
     long long psi_n[NPSI] = {0};
     float profile_vmax = -1.f;
+    bool att_ready = false;
 
     // excitation and images (padded)
     float* ex_amp2_base = nullptr;
@@ -177,7 +182,8 @@ int alloc_volume(ertm_ctx* c, float** base, float** origin)
 int ensure_stage(ertm_ctx* c)
 {
     if (c->stage) return ERTM_OK;
-    long long n = (long long)c->g.nx * c->g.ny * c->g.nz;
+    // sized for the allocated grid: ertm_set_grid may enlarge the active one later
+    long long n = (long long)c->cap_nx * c->cap_ny * c->g.nz;
     CK(c, cudaMalloc(&c->stage, sizeof(float) * 3 * n));
     return ERTM_OK;
 }
@@ -227,8 +233,9 @@ int upload_profiles(ertm_ctx* c, float vmax)
                     a[i] = (float)(d * (bb - 1.0) / (d + al));
                 }
                 if (!c->pa[ax][h]) {
-                    CK(c, cudaMalloc(&c->pa[ax][h], sizeof(float) * n));
-                    CK(c, cudaMalloc(&c->pb[ax][h], sizeof(float) * n));
+                    const int cap = ax == 0 ? c->cap_nx : ax == 1 ? c->cap_ny : g.nz;
+                    CK(c, cudaMalloc(&c->pa[ax][h], sizeof(float) * cap));
+                    CK(c, cudaMalloc(&c->pb[ax][h], sizeof(float) * cap));
                 }
                 CK(c, cudaMemcpyAsync(c->pa[ax][h], a.data(), sizeof(float) * n,
                                       cudaMemcpyHostToDevice, c->stream));
@@ -240,7 +247,7 @@ int upload_profiles(ertm_ctx* c, float vmax)
         c->profile_vmax = vmax;
         return ERTM_OK;
     }
-    if (c->att[0]) return ERTM_OK;
+    if (c->att_ready) return ERTM_OK;
     const double pai = 3.1415926;   // 3D_zzzzz:1
     for (int ax = 0; ax < 3; ax++) {
         int n = ns[ax];
@@ -272,11 +279,15 @@ int upload_profiles(ertm_ctx* c, float vmax)
                 v[i] += val;
             }
         }
-        CK(c, cudaMalloc(&c->att[ax], sizeof(float) * n));
+        if (!c->att[ax]) {
+            const int cap = ax == 0 ? c->cap_nx : ax == 1 ? c->cap_ny : g.nz;
+            CK(c, cudaMalloc(&c->att[ax], sizeof(float) * cap));
+        }
         CK(c, cudaMemcpyAsync(c->att[ax], v.data(), sizeof(float) * n, cudaMemcpyHostToDevice,
                               c->stream));
     }
     CK(c, cudaStreamSynchronize(c->stream));
+    c->att_ready = true;
     return ERTM_OK;
 }
 
@@ -528,6 +539,14 @@ int check_device_error(ertm_ctx* c)
     return ERTM_OK;
 }
 
+// floats of C-PML memory-variable slot p on the active grid g
+long long psi_count(const Geom& g, const ertm_config& c, int p)
+{
+    const int ax = kPsiAxis[p];
+    const long long w = c.pml[2 * ax] + c.pml[2 * ax + 1];
+    return ax == 0 ? (long long)g.nz * g.ny * w : ax == 1 ? (long long)g.nz * w * g.nx : w * g.ny * g.nx;
+}
+
 // z planes per CTA.  3D: chunks of about 32 planes, balanced over nz.  Timed on
 // B200 at 480 x 480 x 380 (R = 4, C-PML), the step kernels get faster as the
 // chunk shrinks from the whole column (380 planes) down to 32-48 planes
@@ -562,6 +581,83 @@ int choose_kchunk(const ertm_ctx* c)
     return best;
 }
 
+// Z-chunk autotuner (ertm_config.autotune = 1).  For each grid shape, stencil
+// radius, boundary kind and device it times the plain step (stress + velocity,
+// no source, no epilogue) for a few steps at every candidate chunk and keeps the
+// fastest; the result is cached for the life of the process.  It runs before a
+// pass resets the wavefields, so the trial steps leave no trace.
+struct TuneKey {
+    int device, nx, ny, nz, R, cpml;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(device, nx, ny, nz, R, cpml) < std::tie(o.device, o.nx, o.ny, o.nz, o.R, o.cpml);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tuned;
+
+int autotune_kchunk(ertm_ctx* c, int which, int* out)
+{
+    const Geom& g = c->g;
+    const bool cpml = c->cfg.boundary == ERTM_BOUNDARY_CPML;
+    const TuneKey key{c->device, g.nx, g.ny, g.nz, c->R, cpml ? 1 : 0};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            *out = it->second;
+            return ERTM_OK;
+        }
+    }
+    std::vector<int> cand;
+    const int base[] = {16, 24, 32, 48, 64, 96, 128};
+    for (int v : base)
+        if (v < g.nz) cand.push_back(v);
+    cand.push_back(g.nz);
+    KArgs a;
+    fill_args(c, which, nullptr, a);
+    a.traces = nullptr;
+    a.wavelet = nullptr;
+    CK(c, launch_set_int(c->it_d, 0, c->stream));   // the kernels read the step index
+    const StressMaps sm = stress_maps(c, which);
+    const VelMaps vm = vel_maps(c, which, EPI_NONE);
+    cudaEvent_t e0, e1;
+    CK(c, cudaEventCreate(&e0));
+    CK(c, cudaEventCreate(&e1));
+    int best = cand.back();
+    float best_ms = 1e30f;
+    cudaError_t e = cudaSuccess;
+    for (int kc : cand) {
+        a.kchunk = kc;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+            if (rep == 1) e = cudaEventRecord(e0, c->stream);
+            if (e == cudaSuccess) e = launch_stress(c->R, g, a, sm, cpml, false, c->stream);
+            if (e == cudaSuccess) e = launch_velocity(c->R, g, a, vm, cpml, EPI_NONE, false, c->stream);
+            c->launches += 2;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kc;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "autotune: %s", cudaGetErrorString(e));
+    int rc = check_device_error(c);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[key] = best;
+    }
+    *out = best;
+    return ERTM_OK;
+}
+
 int reset_state(ertm_ctx* c)
 {
     for (int q = 0; q < NFIELD; q++)
@@ -593,11 +689,13 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
     int rc;
     float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[which];
     if ((rc = upload_profiles(c, vmax))) return rc;
+    int kchunk = choose_kchunk(c);
+    if (c->cfg.autotune == 1 && (rc = autotune_kchunk(c, which, &kchunk))) return rc;
     if ((rc = reset_state(c))) return rc;
     if (mode != MODE_RECEIVER && (rc = upload_wavelet(c, s))) return rc;
     KArgs a;
     fill_args(c, which, s, a);
-    a.kchunk = choose_kchunk(c);
+    a.kchunk = kchunk;
     a.traces = traces;
     const bool cpml = c->cfg.boundary == ERTM_BOUNDARY_CPML;
     const int R = c->R;
@@ -709,8 +807,9 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     }
     if (c.src_steps < 0 || c.src_steps > c.nt)
         return fail(nullptr, ERTM_EINVAL, "src_steps %d outside [0, nt]", c.src_steps);
-    for (int q = 0; q < 6; q++)
+    for (int q = 0; q < 5; q++)
         if (c.reserved[q]) return fail(nullptr, ERTM_EINVAL, "reserved fields must be zero");
+    if (c.autotune != 0 && c.autotune != 1) return fail(nullptr, ERTM_EINVAL, "autotune %d", c.autotune);
     if (c.checkpoint_every < 0) return fail(nullptr, ERTM_EINVAL, "checkpoint_every < 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -772,15 +871,13 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
         if (!field_used(x->g, q)) continue;
         if ((rc = alloc_volume(x, &x->f_base[q], &x->f[q]))) return bail(rc);
     }
+    x->cap_nx = c.nx;
+    x->cap_ny = c.ny;
     if (c.boundary == ERTM_BOUNDARY_CPML) {
         const Geom& g = x->g;
         for (int p = 0; p < NPSI; p++) {
             if (g.two_d && !kPsi2D[p]) continue;
-            int ax = kPsiAxis[p];
-            long long w = c.pml[2 * ax] + c.pml[2 * ax + 1];
-            long long n = ax == 0 ? (long long)g.nz * g.ny * w
-                        : ax == 1 ? (long long)g.nz * w * g.nx
-                                  : w * g.ny * g.nx;
+            const long long n = psi_count(g, c, p);
             x->psi_n[p] = n;
             if (n == 0) continue;
             if (cudaMalloc(&x->psi[p], sizeof(float) * n) != cudaSuccess) {
@@ -793,6 +890,7 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     if (cudaMalloc(&x->it_d, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&x->vmax_d, sizeof(float)) != cudaSuccess ||
         cudaMalloc(&x->err_d, sizeof(int)) != cudaSuccess ||
+        cudaMemsetAsync(x->it_d, 0, sizeof(int), x->stream) != cudaSuccess ||
         cudaMemsetAsync(x->err_d, 0, sizeof(int), x->stream) != cudaSuccess) {
         cudaGetLastError();
         fail(x, ERTM_ENOMEM, "counters");
@@ -859,6 +957,39 @@ int ertm_set_stream(ertm_ctx* c, void* stream)
     if (!c) return ERTM_EINVAL;
     CK(c, cudaStreamSynchronize(c->stream));
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return ERTM_OK;
+}
+
+int ertm_set_grid(ertm_ctx* c, int nx, int ny, int nt, int src_steps)
+{
+    if (!c) return ERTM_EINVAL;
+    if (nx < 1 || ny < 1 || nx > c->cap_nx || ny > c->cap_ny)
+        return fail(c, ERTM_EINVAL, "active grid %dx%d outside the allocated %dx%d", nx, ny, c->cap_nx,
+                    c->cap_ny);
+    if (c->g.two_d && ny != 1) return fail(c, ERTM_EINVAL, "2D context: ny must be 1");
+    if (nt < 1 || src_steps < 0 || src_steps > nt)
+        return fail(c, ERTM_EINVAL, "nt = %d, src_steps = %d", nt, src_steps);
+    const int ns[2] = {nx, ny};
+    for (int ax = 0; ax < 2; ax++) {
+        if (ax == 1 && c->g.two_d) continue;
+        if (c->cfg.pml[2 * ax] + c->cfg.pml[2 * ax + 1] > ns[ax])
+            return fail(c, ERTM_EINVAL, "absorbing widths exceed the active grid on axis %d", ax);
+    }
+    CK(c, cudaSetDevice(c->device));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->g.nx = nx;
+    c->g.ny = ny;
+    c->cfg.nx = nx;
+    c->cfg.ny = ny;
+    c->cfg.nt = nt;
+    c->cfg.src_steps = src_steps;
+    for (int p = 0; p < NPSI; p++)
+        if (c->psi[p]) c->psi_n[p] = psi_count(c->g, c->cfg, p);
+    c->profile_vmax = -1.f;
+    c->att_ready = false;
+    c->model_set[0] = c->model_set[1] = false;
+    c->have_excitation = false;
+    c->born.ready = false;
     return ERTM_OK;
 }
 
@@ -1187,6 +1318,14 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
     const Geom& g = c->g;
     int rc;
     if (!B.ready) {
+        if (B.block) {   // the active grid changed (ertm_set_grid): size everything afresh
+            CK(c, cudaStreamSynchronize(c->stream));
+            cudaFree(B.block);
+            cudaFree(B.ckpt);
+            cudaFree(B.hist);
+            B.block = B.ckpt = B.hist = nullptr;
+            B.nck = B.K = 0;
+        }
         B.px = round_up(2LL * BXH + round_up(g.nx, 32), 32);
         B.n = B.px * (g.nz + 2LL * c->R);
         // one block so that consecutive volumes (the 5 background fields of a

@@ -219,8 +219,9 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     const long long sy = a.sy, sz = a.sz;
     const bool act = (i < a.nx) && (j < a.ny);
     const int it = __ldg(a.it_ptr);
-    const bool src_here = (it < a.nw) && (i == a.ssx) && (j == a.ssy);
-    const float wsrc = (it < a.nw) ? __ldg(a.wavelet + it) : 0.f;
+    const bool src_on = (it >= 0) && (it < a.nw);
+    const bool src_here = src_on && (i == a.ssx) && (j == a.ssy);
+    const float wsrc = src_on ? __ldg(a.wavelet + it) : 0.f;
     const int cell = ty * TX + tx;
     // padded-volume coordinates of the tile
     const int gx = i0 + XH, gy = j0 + (Y ? R : 0), gz0 = k0 + R;

@@ -94,7 +94,9 @@ typedef struct {
     float sponge_coef;       /* reference coe_attenuation (sponge kinds) */
     int   device;            /* CUDA device ordinal */
     int   checkpoint_every;  /* Born adjoint: background checkpoint interval; 0 -> 200 */
-    int   reserved[6];       /* must be zero */
+    int   autotune;          /* 1: time the z-chunk candidates of the step kernels once per
+                                grid shape (cached for the process); 0: fixed rule */
+    int   reserved[5];       /* must be zero */
 } ertm_config;
 
 typedef struct {
@@ -106,6 +108,14 @@ typedef struct {
     int rz;                  /* receiver depth index (receiver_start_z) */
     int inject_mode;         /* ERTM_INJECT_*, receiver pass; 0 -> ADD */
 } ertm_shot;
+
+/* Aperture window of one shot over a shared model (ertm_rtm_windows). */
+typedef struct {
+    int x0, y0;              /* window origin, model cells (no absorbing layers) */
+    int wx, wy;              /* window size, model cells; wy = 1, y0 = 0 in 2D */
+    int nt;                  /* record length of this shot, steps */
+    int src_steps;           /* source-pass steps; 0 -> 2*nt/3 */
+} ertm_window;
 
 /* ---- lifecycle --------------------------------------------------------- */
 
@@ -119,6 +129,35 @@ int ertm_last_error(const ertm_ctx *ctx, char *buf, size_t len);
 /* Use the caller's cudaStream_t (NULL restores the context's own stream). */
 int ertm_set_stream(ertm_ctx *ctx, void *cuda_stream);
 int ertm_abi_version(void);
+
+/* Shrink (or restore) the active grid of a context to nx x ny x cfg.nz cells,
+ * nx <= cfg.nx and ny <= cfg.ny of ertm_create, with record length nt and
+ * source-pass length src_steps (0 -> 2*nt/3).  The buffers stay allocated at the
+ * create-time size; models, excitation and Born state are dropped (set the
+ * models again).  No counterpart in the reference, whose buffers are sized once
+ * per run (allocate_typedef_struct); it lets one context serve shots on
+ * aperture windows of different sizes without reallocating. */
+int ertm_set_grid(ertm_ctx *ctx, int nx, int ny, int nt, int src_steps);
+
+/* Batched RTM over aperture windows of one shared migration model.
+ * No single counterpart in the reference, which migrates one shot per run on
+ * the full grid and writes one image per shot (3D_output_file.cu:339-365).
+ *  base     spacings, dt, order, coefficients, boundary, absorbing widths and
+ *           device of every window grid; base->nx, ny, nz are the shared model's
+ *           size WITHOUT absorbing layers; base->nt, src_steps are ignored.
+ *  vp,vs,rho  the shared migration model, nz*ny*nx floats (host or device).
+ *  win[i], shots[i]  window and shot i.  Source and receiver cells are given in
+ *           model cells; each window grid is the model cropped to the window,
+ *           all depths, extended by the absorbing layers with edge values.
+ *  data[i]  observed data of shot i, [3][win[i].nt][nrx*nry] (host or device).
+ *  lanes    shots in flight at once (one context, stream and host thread each,
+ *           sized for the largest window).
+ *  stack_*  nz*ny*nx sums of the windows' PP / PS / TP images (host or device;
+ *           NULL skips one).  errbuf receives a message on failure. */
+int ertm_rtm_windows(const ertm_config *base, const float *vp, const float *vs, const float *rho,
+                     int nshots, const ertm_window *win, const ertm_shot *shots,
+                     const float *const *data, int lanes, float *stack_pp, float *stack_ps,
+                     float *stack_tp, char *errbuf, size_t errlen);
 
 /* Load a model: which = 0 true model (velocity/velocity1/density),
  * which = 1 migration model (s_velocity/s_velocity1/s_density).

@@ -51,3 +51,21 @@ def test_create_without_gpu_fails_cleanly(ertm):
 def test_null_out_pointer(ertm):
     cfg = ertm.Config(nx=40, ny=1, nz=40, dx=5, dy=5, dz=5, dt_ms=0.5, nt=10).struct()
     assert ertm.lib().ertm_create(C.byref(cfg), None) == -1
+
+
+def test_windows_are_validated_before_touching_a_device(ertm):
+    import numpy as np
+    base = ertm.Config(nx=40, ny=30, nz=20, dx=10, dy=10, dz=10, dt_ms=0.8, nt=1,
+                       pml=(5, 5, 5, 5, 5, 5))
+    m = np.ones((20, 30, 40), np.float32)
+    w = np.zeros(8, np.float32)
+    cases = [
+        (ertm.Window(30, 0, 20, 10, 10), ertm.Shot(35, 5, 2, wavelet=w, nrx=1)),   # past x edge
+        (ertm.Window(0, 0, 10, 10, 10), ertm.Shot(15, 5, 2, wavelet=w, nrx=1)),    # source outside
+        (ertm.Window(0, 0, 10, 10, 0), ertm.Shot(5, 5, 2, wavelet=w, nrx=1)),      # nt = 0
+    ]
+    for win, sh in cases:
+        d = np.zeros((3, win.nt, 1), np.float32)
+        with pytest.raises(ertm.ErtmError) as ei:
+            ertm.rtm_windows(base, m, m, m, [win], [sh], [d], lanes=1)
+        assert ei.value.code == -1 and str(ei.value)
