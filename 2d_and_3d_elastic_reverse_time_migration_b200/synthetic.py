@@ -171,3 +171,30 @@ def layered_3d(n_interior=(300, 400, 400), h: float = 10.0, pml: int = 40, nt: i
     return Workload(f"3d-layered-ellipsoid-{nx}x{ny}x{nz}", vp.shape, h, h, h, dt_ms, nt, pml,
                     vp, vs, rho, svp, svs, srho, 10.0, (nx // 2, ny // 2, sz),
                     dict(rx0=pml, nrx=nrx, drx=rec_every, ry0=pml, nry=nry, dry=rec_every, rz=sz))
+
+
+def windows_3d(nshots: int = 64, seed: int = BASE_SEED + 3, n_interior=(200, 256, 256),
+               wmin: int = 64, wmax: int = 192, ntmin: int = 2000, ntmax: int = 3500,
+               pml: int = 40, rec_every: int = 2, smooth_sigma: float = 8.0):
+    """Batched-window workload: a shared 256 x 256 x 200 model at 10 m (layered plus
+    ellipsoid, generated as `layered_3d`) and `nshots` seeded shots, each on its own
+    aperture window of wx x wy ~ U[wmin, wmax] cells centred on a random source
+    position (shifted to fit the model), nt ~ U[ntmin, ntmax] at 0.8 ms, 10 Hz Ricker
+    at 20 m depth and receivers every `rec_every` cells over the window.  Returns
+    (migration model (vp, vs, rho), windows as dicts, shots as dicts); the absorbing
+    frame of `pml` cells is added around every window by the batched driver."""
+    wl = layered_3d(n_interior=n_interior, pml=0, nt=1, smooth_sigma=smooth_sigma)
+    nz, ny, nx = n_interior
+    rng = np.random.default_rng(seed)
+    wins, shots = [], []
+    for _ in range(nshots):
+        wx, wy = (int(v) for v in rng.integers(wmin, wmax + 1, size=2))
+        cx, cy = int(rng.integers(0, nx)), int(rng.integers(0, ny))
+        x0 = min(max(cx - wx // 2, 0), nx - wx)
+        y0 = min(max(cy - wy // 2, 0), ny - wy)
+        nt = int(rng.integers(ntmin, ntmax + 1))
+        wins.append(dict(x0=x0, y0=y0, wx=wx, wy=wy, nt=nt))
+        shots.append(dict(sx=min(max(cx, x0), x0 + wx - 1), sy=min(max(cy, y0), y0 + wy - 1), sz=2,
+                          rx0=x0, nrx=(wx + rec_every - 1) // rec_every, drx=rec_every,
+                          ry0=y0, nry=(wy + rec_every - 1) // rec_every, dry=rec_every, rz=2))
+    return (wl.svp, wl.svs, wl.srho), wins, shots
