@@ -670,23 +670,67 @@ typedef struct {
     int nx, nz, R;
     long px, pz, n;            /* padded extents (R halo on every side) */
     real c[8], dt, ix, iz;
-    real *M, *U, *L, *B, *g1, *g2;
+    real *M, *U, *B, *g1, *g2; /* relaxed moduli pi = rho vp^2, mu = rho vs^2; buoyancy; damping */
+    int nm;                    /* relaxation mechanisms (0: elastic) */
+    real ra[3], rb[3];         /* memory-variable update r' = ra r + rb f */
+    real tp, ts;               /* GSLS strengths of the P and S moduli */
+    real kp, ks;               /* 1 + nm tp, 1 + nm ts: unrelaxed / relaxed */
 } born2d;
 
 #define B2(S, i, k) (((long)(k) + (S)->R) * (S)->px + (i) + (S)->R)
+
+/* GSLS fit (tau method, first order in tau): relaxation frequencies
+ * f_l = f0 10^(2 (l + 1/2) / nmech - 1) (log-spaced over about two decades
+ * around f0), tau_sigma = 1 / (2 pi f_l); Q^-1(w) ~ tau S(w) with
+ * S(w) = sum_l w tau_sigma / (1 + w^2 tau_sigma^2), fitted in least squares to a
+ * constant 1/q at 32 log-spaced frequencies in [f0/4, 4 f0]:
+ * tau = (1/q) sum S / sum S^2. */
+void orc_visco_fit(int nmech, double qp, double qs, double f0, double *tau_sigma, double *tau_p,
+                   double *tau_s)
+{
+    const double pi = 3.14159265358979323846;
+    if (nmech < 1 || nmech > 3 || !(f0 > 0)) { *tau_p = *tau_s = 0; return; }
+    for (int l = 0; l < nmech; l++) {
+        double fl = f0 * pow(10.0, 2.0 * (l + 0.5) / nmech - 1.0);
+        tau_sigma[l] = 1.0 / (2.0 * pi * fl);
+    }
+    double s1 = 0, s2 = 0;
+    for (int j = 0; j < 32; j++) {
+        double f = f0 / 4.0 * pow(16.0, j / 31.0), w = 2.0 * pi * f, S = 0;
+        for (int l = 0; l < nmech; l++) S += w * tau_sigma[l] / (1.0 + w * w * tau_sigma[l] * tau_sigma[l]);
+        s1 += S;
+        s2 += S * S;
+    }
+    *tau_p = qp > 0 ? (1.0 / qp) * s1 / s2 : 0.0;
+    *tau_s = qs > 0 ? (1.0 / qs) * s1 / s2 : 0.0;
+}
 
 static int born_setup(born2d *S, const orc_grid *g, const float *vp, const float *vs,
                       const float *rho)
 {
     if (g->ny != 1 || g->boundary == ORC_BOUNDARY_CPML) return -1;
+    if (g->visco_nmech < 0 || g->visco_nmech > 3) return -1;
     memset(S, 0, sizeof *S);
     S->nx = g->nx; S->nz = g->nz; S->R = g->R;
     S->px = g->nx + 2L * g->R; S->pz = g->nz + 2L * g->R; S->n = S->px * S->pz;
     for (int q = 0; q <= g->R; q++) S->c[q] = (real)g->coef[q];
     S->dt = (real)(g->dt_ms / 1000.0);
     S->ix = (real)(1.0 / g->dx); S->iz = (real)(1.0 / g->dz);
-    real **arr[6] = {&S->M, &S->U, &S->L, &S->B, &S->g1, &S->g2};
-    for (int q = 0; q < 6; q++) if (!(*arr[q] = zalloc(S->n))) return -2;
+    S->nm = g->visco_nmech;
+    S->kp = S->ks = 1;
+    if (S->nm > 0) {
+        double ts[3], tp, tsh;
+        orc_visco_fit(S->nm, g->visco_qp, g->visco_qs, g->visco_f0, ts, &tp, &tsh);
+        S->tp = (real)tp; S->ts = (real)tsh;
+        S->kp = 1 + S->nm * S->tp; S->ks = 1 + S->nm * S->ts;
+        for (int l = 0; l < S->nm; l++) {
+            double h = g->dt_ms / 1000.0 / (2.0 * ts[l]);
+            S->ra[l] = (real)((1.0 - h) / (1.0 + h));
+            S->rb[l] = (real)(-2.0 * h / (1.0 + h));
+        }
+    }
+    real **arr[5] = {&S->M, &S->U, &S->B, &S->g1, &S->g2};
+    for (int q = 0; q < 5; q++) if (!(*arr[q] = zalloc(S->n))) return -2;
     double *px = (double *)malloc(sizeof(double) * g->nx), *pz = (double *)malloc(sizeof(double) * g->nz);
     if (!px || !pz) { free(px); free(pz); return -2; }
     orc_sponge_profile(g->boundary, g->nx, g->pml[0], g->pml[1], g->sponge_coef, px);
@@ -695,7 +739,7 @@ static int born_setup(born2d *S, const orc_grid *g, const float *vp, const float
         for (int i = 0; i < g->nx; i++) {
             long c = B2(S, i, k), m = (long)k * g->nx + i;
             real r = rho[m], p = vp[m], s = vs[m];
-            S->M[c] = r * p * p; S->U[c] = r * s * s; S->L[c] = S->M[c] - 2 * S->U[c]; S->B[c] = 1 / r;
+            S->M[c] = r * p * p; S->U[c] = r * s * s; S->B[c] = 1 / r;
             real a = (real)((float)pz[k] + (float)px[i]) * S->dt / 2;
             S->g1[c] = 1 / (1 + a); S->g2[c] = 1 - a;
         }
@@ -705,7 +749,7 @@ static int born_setup(born2d *S, const orc_grid *g, const float *vp, const float
 
 static void born_free(born2d *S)
 {
-    free(S->M); free(S->U); free(S->L); free(S->B); free(S->g1); free(S->g2);
+    free(S->M); free(S->U); free(S->B); free(S->g1); free(S->g2);
 }
 
 static real b_dpx(const born2d *S, const real *f, long c) { return dplus(f, c, 1, S->c, S->R) * S->ix; }
@@ -716,41 +760,82 @@ static real b_dmz(const born2d *S, const real *f, long c) { return dminus(f, c, 
 static void born_sources(real dm, real du, real rr, real e0xx, real e0zz, real e0xz, real a0x,
                          real a0z, real dt, real *sxx, real *szz, real *sxz, real *svx, real *svz);
 
-/* one step of background (+ scattered when dM != NULL); stores v0 (start of
- * step) and a0 into keep[4] when keep != NULL */
-static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, real *v0z, real *s0xx,
-                      real *s0zz, real *s0xz, real *vx, real *vz, real *sxx, real *szz, real *sxz,
-                      const real *dM, const real *dU, const real *rr, real **keep)
+/* isotropic combination of strain rates with moduli (m, u):
+ * (m exx + (m-2u) ezz, m ezz + (m-2u) exx, u exz) */
+static void iso(real m, real u, real exx, real ezz, real exz, real *o)
+{
+    o[0] = m * exx + (m - 2 * u) * ezz;
+    o[1] = m * ezz + (m - 2 * u) * exx;
+    o[2] = u * exz;
+}
+
+/* 2D state of one wavefield: velocities, stresses, memory variables r[comp][mech] */
+typedef struct {
+    real *vx, *vz, *sxx, *szz, *sxz;
+    real *r[3][3];
+} bstate;
+
+/* one step of background (+ scattered when sc != NULL).  Stress with GSLS memory
+ * variables (Crank-Nicolson decay, updated before the stress uses them):
+ *   r_l' = ra_l r_l + rb_l f(e),  f = iso(pi tp, mu ts; e)
+ *   sigma' = g1 (g2 sigma + dt (iso(pi kp, mu ks; e) + sum_l r_l'))
+ * Scattered: the same with secondary sources iso(dpi kp, dmu ks; e0) in the stress
+ * and iso(dpi tp, dmu ts; e0) in f, and -dt r_rho a0 in the velocity.  Stores v0
+ * (start of step) and a0 into keep[4] when keep != NULL. */
+static void born_step(const born2d *S, const orc_shot *s, int it, bstate *bg, bstate *sc,
+                      const real *dpi, const real *dmu, const real *rr, real **keep)
 {
     const real dt = S->dt;
+    const int nm = S->nm;
     if (it < s->nw) {
         long c = B2(S, s->sx, s->sz);
-        s0xx[c] += s->wavelet[it];
-        s0zz[c] += s->wavelet[it];
+        bg->sxx[c] += s->wavelet[it];
+        bg->szz[c] += s->wavelet[it];
     }
     if (keep) {
-        memcpy(keep[0], v0x, sizeof(real) * S->n);
-        memcpy(keep[1], v0z, sizeof(real) * S->n);
+        memcpy(keep[0], bg->vx, sizeof(real) * S->n);
+        memcpy(keep[1], bg->vz, sizeof(real) * S->n);
     }
+    real *bs[3] = {bg->sxx, bg->szz, bg->sxz};
+    real *ss[3] = {sc ? sc->sxx : NULL, sc ? sc->szz : NULL, sc ? sc->sxz : NULL};
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < S->nz; k++)
         for (int i = 0; i < S->nx; i++) {
             long c = B2(S, i, k);
-            real e0xx = b_dpx(S, v0x, c), e0zz = b_dmz(S, v0z, c);
-            real e0xz = b_dpz(S, v0x, c) + b_dmx(S, v0z, c);
-            real g1 = S->g1[c], g2 = S->g2[c], M = S->M[c], L = S->L[c], U = S->U[c];
-            s0xx[c] = g1 * (g2 * s0xx[c] + dt * (M * e0xx + L * e0zz));
-            s0zz[c] = g1 * (g2 * s0zz[c] + dt * (M * e0zz + L * e0xx));
-            s0xz[c] = g1 * (g2 * s0xz[c] + dt * U * e0xz);
-            if (dM) {
-                real exx = b_dpx(S, vx, c), ezz = b_dmz(S, vz, c);
-                real exz = b_dpz(S, vx, c) + b_dmx(S, vz, c);
-                real qxx, qzz, qxz, unused0, unused1;
-                born_sources(dM[c], dU[c], 0, e0xx, e0zz, e0xz, 0, 0, dt, &qxx, &qzz, &qxz, &unused0,
-                             &unused1);
-                sxx[c] = g1 * (g2 * sxx[c] + dt * (M * exx + L * ezz) + qxx);
-                szz[c] = g1 * (g2 * szz[c] + dt * (M * ezz + L * exx) + qzz);
-                sxz[c] = g1 * (g2 * sxz[c] + dt * U * exz + qxz);
+            real e0xx = b_dpx(S, bg->vx, c), e0zz = b_dmz(S, bg->vz, c);
+            real e0xz = b_dpz(S, bg->vx, c) + b_dmx(S, bg->vz, c);
+            real g1 = S->g1[c], g2 = S->g2[c], pi = S->M[c], mu = S->U[c];
+            real E0[3], F0[3];
+            iso(pi * S->kp, mu * S->ks, e0xx, e0zz, e0xz, E0);
+            iso(pi * S->tp, mu * S->ts, e0xx, e0zz, e0xz, F0);
+            for (int q = 0; q < 3; q++) {
+                real sum = 0;
+                for (int l = 0; l < nm; l++) {
+                    real *r = bg->r[q][l];
+                    r[c] = S->ra[l] * r[c] + S->rb[l] * F0[q];
+                    sum += r[c];
+                }
+                bs[q][c] = g1 * (g2 * bs[q][c] + dt * (E0[q] + sum));
+            }
+            if (sc) {
+                real exx = b_dpx(S, sc->vx, c), ezz = b_dmz(S, sc->vz, c);
+                real exz = b_dpz(S, sc->vx, c) + b_dmx(S, sc->vz, c);
+                real E[3], F[3], dE[3], dF[3], unused0, unused1;
+                iso(pi * S->kp, mu * S->ks, exx, ezz, exz, E);
+                iso(pi * S->tp, mu * S->ts, exx, ezz, exz, F);
+                /* the reference's stress sources (dem_p), scaled by the GSLS strengths */
+                born_sources(dpi[c] * S->kp, dmu[c] * S->ks, 0, e0xx, e0zz, e0xz, 0, 0, 1, &dE[0],
+                             &dE[1], &dE[2], &unused0, &unused1);
+                iso(dpi[c] * S->tp, dmu[c] * S->ts, e0xx, e0zz, e0xz, dF);
+                for (int q = 0; q < 3; q++) {
+                    real sum = 0;
+                    for (int l = 0; l < nm; l++) {
+                        real *r = sc->r[q][l];
+                        r[c] = S->ra[l] * r[c] + S->rb[l] * (F[q] + dF[q]);
+                        sum += r[c];
+                    }
+                    ss[q][c] = g1 * (g2 * ss[q][c] + dt * (E[q] + dE[q] + sum));
+                }
             }
         }
 #pragma omp parallel for schedule(static)
@@ -758,18 +843,18 @@ static void born_step(const born2d *S, const orc_shot *s, int it, real *v0x, rea
         for (int i = 0; i < S->nx; i++) {
             long c = B2(S, i, k);
             real g1 = S->g1[c], g2 = S->g2[c], b = S->B[c];
-            real a0x = b * (b_dmx(S, s0xx, c) + b_dmz(S, s0xz, c));
-            real a0z = b * (b_dpx(S, s0xz, c) + b_dpz(S, s0zz, c));
+            real a0x = b * (b_dmx(S, bg->sxx, c) + b_dmz(S, bg->sxz, c));
+            real a0z = b * (b_dpx(S, bg->sxz, c) + b_dpz(S, bg->szz, c));
             if (keep) { keep[2][c] = a0x; keep[3][c] = a0z; }
-            v0x[c] = g1 * (g2 * v0x[c] + dt * a0x);
-            v0z[c] = g1 * (g2 * v0z[c] + dt * a0z);
-            if (dM) {
-                real ax = b * (b_dmx(S, sxx, c) + b_dmz(S, sxz, c));
-                real az = b * (b_dpx(S, sxz, c) + b_dpz(S, szz, c));
+            bg->vx[c] = g1 * (g2 * bg->vx[c] + dt * a0x);
+            bg->vz[c] = g1 * (g2 * bg->vz[c] + dt * a0z);
+            if (sc) {
+                real ax = b * (b_dmx(S, sc->sxx, c) + b_dmz(S, sc->sxz, c));
+                real az = b * (b_dpx(S, sc->sxz, c) + b_dpz(S, sc->szz, c));
                 real q0, q1, q2, svx, svz;
                 born_sources(0, 0, rr[c], 0, 0, 0, a0x, a0z, dt, &q0, &q1, &q2, &svx, &svz);
-                vx[c] = g1 * (g2 * vx[c] + dt * ax + svx);
-                vz[c] = g1 * (g2 * vz[c] + dt * az + svz);
+                sc->vx[c] = g1 * (g2 * sc->vx[c] + dt * ax + svx);
+                sc->vz[c] = g1 * (g2 * sc->vz[c] + dt * az + svz);
             }
         }
 }
@@ -797,6 +882,25 @@ static int born_rec(const born2d *S, const orc_shot *s, int r, long *c)
     return 1;
 }
 
+/* allocate a zeroed state (memory variables for S->nm mechanisms) */
+static int bstate_new(const born2d *S, bstate *b)
+{
+    memset(b, 0, sizeof *b);
+    real **f[5] = {&b->vx, &b->vz, &b->sxx, &b->szz, &b->sxz};
+    int bad = 0;
+    for (int q = 0; q < 5; q++) if (!(*f[q] = zalloc(S->n))) bad = 1;
+    for (int q = 0; q < 3; q++)
+        for (int l = 0; l < S->nm; l++) if (!(b->r[q][l] = zalloc(S->n))) bad = 1;
+    return bad ? -2 : 0;
+}
+
+static void bstate_free(bstate *b)
+{
+    free(b->vx); free(b->vz); free(b->sxx); free(b->szz); free(b->sxz);
+    for (int q = 0; q < 3; q++)
+        for (int l = 0; l < 3; l++) free(b->r[q][l]);
+}
+
 int orc_born_forward(const orc_grid *g, const float *vp, const float *vs, const float *rho,
                      const orc_shot *s, int nt, const float *r_vp, const float *r_vs,
                      const float *r_rho, float *data)
@@ -805,31 +909,63 @@ int orc_born_forward(const orc_grid *g, const float *vp, const float *vs, const 
     if (!s || !data || nt < 1 || s->nry != 1) return -1;
     int rc = born_setup(&S, g, vp, vs, rho);
     if (rc) { born_free(&S); return rc; }
-    real *f[13];
-    for (int q = 0; q < 13; q++) if (!(f[q] = zalloc(S.n))) { rc = -2; }
+    bstate bg, sc;
+    real *dpi = zalloc(S.n), *dmu = zalloc(S.n), *rr = zalloc(S.n);
+    rc = bstate_new(&S, &bg);
+    if (!rc) rc = bstate_new(&S, &sc);
+    if (!dpi || !dmu || !rr) rc = -2;
     if (!rc) {
-        real *dM = f[10], *dU = f[11], *rr = f[12];
         for (int k = 0; k < S.nz; k++)
             for (int i = 0; i < S.nx; i++) {
                 long c = B2(&S, i, k), m = (long)k * S.nx + i;
-                dM[c] = S.M[c] * ((real)r_rho[m] + 2 * (real)r_vp[m]);
-                dU[c] = S.U[c] * ((real)r_rho[m] + 2 * (real)r_vs[m]);
+                dpi[c] = S.M[c] * ((real)r_rho[m] + 2 * (real)r_vp[m]);
+                dmu[c] = S.U[c] * ((real)r_rho[m] + 2 * (real)r_vs[m]);
                 rr[c] = r_rho[m];
             }
         const long nrec = s->nrx;
         memset(data, 0, sizeof(float) * 3 * (size_t)nt * nrec);
         for (int it = 0; it < nt; it++) {
-            born_step(&S, s, it, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], dM, dU,
-                      rr, NULL);
+            born_step(&S, s, it, &bg, &sc, dpi, dmu, rr, NULL);
             for (long r = 0; r < nrec; r++) {
                 long c;
                 if (!born_rec(&S, s, (int)r, &c)) continue;
-                data[((long)0 * nt + it) * nrec + r] = (float)f[5][c];
-                data[((long)2 * nt + it) * nrec + r] = (float)f[6][c];
+                data[((long)0 * nt + it) * nrec + r] = (float)sc.vx[c];
+                data[((long)2 * nt + it) * nrec + r] = (float)sc.vz[c];
             }
         }
     }
-    for (int q = 0; q < 13; q++) free(f[q]);
+    bstate_free(&bg); bstate_free(&sc);
+    free(dpi); free(dmu); free(rr);
+    born_free(&S);
+    return rc;
+}
+
+/* Modelling pass of the Born background scheme (2D, sponge, GSLS memory
+ * variables when g->visco_nmech > 0): records vx, vz at the receivers after
+ * every step into data[3][nt][nrx] (vy row zero). */
+int orc_visco_model(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                    const orc_shot *s, int nt, float *data)
+{
+    born2d S;
+    if (!s || !data || nt < 1 || s->nry != 1) return -1;
+    int rc = born_setup(&S, g, vp, vs, rho);
+    if (rc) { born_free(&S); return rc; }
+    bstate bg;
+    rc = bstate_new(&S, &bg);
+    if (!rc) {
+        const long nrec = s->nrx;
+        memset(data, 0, sizeof(float) * 3 * (size_t)nt * nrec);
+        for (int it = 0; it < nt; it++) {
+            born_step(&S, s, it, &bg, NULL, NULL, NULL, NULL, NULL);
+            for (long r = 0; r < nrec; r++) {
+                long c;
+                if (!born_rec(&S, s, (int)r, &c)) continue;
+                data[((long)0 * nt + it) * nrec + r] = (float)bg.vx[c];
+                data[((long)2 * nt + it) * nrec + r] = (float)bg.vz[c];
+            }
+        }
+    }
+    bstate_free(&bg);
     born_free(&S);
     return rc;
 }
@@ -843,27 +979,28 @@ int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const 
     int rc = born_setup(&S, g, vp, vs, rho);
     if (rc) { born_free(&S); return rc; }
     const long n = S.n;
+    const int nm = S.nm;
     /* background history: v0 at the start of every step and a0 of every step */
     real *hist = (real *)malloc(sizeof(real) * (size_t)4 * n * nt);
-    real *w[16];
-    for (int q = 0; q < 16; q++) w[q] = zalloc(n);
-    for (int q = 0; q < 16; q++) if (!w[q]) rc = -2;
+    bstate bg;
+    rc = bstate_new(&S, &bg);
+    real *w[14], *lr[3][3] = {{0}};
+    for (int q = 0; q < 14; q++) if (!(w[q] = zalloc(n))) rc = -2;
+    for (int q = 0; q < 3; q++)
+        for (int l = 0; l < nm; l++) if (!(lr[q][l] = zalloc(n))) rc = -2;
     if (!hist) rc = -2;
     if (!rc) {
-        real *v0x = w[0], *v0z = w[1], *s0xx = w[2], *s0zz = w[3], *s0xz = w[4];
         for (int it = 0; it < nt; it++) {
             real *keep[4] = {hist + (4L * it + 0) * n, hist + (4L * it + 1) * n,
                              hist + (4L * it + 2) * n, hist + (4L * it + 3) * n};
-            born_step(&S, s, it, v0x, v0z, s0xx, s0zz, s0xz, NULL, NULL, NULL, NULL, NULL, NULL,
-                      NULL, NULL, keep);
+            born_step(&S, s, it, &bg, NULL, NULL, NULL, NULL, keep);
         }
-        real *ax = w[5], *az = w[6], *hxx = w[7], *hzz = w[8], *hxz = w[9];
-        real *gM = w[10], *gL = w[11], *gU = w[12], *gR = w[13], *tx = w[14], *tz = w[15];
-        for (long q = 0; q < n; q++) ax[q] = az[q] = hxx[q] = hzz[q] = hxz[q] = 0;
+        real *ax = w[0], *az = w[1], *hxx = w[2], *hzz = w[3], *hxz = w[4];
+        real *gP = w[5], *gU = w[6], *gR = w[7], *tx = w[8], *tz = w[9];
+        real *Sxx = w[10], *Szz = w[11], *Sxz = w[12], *Qb = w[13];
+        (void)Qb;
         const long nrec = s->nrx;
         const real dt = S.dt;
-        real *Qxx = (real *)calloc(n, sizeof(real)), *Qzz = (real *)calloc(n, sizeof(real));
-        real *Qxz = (real *)calloc(n, sizeof(real));
         for (int it = nt - 1; it >= 0; it--) {
             const real *hv0x = hist + (4L * it + 0) * n, *hv0z = hist + (4L * it + 1) * n;
             const real *ha0x = hist + (4L * it + 2) * n, *ha0z = hist + (4L * it + 3) * n;
@@ -888,49 +1025,60 @@ int orc_born_adjoint(const orc_grid *g, const float *vp, const float *vs, const 
                     hxz[c] += -dt * (b_dpz(&S, tx, c) + b_dmx(&S, tz, c));
                     hzz[c] += -dt * b_dmz(&S, tz, c);
                 }
-            /* stress update^T */
-            for (long q = 0; q < n; q++) {
-                real g1 = S.g1[q];
-                Qxx[q] = g1 * hxx[q]; Qzz[q] = g1 * hzz[q]; Qxz[q] = g1 * hxz[q];
-                tx[q] = S.M[q] * Qxx[q] + S.L[q] * Qzz[q];     /* reused as M Qxx + L Qzz */
-                tz[q] = S.L[q] * Qxx[q] + S.M[q] * Qzz[q];     /* L Qxx + M Qzz */
-            }
-            real *uq = hxx;                                    /* U Qxz, written after use */
+            /* stress and memory-variable update^T: Q = g1 h is the adjoint of the
+             * bracket; Lambda_l = lr_l + dt Q that of r_l'; P = sum_l rb_l Lambda_l
+             * that of f; the strain adjoint S = dt E^T Q + F^T P */
 #pragma omp parallel for schedule(static)
             for (int k = 0; k < S.nz; k++)
                 for (int i = 0; i < S.nx; i++) {
                     long c = B2(&S, i, k);
+                    real g1 = S.g1[c], pi = S.M[c], mu = S.U[c];
+                    real Q[3] = {g1 * hxx[c], g1 * hzz[c], g1 * hxz[c]}, P[3] = {0, 0, 0};
+                    for (int q = 0; q < 3; q++)
+                        for (int l = 0; l < nm; l++) {
+                            real lam = lr[q][l][c] + dt * Q[q];
+                            P[q] += S.rb[l] * lam;
+                            lr[q][l][c] = S.ra[l] * lam;
+                        }
                     real e0xx = b_dpx(&S, hv0x, c), e0zz = b_dmz(&S, hv0z, c);
                     real e0xz = b_dpz(&S, hv0x, c) + b_dmx(&S, hv0z, c);
-                    gM[c] += dt * (Qxx[c] * e0xx + Qzz[c] * e0zz);
-                    gL[c] += dt * (Qxx[c] * e0zz + Qzz[c] * e0xx);
-                    gU[c] += dt * Qxz[c] * e0xz;
+                    real div0 = e0xx + e0zz;
+                    real tq = dt * Q[0], tz_ = dt * Q[1], tx_ = dt * Q[2];
+                    gP[c] += (S.kp * (tq + tz_) + S.tp * (P[0] + P[1])) * div0;
+                    gU[c] += S.ks * (-2 * tq * e0zz - 2 * tz_ * e0xx + tx_ * e0xz) +
+                             S.ts * (-2 * P[0] * e0zz - 2 * P[1] * e0xx + P[2] * e0xz);
+                    real E[3], F[3];
+                    /* E^T and F^T are symmetric in (xx, zz): iso() gives them */
+                    iso(pi * S.kp, mu * S.ks, tq, tz_, tx_, E);
+                    iso(pi * S.tp, mu * S.ts, P[0], P[1], P[2], F);
+                    Sxx[c] = E[0] + F[0];
+                    Szz[c] = E[1] + F[1];
+                    Sxz[c] = E[2] + F[2];
+                    hxx[c] = S.g2[c] * Q[0];
+                    hzz[c] = S.g2[c] * Q[1];
+                    hxz[c] = S.g2[c] * Q[2];
                 }
-            for (long q = 0; q < n; q++) uq[q] = S.U[q] * Qxz[q];
 #pragma omp parallel for schedule(static)
             for (int k = 0; k < S.nz; k++)
                 for (int i = 0; i < S.nx; i++) {
                     long c = B2(&S, i, k);
                     real g12 = S.g2[c] * S.g1[c];
-                    ax[c] = g12 * ax[c] - dt * (b_dmx(&S, tx, c) + b_dmz(&S, uq, c));
-                    az[c] = g12 * az[c] - dt * (b_dpz(&S, tz, c) + b_dpx(&S, uq, c));
+                    ax[c] = g12 * ax[c] - (b_dmx(&S, Sxx, c) + b_dmz(&S, Sxz, c));
+                    az[c] = g12 * az[c] - (b_dpz(&S, Szz, c) + b_dpx(&S, Sxz, c));
                 }
-            for (long q = 0; q < n; q++) {
-                real g2 = S.g2[q];
-                hxx[q] = g2 * Qxx[q]; hzz[q] = g2 * Qzz[q]; hxz[q] = g2 * Qxz[q];
-            }
         }
         for (int k = 0; k < S.nz; k++)
             for (int i = 0; i < S.nx; i++) {
                 long c = B2(&S, i, k), m = (long)k * S.nx + i;
-                real gm = gM[c] + gL[c], gu = gU[c] - 2 * gL[c];
-                g_vp[m] = (float)(2 * S.M[c] * gm);
-                g_vs[m] = (float)(2 * S.U[c] * gu);
-                g_rho[m] = (float)(S.M[c] * gm + S.U[c] * gu + gR[c]);
+                g_vp[m] = (float)(2 * S.M[c] * gP[c]);
+                g_vs[m] = (float)(2 * S.U[c] * gU[c]);
+                g_rho[m] = (float)(S.M[c] * gP[c] + S.U[c] * gU[c] + gR[c]);
             }
-        free(Qxx); free(Qzz); free(Qxz);
     }
-    for (int q = 0; q < 16; q++) free(w[q]);
+    for (int q = 0; q < 14; q++) free(w[q]);
+    for (int q = 0; q < 3; q++)
+        for (int l = 0; l < 3; l++) free(lr[q][l]);
+    bstate_free(&bg);
     free(hist);
     born_free(&S);
     return rc;

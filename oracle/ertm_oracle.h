@@ -52,7 +52,14 @@ typedef struct {
     double pml_f0;           /* CPML alpha frequency (Hz) */
     double pml_vmax;         /* CPML reference velocity (m/s) */
     double sponge_coef;      /* reference `coe_attenuation` */
+    int visco_nmech;         /* Born operators: relaxation mechanisms (0 elastic, 1..3 GSLS) */
+    double visco_qp, visco_qs, visco_f0;   /* constant Q targets and reference frequency (Hz) */
 } orc_grid;
+
+/* GSLS relaxation of `nmech` mechanisms fitted to constant qp, qs around f0
+ * (tau method, first order): tau_sigma[l] and the P and S strengths. */
+void orc_visco_fit(int nmech, double qp, double qs, double f0, double *tau_sigma, double *tau_p,
+                   double *tau_s);
 
 typedef struct {
     int sx, sy, sz;          /* explosive source cell */
@@ -121,6 +128,10 @@ int orc_divcurl(const orc_grid *g, const float *vp, const float *vs,
  * born_forward records vx, vz of the scattered field into data[3][nt][nrec].
  * born_adjoint applies the exact transpose of born_forward to `residual`
  * ([3][nt][nrec]) and returns the gradients w.r.t. r_vp, r_vs, r_rho. */
+/* Modelling pass of the Born background scheme (2D, sponge; viscoelastic when
+ * g->visco_nmech > 0): data[3][nt][nrx] of vx, (0), vz after every step. */
+int orc_visco_model(const orc_grid *g, const float *vp, const float *vs, const float *rho,
+                    const orc_shot *s, int nt, float *data);
 int orc_born_forward(const orc_grid *g, const float *vp, const float *vs, const float *rho,
                      const orc_shot *s, int nt, const float *r_vp, const float *r_vs,
                      const float *r_rho, float *data);

@@ -29,7 +29,8 @@ class Grid(C.Structure):
                 ("dt_ms", C.c_double), ("R", C.c_int), ("coef", C.c_double * 8),
                 ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_double),
                 ("pml_f0", C.c_double), ("pml_vmax", C.c_double),
-                ("sponge_coef", C.c_double)]
+                ("sponge_coef", C.c_double), ("visco_nmech", C.c_int), ("visco_qp", C.c_double),
+                ("visco_qs", C.c_double), ("visco_f0", C.c_double)]
 
 
 class Shot(C.Structure):
@@ -92,6 +93,10 @@ def lib(bits: int = 64) -> C.CDLL:
         L.orc_born_sources_given.restype = C.c_int
         L.orc_image_given.argtypes = [C.c_long] + [f] * 8
         L.orc_image_given.restype = C.c_int
+        L.orc_visco_model.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f]
+        L.orc_visco_model.restype = C.c_int
+        L.orc_visco_fit.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, P(C.c_double),
+                                    P(C.c_double), P(C.c_double)]
         L.orc_threads.restype = C.c_int
         L.orc_real_size.restype = C.c_int
         _libs[bits] = L
@@ -139,7 +144,8 @@ def cpml_profile(n, w0, w1, h, dt_s, vmax, rc, f0, stagger):
 
 
 def make_grid(nx, ny, nz, dx, dy, dz, dt_ms, R=4, coef=None, boundary=CPML, pml=(0,) * 6,
-              pml_r=1e-3, pml_f0=10.0, pml_vmax=4000.0, sponge_coef=0.0) -> Grid:
+              pml_r=1e-3, pml_f0=10.0, pml_vmax=4000.0, sponge_coef=0.0, visco=None) -> Grid:
+    """visco: None (elastic) or (nmech, qp, qs, f0) for the Born operators."""
     g = Grid()
     g.nx, g.ny, g.nz = nx, ny, nz
     g.dx, g.dy, g.dz = dx, dy, dz
@@ -152,7 +158,16 @@ def make_grid(nx, ny, nz, dx, dy, dz, dt_ms, R=4, coef=None, boundary=CPML, pml=
     for i in range(6):
         g.pml[i] = int(pml[i])
     g.pml_r, g.pml_f0, g.pml_vmax, g.sponge_coef = pml_r, pml_f0, pml_vmax, sponge_coef
+    if visco:
+        g.visco_nmech, g.visco_qp, g.visco_qs, g.visco_f0 = visco
     return g
+
+
+def visco_fit(nmech, qp, qs, f0):
+    ts = (C.c_double * 3)()
+    tp, tsh = C.c_double(), C.c_double()
+    lib().orc_visco_fit(nmech, qp, qs, f0, ts, C.byref(tp), C.byref(tsh))
+    return np.array(ts[:nmech]), tp.value, tsh.value
 
 
 def make_shot(sx, sy, sz, wavelet, rx0=0, nrx=1, drx=1, ry0=0, nry=1, dry=1, rz=0,
@@ -280,3 +295,12 @@ def image_given(ex, ez, rpx, rpz, rsx, rsz):
     pp, ps = np.zeros(n, np.float32), np.zeros(n, np.float32)
     lib().orc_image_given(n, *[_fp(a) for a in ins], _fp(pp), _fp(ps))
     return pp, ps
+
+
+def visco_model(g: Grid, vp, vs, rho, shot: Shot, nt: int, bits=64):
+    """Data [3][nt][nrec] of the Born background scheme (2D; viscoelastic if g.visco_nmech)."""
+    data = np.zeros((3, nt, shot.nrx * shot.nry), np.float32)
+    rc = lib(bits).orc_visco_model(C.byref(g), _fp(vp), _fp(vs), _fp(rho), C.byref(shot), nt, _fp(data))
+    if rc != 0:
+        raise RuntimeError(f"orc_visco_model failed: {rc}")
+    return data

@@ -20,3 +20,13 @@ def born_case(orc, nz=50, nx=60, nt=250, R=4, seed=0):
 
 def oracle_shot(orc, c):
     return orc.make_shot(*c["geo"]["src"], c["w"], **c["geo"]["rec"])
+
+
+VISCO = (3, 100.0, 50.0, 15.0)   # GSLS-3, Qp 100, Qs 50, reference 15 Hz
+
+
+def visco_case(orc, **kw):
+    """The Born case with GSLS-3 attenuation (Qp 100, Qs 50 around 15 Hz)."""
+    c = born_case(orc, **kw)
+    c["g"].visco_nmech, c["g"].visco_qp, c["g"].visco_qs, c["g"].visco_f0 = VISCO
+    return c
