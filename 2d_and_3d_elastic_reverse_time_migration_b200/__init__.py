@@ -50,7 +50,8 @@ class _Config(C.Structure):
                 ("boundary", C.c_int), ("pml", C.c_int * 6), ("pml_r", C.c_float),
                 ("pml_f0", C.c_float), ("pml_vmax", C.c_float), ("sponge_coef", C.c_float),
                 ("device", C.c_int), ("checkpoint_every", C.c_int), ("autotune", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("visco_nmech", C.c_int), ("visco_qp", C.c_float), ("visco_qs", C.c_float),
+                ("visco_f0", C.c_float), ("reserved", C.c_int * 1)]
 
 
 class _Shot(C.Structure):
@@ -138,12 +139,17 @@ class Config:
     device: int = 0
     checkpoint_every: int = 0
     autotune: int = 0
+    visco_nmech: int = 0
+    visco_qp: float = 0.0
+    visco_qs: float = 0.0
+    visco_f0: float = 0.0
 
     def struct(self) -> _Config:
         c = _Config()
         for f in ("nx", "ny", "nz", "dx", "dy", "dz", "dt_ms", "nt", "src_steps", "order",
                   "coef_kind", "boundary", "pml_r", "pml_f0", "pml_vmax", "sponge_coef", "device",
-                  "checkpoint_every", "autotune"):
+                  "checkpoint_every", "autotune", "visco_nmech", "visco_qp", "visco_qs",
+                  "visco_f0"):
             setattr(c, f, getattr(self, f))
         for i, v in enumerate(self.coef[:8]):
             c.coef[i] = v

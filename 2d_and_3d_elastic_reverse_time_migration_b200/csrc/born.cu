@@ -1,4 +1,14 @@
-// Born (linearised) modelling and its exact adjoint, 2D elastic, sponge boundaries.
+// Born (linearised) modelling and its exact adjoint, 2D elastic or viscoelastic
+// (generalised standard linear solid, up to 3 mechanisms), sponge boundaries.
+//
+// Viscoelastic stress (a = attenuation strengths tp, ts of the tau method; pi =
+// rho vp^2, mu = rho vs^2 relaxed moduli; iso(m, u; e) = (m exx + (m-2u) ezz,
+// m ezz + (m-2u) exx, u exz)):
+//   r_l'   = ra_l r_l + rb_l iso(pi tp, mu ts; e)          (Crank-Nicolson decay)
+//   sigma' = g1 (g2 sigma + dt (iso(pi kp, mu ks; e) + sum_l r_l'))
+// with kp = 1 + nm tp, ks = 1 + nm ts (unrelaxed / relaxed); nm = 0 is elastic.
+// This is the reference's memory-variable update (fwd_txxzzxzpp_viscoelastic_and_memory,
+// 2D_elastic_RTM/viscoelastic_equation.cu:184-325, one mechanism) generalised to nm.
 //
 // The scattered field obeys the background scheme with secondary sources from
 // relative perturbations (r_vp, r_vs, r_rho) of the migration model:
@@ -126,33 +136,72 @@ __device__ __forceinline__ int recv_of(const BornArgs& a, int i, int k)
     return d < a.nrx ? d : -1;
 }
 
+__device__ __forceinline__ void iso(float m, float u, float exx, float ezz, float exz, float* o)
+{
+    const float l = m - 2.f * u;
+    o[0] = m * exx + l * ezz;
+    o[1] = m * ezz + l * exx;
+    o[2] = u * exz;
+}
+
 // ---- forward ---------------------------------------------------------------
-template <int R, bool BORN>
+template <int R, bool BORN, int NM>
 __global__ void k_born_stress(BornArgs a, int it)
 {
     int i, k;
     long long c;
     if (!cell_of(a, i, k, c)) return;
     const float dt = a.dt;
-    const float g1 = a.g1[c], g2 = a.g2[c], M = a.M[c], L = a.L[c], U = a.U[c];
+    const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
     const float e0xx = dpx<R>(a.v0x, c, a), e0zz = dmz<R>(a.v0z, c, a);
     const float e0xz = dpz<R>(a.v0x, c, a) + dmx<R>(a.v0z, c, a);
-    float oxx = a.s0xx[c], ozz = a.s0zz[c];
-    if (it < a.nw && i == a.ssx && k == a.ssz) {   // explosive source into the background
+    float o[3] = {a.s0xx[c], a.s0zz[c], a.s0xz[c]};
+    if (it >= 0 && it < a.nw && i == a.ssx && k == a.ssz) {   // explosive source into the background
         const float w = __ldg(a.wavelet + it);
-        oxx += w;
-        ozz += w;
+        o[0] += w;
+        o[1] += w;
     }
-    a.s0xx[c] = g1 * (g2 * oxx + dt * (M * e0xx + L * e0zz));
-    a.s0zz[c] = g1 * (g2 * ozz + dt * (M * e0zz + L * e0xx));
-    a.s0xz[c] = g1 * (g2 * a.s0xz[c] + dt * U * e0xz);
+    float E0[3], F0[3];
+    iso(pi * a.kp, mu * a.ks, e0xx, e0zz, e0xz, E0);
+    if (NM) iso(pi * a.tp, mu * a.ts, e0xx, e0zz, e0xz, F0);
+    float* s0[3] = {a.s0xx, a.s0zz, a.s0xz};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        float sum = 0.f;
+#pragma unroll
+        for (int l = 0; l < NM; l++) {
+            float* r = a.r0[q * 3 + l];
+            const float v = a.ra[l] * r[c] + a.rb[l] * F0[q];
+            r[c] = v;
+            sum += v;
+        }
+        s0[q][c] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
+    }
     if (BORN) {
         const float exx = dpx<R>(a.vx, c, a), ezz = dmz<R>(a.vz, c, a);
         const float exz = dpz<R>(a.vx, c, a) + dmx<R>(a.vz, c, a);
-        const float dm = a.dM[c], du = a.dU[c], dl = dm - 2.f * du;
-        a.sxx[c] = g1 * (g2 * a.sxx[c] + dt * (M * exx + L * ezz + dm * e0xx + dl * e0zz));
-        a.szz[c] = g1 * (g2 * a.szz[c] + dt * (M * ezz + L * exx + dm * e0zz + dl * e0xx));
-        a.sxz[c] = g1 * (g2 * a.sxz[c] + dt * (U * exz + du * e0xz));
+        const float dpi = a.dM[c], dmu = a.dU[c];
+        float E[3], dE[3], F[3], dF[3];
+        iso(pi * a.kp, mu * a.ks, exx, ezz, exz, E);
+        // the reference's stress sources (dem_p), scaled by the GSLS strengths
+        iso(dpi * a.kp, dmu * a.ks, e0xx, e0zz, e0xz, dE);
+        if (NM) {
+            iso(pi * a.tp, mu * a.ts, exx, ezz, exz, F);
+            iso(dpi * a.tp, dmu * a.ts, e0xx, e0zz, e0xz, dF);
+        }
+        float* sc[3] = {a.sxx, a.szz, a.sxz};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            float sum = 0.f;
+#pragma unroll
+            for (int l = 0; l < NM; l++) {
+                float* r = a.r[q * 3 + l];
+                const float v = a.ra[l] * r[c] + a.rb[l] * (F[q] + dF[q]);
+                r[c] = v;
+                sum += v;
+            }
+            sc[q][c] = g1 * (g2 * sc[q][c] + dt * (E[q] + dE[q] + sum));
+        }
     }
 }
 
@@ -208,6 +257,8 @@ __global__ void k_adj_inject(BornArgs a, int it)
     a.az[c] += d[2 * cs];
 }
 
+// velocity update^T: h (the stress adjoint, already carried through g2 g1 by
+// k_adj_mem) gains the velocity update's stencil transposed; rho gradient from a0
 template <int R>
 __global__ void k_adj_vel(BornArgs a)
 {
@@ -219,40 +270,69 @@ __global__ void k_adj_vel(BornArgs a)
     // rho gradient: -dt g1 (vx^ a0x + vz^ a0z)
     a.gR[c] += -dt * (g1 * a.ax[c] * __ldg(a.ha0x + c) + g1 * a.az[c] * __ldg(a.ha0z + c));
     const Prod2 tx{a.B, a.g1, a.ax}, tz{a.B, a.g1, a.az};
-    const float g12 = a.g2[c] * g1;
-    a.hxx[c] = g12 * a.hxx[c] - dt * tdpx<R>(tx, c, a);
-    a.hxz[c] = g12 * a.hxz[c] - dt * (tdpz<R>(tx, c, a) + tdmx<R>(tz, c, a));
-    a.hzz[c] = g12 * a.hzz[c] - dt * tdmz<R>(tz, c, a);
+    a.hxx[c] = a.hxx[c] - dt * tdpx<R>(tx, c, a);
+    a.hxz[c] = a.hxz[c] - dt * (tdpz<R>(tx, c, a) + tdmx<R>(tz, c, a));
+    a.hzz[c] = a.hzz[c] - dt * tdmz<R>(tz, c, a);
 }
 
+// stress and memory-variable update^T of one cell: Q = g1 h is the adjoint of
+// the stress bracket, Lambda_l = lr_l + dt Q that of r_l', P = sum_l rb_l Lambda_l
+// that of f; writes the strain adjoint S = iso(pi kp, mu ks; dt Q) + iso(pi tp,
+// mu ts; P) (both maps are symmetric), carries lr_l = ra_l Lambda_l and h = g2 Q,
+// and accumulates the pi and mu gradients from the background strain rates.
+template <int R, int NM>
+__global__ void k_adj_mem(BornArgs a)
+{
+    int i, k;
+    long long c;
+    if (!cell_of(a, i, k, c)) return;
+    const float dt = a.dt;
+    const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
+    const float Q[3] = {g1 * a.hxx[c], g1 * a.hzz[c], g1 * a.hxz[c]};
+    float P[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int l = 0; l < NM; l++) {
+            float* lr = a.lr[q * 3 + l];
+            const float lam = lr[c] + dt * Q[q];
+            P[q] += a.rb[l] * lam;
+            lr[c] = a.ra[l] * lam;
+        }
+    const float e0xx = dpx<R>(a.hv0x, c, a), e0zz = dmz<R>(a.hv0z, c, a);
+    const float e0xz = dpz<R>(a.hv0x, c, a) + dmx<R>(a.hv0z, c, a);
+    const float tq0 = dt * Q[0], tq1 = dt * Q[1], tq2 = dt * Q[2];
+    a.gM[c] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
+    a.gU[c] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
+               a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
+    float E[3], F[3] = {0.f, 0.f, 0.f};
+    iso(pi * a.kp, mu * a.ks, tq0, tq1, tq2, E);
+    if (NM) iso(pi * a.tp, mu * a.ts, P[0], P[1], P[2], F);
+    a.Sxx[c] = E[0] + F[0];
+    a.Szz[c] = E[1] + F[1];
+    a.Sxz[c] = E[2] + F[2];
+    a.hxx[c] = g2 * Q[0];
+    a.hzz[c] = g2 * Q[1];
+    a.hxz[c] = g2 * Q[2];
+}
+
+struct Load {
+    const float* p;
+    __device__ __forceinline__ float operator()(long long c) const { return p[c]; }
+};
+
+// velocity adjoint: a <- g2 g1 a (the velocity update^T) - D^T S (the stress
+// update's stencils transposed), plus the next (earlier) step's residual
 template <int R>
 __global__ void k_adj_str(BornArgs a, int it_next)
 {
     int i, k;
     long long c;
     if (!cell_of(a, i, k, c)) return;
-    const float dt = a.dt;
-    const float g1 = a.g1[c];
-    const float qxx = g1 * a.hxx[c], qzz = g1 * a.hzz[c], qxz = g1 * a.hxz[c];
-    const float e0xx = dpx<R>(a.hv0x, c, a), e0zz = dmz<R>(a.hv0z, c, a);
-    const float e0xz = dpz<R>(a.hv0x, c, a) + dmx<R>(a.hv0z, c, a);
-    a.gM[c] += dt * (qxx * e0xx + qzz * e0zz);
-    a.gL[c] += dt * (qxx * e0zz + qzz * e0xx);
-    a.gU[c] += dt * qxz * e0xz;
-    // neighbour products: M q_xx + L q_zz, L q_xx + M q_zz, U q_xz
-    auto mx = [&](long long e) {
-        const float ge = __ldg(a.g1 + e);
-        return __ldg(a.M + e) * ge * a.hxx[e] + __ldg(a.L + e) * ge * a.hzz[e];
-    };
-    auto mz = [&](long long e) {
-        const float ge = __ldg(a.g1 + e);
-        return __ldg(a.L + e) * ge * a.hxx[e] + __ldg(a.M + e) * ge * a.hzz[e];
-    };
-    auto ux = [&](long long e) { return __ldg(a.U + e) * __ldg(a.g1 + e) * a.hxz[e]; };
-    const float g12 = a.g2[c] * g1;
-    float nx = g12 * a.ax[c] - dt * (tdmx<R>(mx, c, a) + tdmz<R>(ux, c, a));
-    float nz = g12 * a.az[c] - dt * (tdpz<R>(mz, c, a) + tdpx<R>(ux, c, a));
-    // residual of the next (earlier) step, injected at the receivers
+    const float g12 = a.g2[c] * a.g1[c];
+    const Load sxx{a.Sxx}, szz{a.Szz}, sxz{a.Sxz};
+    float nx = g12 * a.ax[c] - (tdmx<R>(sxx, c, a) + tdmz<R>(sxz, c, a));
+    float nz = g12 * a.az[c] - (tdpz<R>(szz, c, a) + tdpx<R>(sxz, c, a));
     if (it_next >= 0) {
         const int rec = recv_of(a, i, k);
         if (rec >= 0) {
@@ -273,10 +353,10 @@ __global__ void k_born_final(BornArgs a, float* gvp, float* gvs, float* grho)
     long long c;
     if (!cell_of(a, i, k, c)) return;
     const long long m = (long long)k * a.nx + i;
-    const float gm = a.gM[c] + a.gL[c], gu = a.gU[c] - 2.f * a.gL[c];
-    gvp[m] = 2.f * a.M[c] * gm;
+    const float gp = a.gM[c], gu = a.gU[c];
+    gvp[m] = 2.f * a.M[c] * gp;
     gvs[m] = 2.f * a.U[c] * gu;
-    grho[m] = a.M[c] * gm + a.U[c] * gu + a.gR[c];
+    grho[m] = a.M[c] * gp + a.U[c] * gu + a.gR[c];
 }
 
 // model products (copied from the context's padded model, plane j = 0) and damping
@@ -331,36 +411,58 @@ cudaError_t born_launch_pert(const BornArgs& a, const float* rvp, const float* r
     return cudaGetLastError();
 }
 
-cudaError_t born_launch_step(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
+namespace {
+template <int R, int NM>
+void step_r(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
 {
     const dim3 g = born_grid(a), b(32, 8);
-    if (a.R == 4) {
-        if (born) k_born_stress<4, true><<<g, b, 0, s>>>(a, it);
-        else k_born_stress<4, false><<<g, b, 0, s>>>(a, it);
-        if (born) k_born_velocity<4, true, false><<<g, b, 0, s>>>(a, it);
-        else if (keep) k_born_velocity<4, false, true><<<g, b, 0, s>>>(a, it);
-        else k_born_velocity<4, false, false><<<g, b, 0, s>>>(a, it);
-    } else {
-        if (born) k_born_stress<6, true><<<g, b, 0, s>>>(a, it);
-        else k_born_stress<6, false><<<g, b, 0, s>>>(a, it);
-        if (born) k_born_velocity<6, true, false><<<g, b, 0, s>>>(a, it);
-        else if (keep) k_born_velocity<6, false, true><<<g, b, 0, s>>>(a, it);
-        else k_born_velocity<6, false, false><<<g, b, 0, s>>>(a, it);
+    if (born) k_born_stress<R, true, NM><<<g, b, 0, s>>>(a, it);
+    else k_born_stress<R, false, NM><<<g, b, 0, s>>>(a, it);
+    if (born) k_born_velocity<R, true, false><<<g, b, 0, s>>>(a, it);
+    else if (keep) k_born_velocity<R, false, true><<<g, b, 0, s>>>(a, it);
+    else k_born_velocity<R, false, false><<<g, b, 0, s>>>(a, it);
+}
+template <int R, int NM>
+void adj_r(const BornArgs& a, int it, cudaStream_t s)
+{
+    const dim3 g = born_grid(a), b(32, 8);
+    k_adj_vel<R><<<g, b, 0, s>>>(a);
+    k_adj_mem<R, NM><<<g, b, 0, s>>>(a);
+    k_adj_str<R><<<g, b, 0, s>>>(a, it - 1);
+}
+template <int R>
+void step_nm(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
+{
+    switch (a.nm) {
+    case 0: step_r<R, 0>(a, it, born, keep, s); break;
+    case 1: step_r<R, 1>(a, it, born, keep, s); break;
+    case 2: step_r<R, 2>(a, it, born, keep, s); break;
+    default: step_r<R, 3>(a, it, born, keep, s); break;
     }
+}
+template <int R>
+void adj_nm(const BornArgs& a, int it, cudaStream_t s)
+{
+    switch (a.nm) {
+    case 0: adj_r<R, 0>(a, it, s); break;
+    case 1: adj_r<R, 1>(a, it, s); break;
+    case 2: adj_r<R, 2>(a, it, s); break;
+    default: adj_r<R, 3>(a, it, s); break;
+    }
+}
+}  // namespace
+
+cudaError_t born_launch_step(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
+{
+    if (a.R == 4) step_nm<4>(a, it, born, keep, s);
+    else step_nm<6>(a, it, born, keep, s);
     return cudaGetLastError();
 }
 
 cudaError_t born_launch_adjoint_step(const BornArgs& a, int it, cudaStream_t s)
 {
-    const dim3 g = born_grid(a), b(32, 8);
-    const int it_next = it - 1;
-    if (a.R == 4) {
-        k_adj_vel<4><<<g, b, 0, s>>>(a);
-        k_adj_str<4><<<g, b, 0, s>>>(a, it_next);
-    } else {
-        k_adj_vel<6><<<g, b, 0, s>>>(a);
-        k_adj_str<6><<<g, b, 0, s>>>(a, it_next);
-    }
+    if (a.R == 4) adj_nm<4>(a, it, s);
+    else adj_nm<6>(a, it, s);
     return cudaGetLastError();
 }
 

@@ -1,4 +1,5 @@
-// Born modelling / adjoint kernels (2D, sponge boundaries): argument block and launchers.
+// Born modelling / adjoint kernels (2D, sponge boundaries, elastic or GSLS
+// viscoelastic): argument block and launchers.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -17,7 +18,14 @@ struct BornArgs {
     float *vx, *vz, *sxx, *szz, *sxz;      // scattered state
     const float *dM, *dU, *rr;             // perturbation products
     float *ax, *az, *hxx, *hzz, *hxz;      // adjoint state
-    float *gM, *gL, *gU, *gR;              // gradient accumulators
+    float *gM, *gL, *gU, *gR;              // gradient accumulators (pi, unused, mu, rho)
+    // GSLS attenuation (nm = 0: elastic): memory variables r[q*3 + l] of stress
+    // component q (xx, zz, xz) and mechanism l; r' = ra_l r + rb_l f
+    int nm;
+    float ra[3], rb[3];
+    float tp, ts, kp, ks;                  // strengths; kp = 1 + nm tp, ks = 1 + nm ts
+    float *r0[9], *r[9], *lr[9];           // background, scattered, adjoint memory variables
+    float *Sxx, *Szz, *Sxz;                // strain adjoint of the reverse step (scratch)
     const float *hv0x, *hv0z, *ha0x, *ha0z;// background history read by the adjoint step
     float *kv0x, *kv0z, *ka0x, *ka0z;      // history slot written by a recording step
     int ssx, ssz, nw;

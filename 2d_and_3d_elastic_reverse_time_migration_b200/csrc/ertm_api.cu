@@ -100,7 +100,7 @@ struct ertm_ctx {
         bool ready = false;
         long long px = 0, n = 0;          // pitch and floats per compact volume
         float* block = nullptr;           // one allocation holding every compact volume
-        float* vol[30] = {nullptr};       // M U L B g1 g2 | bg 5 | sc 5 | dM dU rr | adj 5 | grad 4
+        float* vol[64] = {nullptr};       // the BV_* volumes (BV_N of them)
         float* ckpt = nullptr;            // checkpoints: nck x 5 volumes
         int nck = 0;
         float* hist = nullptr;            // history: K x 4 volumes
@@ -807,8 +807,11 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     }
     if (c.src_steps < 0 || c.src_steps > c.nt)
         return fail(nullptr, ERTM_EINVAL, "src_steps %d outside [0, nt]", c.src_steps);
-    for (int q = 0; q < 5; q++)
-        if (c.reserved[q]) return fail(nullptr, ERTM_EINVAL, "reserved fields must be zero");
+    if (c.reserved[0]) return fail(nullptr, ERTM_EINVAL, "reserved fields must be zero");
+    if (c.visco_nmech < 0 || c.visco_nmech > 3)
+        return fail(nullptr, ERTM_EINVAL, "visco_nmech %d (0..3)", c.visco_nmech);
+    if (c.visco_nmech > 0 && !(c.visco_qp > 0 && c.visco_qs > 0 && c.visco_f0 > 0))
+        return fail(nullptr, ERTM_EINVAL, "viscoelastic Born needs positive visco_qp, visco_qs, visco_f0");
     if (c.autotune != 0 && c.autotune != 1) return fail(nullptr, ERTM_EINVAL, "autotune %d", c.autotune);
     if (c.checkpoint_every < 0) return fail(nullptr, ERTM_EINVAL, "checkpoint_every < 0");
     int ndev = 0;
@@ -1297,8 +1300,34 @@ int64_t ertm_kernel_launches(const ertm_ctx* c) { return c ? c->launches : 0; }
 // ---------------------------------------------------------------------------
 namespace {
 
-enum { BV_M, BV_U, BV_L, BV_B, BV_G1, BV_G2, BV_BG, BV_SC = BV_BG + 5, BV_DM = BV_SC + 5, BV_DU,
-       BV_RR, BV_ADJ, BV_GRAD = BV_ADJ + 5, BV_N = BV_GRAD + 4 };
+// compact volumes: model products; background state (5 fields + 9 memory
+// variables, contiguous so that a checkpoint is one copy); scattered state;
+// perturbation products; adjoint state, gradients, adjoint memory variables and
+// the strain-adjoint scratch
+enum { BV_M, BV_U, BV_L, BV_B, BV_G1, BV_G2, BV_BG, BV_R0 = BV_BG + 5, BV_SC = BV_R0 + 9,
+       BV_R = BV_SC + 5, BV_DM = BV_R + 9, BV_DU, BV_RR, BV_ADJ, BV_GRAD = BV_ADJ + 5,
+       BV_LR = BV_GRAD + 4, BV_S = BV_LR + 9, BV_N = BV_S + 3 };
+static_assert(BV_N <= 64, "BornState::vol holds 64 volumes");
+
+// GSLS fit (tau method, first order): relaxation frequencies
+// f_l = f0 10^(2 (l + 1/2) / nm - 1), tau_sigma = 1 / (2 pi f_l);
+// Q^-1(w) ~ tau S(w), S(w) = sum_l w tau_sigma / (1 + w^2 tau_sigma^2), fitted in
+// least squares to constant 1/q at 32 log-spaced frequencies in [f0/4, 4 f0]
+void visco_fit(int nm, double qp, double qs, double f0, double* tau_sigma, double* tp, double* ts)
+{
+    const double pi = 3.14159265358979323846;
+    for (int l = 0; l < nm; l++) tau_sigma[l] = 1.0 / (2.0 * pi * f0 * std::pow(10.0, 2.0 * (l + 0.5) / nm - 1.0));
+    double s1 = 0, s2 = 0;
+    for (int j = 0; j < 32; j++) {
+        const double w = 2.0 * pi * f0 / 4.0 * std::pow(16.0, j / 31.0);
+        double S = 0;
+        for (int l = 0; l < nm; l++) S += w * tau_sigma[l] / (1.0 + w * w * tau_sigma[l] * tau_sigma[l]);
+        s1 += S;
+        s2 += S * S;
+    }
+    *tp = (1.0 / qp) * s1 / s2;
+    *ts = (1.0 / qs) * s1 / s2;
+}
 
 int born_check(ertm_ctx* c, const ertm_shot* s)
 {
@@ -1328,8 +1357,8 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
         }
         B.px = round_up(2LL * BXH + round_up(g.nx, 32), 32);
         B.n = B.px * (g.nz + 2LL * c->R);
-        // one block so that consecutive volumes (the 5 background fields of a
-        // checkpoint) are contiguous
+        // one block so that consecutive volumes (the background fields and memory
+        // variables of a checkpoint) are contiguous
         CK(c, cudaMalloc(&B.block, sizeof(float) * B.n * BV_N));
         CK(c, cudaMemsetAsync(B.block, 0, sizeof(float) * B.n * BV_N, c->stream));
         for (int q = 0; q < BV_N; q++) B.vol[q] = B.block + (size_t)q * B.n;
@@ -1359,6 +1388,29 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
     a.dM = B.vol[BV_DM]; a.dU = B.vol[BV_DU]; a.rr = B.vol[BV_RR];
     a.gM = B.vol[BV_GRAD]; a.gL = B.vol[BV_GRAD + 1]; a.gU = B.vol[BV_GRAD + 2];
     a.gR = B.vol[BV_GRAD + 3];
+    for (int q = 0; q < 9; q++) {
+        a.r0[q] = B.vol[BV_R0 + q];
+        a.r[q] = B.vol[BV_R + q];
+        a.lr[q] = B.vol[BV_LR + q];
+    }
+    a.Sxx = B.vol[BV_S]; a.Szz = B.vol[BV_S + 1]; a.Sxz = B.vol[BV_S + 2];
+    a.nm = c->cfg.visco_nmech;
+    a.kp = a.ks = 1.f;
+    a.tp = a.ts = 0.f;
+    for (int l = 0; l < 3; l++) a.ra[l] = a.rb[l] = 0.f;
+    if (a.nm > 0) {
+        double tau[3], tp, ts;
+        visco_fit(a.nm, c->cfg.visco_qp, c->cfg.visco_qs, c->cfg.visco_f0, tau, &tp, &ts);
+        a.tp = (float)tp;
+        a.ts = (float)ts;
+        a.kp = (float)(1.0 + a.nm * tp);
+        a.ks = (float)(1.0 + a.nm * ts);
+        for (int l = 0; l < a.nm; l++) {
+            const double h = c->cfg.dt_ms / 1000.0 / (2.0 * tau[l]);
+            a.ra[l] = (float)((1.0 - h) / (1.0 + h));
+            a.rb[l] = (float)(-2.0 * h / (1.0 + h));
+        }
+    }
     a.nt = c->cfg.nt;
     CK(c, born_launch_model(a, c->m[1][0], c->m[1][1], c->m[1][2], g.sz, c->att[0], c->att[2],
                             B.vol[BV_M], B.vol[BV_U], B.vol[BV_L], B.vol[BV_B], B.vol[BV_G1],
@@ -1425,7 +1477,7 @@ int ertm_born_forward(ertm_ctx* c, const ertm_shot* s, const float* r_vp, const 
     if ((rc = born_stage_in(c, src, 3, dev))) return rc;
     CK(c, born_launch_pert(a, dev[0], dev[1], dev[2], c->born.vol[BV_DM], c->born.vol[BV_DU],
                            c->born.vol[BV_RR], c->stream));
-    if ((rc = born_zero(c, BV_BG, 10))) return rc;
+    if ((rc = born_zero(c, BV_BG, BV_DM - BV_BG))) return rc;   // background and scattered states
     const size_t nd = 3 * (size_t)c->cfg.nt * s->nrx;
     const bool dev_out = is_device_ptr(data_out);
     if (!dev_out && (rc = ensure_traces(c, nd))) return rc;
@@ -1455,10 +1507,11 @@ int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, fl
     const int nt = c->cfg.nt;
     const int K = std::min(nt, c->cfg.checkpoint_every > 0 ? c->cfg.checkpoint_every : 200);
     const int nck = (nt + K - 1) / K;
+    const int nbg = 5 + (a.nm ? 9 : 0);   // background volumes in a checkpoint
     if (B.nck < nck) {
         cudaFree(B.ckpt);
         B.ckpt = nullptr;
-        CK(c, cudaMalloc(&B.ckpt, sizeof(float) * 5 * B.n * nck));
+        CK(c, cudaMalloc(&B.ckpt, sizeof(float) * 14 * B.n * nck));
         B.nck = nck;
     }
     if (B.K < K) {
@@ -1476,19 +1529,19 @@ int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, fl
         a.traces = c->traces;
     }
     // 1. background forward, checkpointing its state every K steps
-    if ((rc = born_zero(c, BV_BG, 5))) return rc;
+    if ((rc = born_zero(c, BV_BG, 14))) return rc;
     for (int it = 0; it < nt; it++) {
         if (it % K == 0)
-            CK(c, cudaMemcpyAsync(B.ckpt + (size_t)(it / K) * 5 * B.n, B.vol[BV_BG],
-                                  sizeof(float) * 5 * B.n, cudaMemcpyDeviceToDevice, c->stream));
+            CK(c, cudaMemcpyAsync(B.ckpt + (size_t)(it / K) * nbg * B.n, B.vol[BV_BG],
+                                  sizeof(float) * nbg * B.n, cudaMemcpyDeviceToDevice, c->stream));
         CK(c, born_launch_step(a, it, false, false, c->stream));
     }
     // 2. reverse sweep, one checkpoint segment at a time
-    if ((rc = born_zero(c, BV_ADJ, 9))) return rc;
+    if ((rc = born_zero(c, BV_ADJ, BV_N - BV_ADJ))) return rc;   // adjoint, gradients, scratch
     CK(c, born_launch_inject(a, nt - 1, c->stream));
     for (int sg = nck - 1; sg >= 0; sg--) {
         const int t0 = sg * K, t1 = std::min(nt, t0 + K);
-        CK(c, cudaMemcpyAsync(B.vol[BV_BG], B.ckpt + (size_t)sg * 5 * B.n, sizeof(float) * 5 * B.n,
+        CK(c, cudaMemcpyAsync(B.vol[BV_BG], B.ckpt + (size_t)sg * nbg * B.n, sizeof(float) * nbg * B.n,
                               cudaMemcpyDeviceToDevice, c->stream));
         for (int it = t0; it < t1; it++) {
             float* h = B.hist + (size_t)(it - t0) * 4 * B.n;
@@ -1507,7 +1560,7 @@ int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, fl
             CK(c, born_launch_adjoint_step(a, it, c->stream));
         }
     }
-    c->launches += 2LL * nt * 2 + 2LL * nt + 2;
+    c->launches += 2LL * nt * 2 + 3LL * nt + 2;
     // 3. gradients w.r.t. the relative perturbations
     float* outs[3] = {g_vp, g_vs, g_rho};
     const long long n = (long long)c->g.nx * c->g.nz;

@@ -96,7 +96,10 @@ typedef struct {
     int   checkpoint_every;  /* Born adjoint: background checkpoint interval; 0 -> 200 */
     int   autotune;          /* 1: time the z-chunk candidates of the step kernels once per
                                 grid shape (cached for the process); 0: fixed rule */
-    int   reserved[5];       /* must be zero */
+    int   visco_nmech;       /* Born operators: GSLS relaxation mechanisms, 0 (elastic) .. 3 */
+    float visco_qp, visco_qs;  /* constant quality factors fitted by the mechanisms */
+    float visco_f0;          /* centre of the fitted band, Hz */
+    int   reserved[1];       /* must be zero */
 } ertm_config;
 
 typedef struct {

@@ -1,33 +1,35 @@
-"""CUDA Born operators against the oracle, adjointness in FP32, checkpoint independence."""
+"""CUDA Born operators (elastic and GSLS-3 viscoelastic) against the oracle, adjointness
+in FP32, checkpoint independence."""
 import numpy as np
 import pytest
 
-from _born_case import born_case, oracle_shot
+from _born_case import VISCO, born_case, oracle_shot, visco_case
 from _cases import rel
 
 pytestmark = pytest.mark.gpu
 
 
-def _ctx(ertm, c, K=0):
+def _ctx(ertm, c, K=0, visco=False):
     nz, _, nx = c["shape"]
+    v = dict(zip(("visco_nmech", "visco_qp", "visco_qs", "visco_f0"), VISCO)) if visco else {}
     cfg = ertm.Config(nx=nx, ny=1, nz=nz, dx=10, dy=10, dz=10, dt_ms=1.0, nt=c["nt"],
                       order=2 * c["R"], boundary=ertm.BOUNDARY_SPONGE_CUBIC, pml=c["pml"],
-                      sponge_coef=150.0, checkpoint_every=K)
+                      sponge_coef=150.0, checkpoint_every=K, **v)
     ctx = ertm.Context(cfg)
     ctx.set_model(ertm.MIGRATION_MODEL, c["vp"], c["vs"], c["rho"])
     shot = ertm.Shot(*c["geo"]["src"], wavelet=c["w"], **c["geo"]["rec"])
     return ctx, shot
 
 
-@pytest.mark.parametrize("R", [4, 6])
-def test_born_forward_and_adjoint_match_oracle(ertm, orc, R):
-    c = born_case(orc, R=R)
+@pytest.mark.parametrize("R,visco", [(4, False), (6, False), (4, True)])
+def test_born_forward_and_adjoint_match_oracle(ertm, orc, R, visco):
+    c = (visco_case if visco else born_case)(orc, R=R)
     s = oracle_shot(orc, c)
     rng = c["rng"]
     m = [(0.05 * rng.standard_normal(c["shape"])).astype(np.float32) for _ in range(3)]
     ref = orc.born_forward(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], *m)
     r32 = orc.born_forward(c["g"], c["vp"], c["vs"], c["rho"], s, c["nt"], *m, bits=32)
-    ctx, shot = _ctx(ertm, c, K=40)
+    ctx, shot = _ctx(ertm, c, K=40, visco=visco)
     gpu = ctx.born_forward(shot, *m)
     for q in (0, 2):
         assert rel(gpu[q], ref[q]) <= max(1e-5, 3 * rel(r32[q], ref[q])), q
@@ -40,11 +42,12 @@ def test_born_forward_and_adjoint_match_oracle(ertm, orc, R):
         assert rel(a, b) <= max(1e-5, 3 * rel(f, b))
 
 
-def test_gpu_dot_product_and_checkpoint_independence(ertm, orc):
+@pytest.mark.parametrize("visco", [False, True])
+def test_gpu_dot_product_and_checkpoint_independence(ertm, orc, visco):
     c = born_case(orc, nz=64, nx=80, nt=400)
     rng = c["rng"]
     m = [(0.05 * rng.standard_normal(c["shape"])).astype(np.float32) for _ in range(3)]
-    ctx, shot = _ctx(ertm, c, K=0)
+    ctx, shot = _ctx(ertm, c, K=0, visco=visco)
     d = ctx.born_forward(shot, *m)
     dh = rng.standard_normal(d.shape).astype(np.float32)
     dh[1] = 0
@@ -52,7 +55,7 @@ def test_gpu_dot_product_and_checkpoint_independence(ertm, orc):
     lhs = float(np.sum(d.astype(np.float64) * dh))
     rhs = sum(float(np.sum(a.astype(np.float64) * b)) for a, b in zip(m, g_default))
     assert abs(lhs - rhs) <= 1e-4 * abs(lhs), (lhs, rhs)
-    ctx7, shot7 = _ctx(ertm, c, K=7)
+    ctx7, shot7 = _ctx(ertm, c, K=7, visco=visco)
     g7 = ctx7.born_adjoint(shot7, dh)
     for a, b in zip(g7, g_default):
         assert np.array_equal(a, b)       # the rebuilt background is bit-identical

@@ -4,18 +4,20 @@ import importlib
 import numpy as np
 import pytest
 
-from _born_case import born_case
+from _born_case import VISCO, born_case
 
 pytestmark = pytest.mark.gpu
 
 
-def test_cgls_lowers_the_misfit_monotonically(ertm, orc):
+@pytest.mark.parametrize("visco", [False, True])
+def test_cgls_lowers_the_misfit_monotonically(ertm, orc, visco):
     lsrtm = importlib.import_module("2d_and_3d_elastic_reverse_time_migration_b200.lsrtm")
     c = born_case(orc, nz=60, nx=90, nt=350)
     nz, _, nx = c["shape"]
+    v = dict(zip(("visco_nmech", "visco_qp", "visco_qs", "visco_f0"), VISCO)) if visco else {}
     cfg = ertm.Config(nx=nx, ny=1, nz=nz, dx=10, dy=10, dz=10, dt_ms=1.0, nt=c["nt"],
                       order=8, boundary=ertm.BOUNDARY_SPONGE_CUBIC, pml=c["pml"],
-                      sponge_coef=150.0, checkpoint_every=50)
+                      sponge_coef=150.0, checkpoint_every=50, **v)
     ctx = ertm.Context(cfg)
     ctx.set_model(ertm.MIGRATION_MODEL, c["vp"], c["vs"], c["rho"])
     shots = [ertm.Shot(sx, 0, 12, wavelet=c["w"], rx0=10, nrx=nx - 20, rz=12)
