@@ -67,6 +67,11 @@ class _Window(C.Structure):
                 ("nt", C.c_int), ("src_steps", C.c_int)]
 
 
+class _NnAct(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("n", C.c_int), ("h", C.c_int), ("w", C.c_int),
+                ("cstride", C.c_int), ("coff", C.c_int), ("c", C.c_int)]
+
+
 # every entry point of include/ertm.h: name -> (restype, argtypes)
 _P = C.c_void_p
 SIGNATURES = {
@@ -93,6 +98,24 @@ SIGNATURES = {
     "ertm_kernel_launches": (C.c_int64, [_P]),
     "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_nn_gemm": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
+    "ertm_nn_conv3x3": (C.c_int, [C.POINTER(_NnAct), _P, _P, C.POINTER(_NnAct), C.c_int, _P, _P, _P]),
+    "ertm_nn_conv3x3_dgrad": (C.c_int, [C.POINTER(_NnAct), _P, C.POINTER(_NnAct), C.POINTER(_NnAct),
+                                        _P, _P]),
+    "ertm_nn_conv3x3_wgrad": (C.c_int, [C.POINTER(_NnAct), C.POINTER(_NnAct), _P, C.c_int, _P, _P]),
+    "ertm_nn_up2": (C.c_int, [C.POINTER(_NnAct), _P, _P, C.POINTER(_NnAct), C.c_int, _P, _P]),
+    "ertm_nn_up2_dgrad": (C.c_int, [C.POINTER(_NnAct), _P, C.POINTER(_NnAct), C.POINTER(_NnAct), _P,
+                                    _P]),
+    "ertm_nn_up2_wgrad": (C.c_int, [C.POINTER(_NnAct), C.POINTER(_NnAct), _P, C.c_int, _P, _P]),
+    "ertm_nn_pool2": (C.c_int, [C.POINTER(_NnAct), _P, _P]),
+    "ertm_nn_pool2_bwd": (C.c_int, [C.POINTER(_NnAct), _P, C.POINTER(_NnAct), C.c_int, _P]),
+    "ertm_nn_bias_grad": (C.c_int, [C.POINTER(_NnAct), _P, _P]),
+    "ertm_nn_mse": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_longlong, C.c_float, _P, _P, _P]),
+    "ertm_nn_adam": (C.c_int, [_P, _P, _P, _P, _P, C.c_longlong, C.c_float, C.c_float, C.c_float,
+                               C.c_float, C.c_int, _P]),
+    "ertm_nn_flip3": (C.c_int, [_P, _P, C.c_int, C.c_int, _P]),
+    "ertm_nn_transpose": (C.c_int, [_P, _P, C.c_int, C.c_int, _P]),
+    "ertm_nn_to_bf16": (C.c_int, [_P, _P, C.c_longlong, _P]),
     "ertm_forward_together_using_real_model_noalloc": (
         C.c_int, [C.POINTER(_Config), _P, _P, _P, C.POINTER(_Shot), _P, _P, C.c_char_p, C.c_size_t]),
 }

@@ -1,0 +1,771 @@
+// Learned LSRTM preconditioner: the U-Net's tensor-core kernels (BF16 inputs,
+// FP32 accumulation in tensor memory) and its small elementwise kernels.
+//
+// Every convolution, transposed convolution and weight gradient is one GEMM
+//   D[M x N] = sum_k A[m, k] B[n, k]          (A, B BF16; D FP32 in TMEM)
+// issued with tcgen05.mma (kind::f16, M = 128 rows per CTA, N = BN <= 128
+// columns, K = 16 per instruction) by one thread of the CTA.  The operands are
+// staged in shared memory by all 128 threads through "loaders" that gather 8
+// consecutive K elements (16 bytes) of one row: an implicit im2col for 3x3
+// convolutions on NHWC activations, plain rows of K-major weights, or
+// transposing gathers for the weight gradients.  Two shared-memory stages
+// alternate: while the tensor core works on one, the threads fill the other,
+// and tcgen05.commit on a per-stage mbarrier tells them when a stage is free.
+// After the K loop each warp reads its 32 accumulator rows from TMEM
+// (tcgen05.ld 32x32b) and an epilogue functor writes them (bias, ReLU, BF16
+// store, scatter of a transposed convolution, or FP32 atomics for split-K
+// weight gradients).
+//
+// Shared-memory operand layout (K-major, no swizzle): element (r, k) of an
+// R-row, 64-column stage at byte ((k / 8) * R + r) * 16 + (k % 8) * 2, i.e. the
+// 8 x 16-byte core matrices of the canonical layout with SBO = 128 bytes
+// (next 8 rows) and LBO = R * 16 bytes (next 8 K elements).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "ertm.h"
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int BM = 128;      // rows per CTA (tcgen05 M)
+constexpr int BK = 64;       // K elements per stage
+constexpr int NT = 128;      // threads per CTA
+constexpr unsigned kPolls = 1u << 24;
+
+enum NnError { NN_OK = 0, NN_WAIT = 1 };
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(su32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(su32(b)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity)
+{
+    for (unsigned n = 0; n < kPolls; n++)
+        if (mbar_try(b, parity)) return true;
+    return false;
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle, LBO = lbo bytes, SBO = 128 bytes
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((128u >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;   // descriptor version for sm_100
+    return d;                  // base offset 0, legacy LBO mode, layout SWIZZLE_NONE
+}
+
+// instruction descriptor of kind::f16: BF16 x BF16 -> F32, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_bf16(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = __uint_as_float(r[q]);
+}
+
+// ---------------------------------------------------------------------------
+// Operand loaders: 16 bytes = 8 consecutive K elements of row `r` starting at k
+// (k % 8 == 0).  Rows or K past the bounds read zeros.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 zero4() { return make_uint4(0, 0, 0, 0); }
+
+// NHWC activation view: pixel p = (n*H + y)*W + x, channels [off, off+C) of a
+// pixel stride of cs channels
+struct Act {
+    const bf16* p;
+    int nb, h, w, cs, off, c;
+};
+
+// implicit im2col of a 3x3, pad-1 convolution: row = output pixel, k = tap * C + c
+struct LoadConv3 {
+    Act x;
+    int M, K;
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= M || k >= K) return zero4();
+        const int tap = k / x.c, c = k - tap * x.c;
+        const int xx = r % x.w, t = r / x.w, yy = t % x.h, n = t / x.h;
+        const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
+        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return zero4();
+        const long long q = ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c;
+        return *reinterpret_cast<const uint4*>(x.p + q);
+    }
+};
+
+// rows of a K-major matrix [rows][ld]
+struct LoadRows {
+    const bf16* p;
+    int rows, K, ld;
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= rows || k >= K) return zero4();
+        return *reinterpret_cast<const uint4*>(p + (long long)r * ld + k);
+    }
+};
+
+// transposed-convolution backward input: row = low-resolution pixel (n, i, j),
+// k = (a*2 + b) * C + o reads dy at (2i+a, 2j+b), channel o (dy at 2h x 2w)
+struct LoadUp2 {
+    Act dy;      // high-resolution view (h, w = 2x the rows' grid)
+    int M, K;
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= M || k >= K) return zero4();
+        const int ab = k / dy.c, o = k - ab * dy.c;
+        const int lw = dy.w / 2, lh = dy.h / 2;
+        const int j = r % lw, t = r / lw, i = t % lh, n = t / lh;
+        const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
+        const long long q = ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o;
+        return *reinterpret_cast<const uint4*>(dy.p + q);
+    }
+};
+
+// weight-gradient operands: row = channel index of an activation, k = pixel.
+// Gathers 8 pixels of one channel (strided 2-byte loads).
+__device__ __forceinline__ uint4 pack8(const bf16* v)
+{
+    uint4 u;
+    u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
+    u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
+    u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
+    u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
+    return u;
+}
+
+// row o of dy^T (dy an NHWC view with C channels), k = pixel
+struct LoadChanT {
+    Act a;
+    int rows, P;   // rows = channels used, P = pixels
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= rows) return zero4();
+        bf16 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            v[q] = (k + q < P) ? a.p[(long long)(k + q) * a.cs + a.off + r] : __float2bfloat16(0.f);
+        return pack8(v);
+    }
+};
+
+// row (tap, c) of the 3x3 im2col transposed, k = output pixel
+struct LoadConv3T {
+    Act x;
+    int rows, P;   // rows = 9 C
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= rows) return zero4();
+        const int tap = r / x.c, c = r - tap * x.c, dy = tap / 3 - 1, dx = tap % 3 - 1;
+        bf16 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            v[q] = __float2bfloat16(0.f);
+            const int p = k + q;
+            if (p < P) {
+                const int xx = p % x.w, t = p / x.w, yy = t % x.h, n = t / x.h;
+                const int sy = yy + dy, sx = xx + dx;
+                if (sy >= 0 && sy < x.h && sx >= 0 && sx < x.w)
+                    v[q] = x.p[((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c];
+            }
+        }
+        return pack8(v);
+    }
+};
+
+// row (a, b, o) of the 2x2 up-sampling gather of dy transposed, k = low-res pixel
+struct LoadUp2T {
+    Act dy;
+    int rows, P;   // rows = 4 C
+    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    {
+        if (r >= rows) return zero4();
+        const int ab = r / dy.c, o = r - ab * dy.c;
+        const int lw = dy.w / 2, lh = dy.h / 2;
+        bf16 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            v[q] = __float2bfloat16(0.f);
+            const int p = k + q;
+            if (p < P) {
+                const int j = p % lw, t = p / lw, i = t % lh, n = t / lh;
+                const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
+                v[q] = dy.p[((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o];
+            }
+        }
+        return pack8(v);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Epilogues: called with 8 consecutive columns n0..n0+7 of row m
+// ---------------------------------------------------------------------------
+// NHWC output (bias, optional ReLU): y[m][off + n]
+struct EpiAct {
+    bf16* y;
+    int cs, off, N, M;
+    const float* bias;
+    int relu;
+    __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
+    {
+        if (m >= M) return;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int n = n0 + q;
+            if (n >= N) break;
+            float t = v[q] + (bias ? bias[n] : 0.f);
+            if (relu) t = fmaxf(t, 0.f);
+            y[(long long)m * cs + off + n] = __float2bfloat16(t);
+        }
+    }
+};
+
+// FP32 NHWC output without activation (network output)
+struct EpiF32 {
+    float* y;
+    int cs, N, M;
+    const float* bias;
+    __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
+    {
+        if (m >= M) return;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int n = n0 + q;
+            if (n >= N) break;
+            y[(long long)m * cs + n] = v[q] + (bias ? bias[n] : 0.f);
+        }
+    }
+};
+
+// input gradient: dx[m][off + n] = acc * (x[m][off + n] > 0) when mask is given
+struct EpiGrad {
+    bf16* dx;
+    int cs, off, N, M;
+    const bf16* mask;   // activation whose ReLU produced the layer input, same view
+    __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
+    {
+        if (m >= M) return;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int n = n0 + q;
+            if (n >= N) break;
+            const long long i = (long long)m * cs + off + n;
+            float t = v[q];
+            if (mask && !(__bfloat162float(mask[i]) > 0.f)) t = 0.f;
+            dx[i] = __float2bfloat16(t);
+        }
+    }
+};
+
+// transposed 2x2 stride-2 convolution: column n = (a*2 + b) * C + o scatters to
+// the high-resolution pixel (2i+a, 2j+b) of low-resolution row m
+struct EpiUp2 {
+    bf16* y;
+    int cs, off, C, lh, lw, M;
+    const float* bias;
+    int relu;
+    __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
+    {
+        if (m >= M) return;
+        const int j = m % lw, t = m / lw, i = t % lh, nb = t / lh;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int n = n0 + q;
+            if (n >= 4 * C) break;
+            const int ab = n / C, o = n - ab * C;
+            const int yy = 2 * i + (ab >> 1), xx = 2 * j + (ab & 1);
+            float s = v[q] + (bias ? bias[o] : 0.f);
+            if (relu) s = fmaxf(s, 0.f);
+            y[((long long)(nb * 2 * lh + yy) * 2 * lw + xx) * cs + off + o] = __float2bfloat16(s);
+        }
+    }
+};
+
+// FP32 accumulation (split-K weight gradients): g[m][n] += acc
+struct EpiAtomic {
+    float* g;
+    int ld, N, M;
+    __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
+    {
+        if (m >= M) return;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int n = n0 + q;
+            if (n >= N) break;
+            atomicAdd(g + (long long)m * ld + n, v[q]);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// The GEMM kernel
+// ---------------------------------------------------------------------------
+template <int BN>
+struct Smem {
+    alignas(128) uint8_t a[2][BM * BK * 2];
+    alignas(128) uint8_t b[2][BN * BK * 2];
+    uint64_t bar[2];
+    uint32_t tmem;
+};
+
+// stage one operand tile: rows [r0, r0 + R), K chunk [k0, k0 + 64)
+template <int R, class L>
+__device__ __forceinline__ void stage(uint8_t* dst, const L& ld, int r0, int k0)
+{
+    constexpr int CH = R * (BK / 8);   // 16-byte chunks
+#pragma unroll 4
+    for (int q = threadIdx.x; q < CH; q += NT) {
+        const int r = q % R, j = q / R;    // consecutive threads take consecutive rows
+        const uint4 v = ld(r0 + r, k0 + j * 8);
+        *reinterpret_cast<uint4*>(dst + ((size_t)j * R + r) * 16) = v;
+    }
+}
+
+template <int BN, class LA, class LB, class EP>
+__global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, int K, int kt_per, int* err)
+{
+    extern __shared__ __align__(128) uint8_t smraw[];
+    Smem<BN>& S = *reinterpret_cast<Smem<BN>*>(smraw);
+    constexpr int TCOLS = BN < 32 ? 32 : BN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int KT = (K + BK - 1) / BK;
+    const int kt0 = blockIdx.z * kt_per, kt1 = min(KT, kt0 + kt_per);
+
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    constexpr uint32_t IDESC = idesc_bf16(BN);
+    bool ok = true;
+
+    for (int t = kt0; t < kt1; ++t) {
+        const int u = t - kt0, s = u & 1;
+        if (u >= 2 && ok) ok = mbar_wait(&S.bar[s], ((u >> 1) - 1) & 1);   // MMAs of u-2 done
+        stage<BM>(S.a[s], la, m0, t * BK);
+        stage<BN>(S.b[s], lb, n0, t * BK);
+        proxy_fence();
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            tc_fence_after();
+            const uint32_t a0 = su32(S.a[s]), b0 = su32(S.b[s]);
+#pragma unroll
+            for (int j = 0; j < BK / 16; j++) {
+                // K step j covers the core-matrix columns 2j, 2j+1
+                const uint64_t da = sdesc(a0 + (uint32_t)(2 * j * BM * 16), BM * 16);
+                const uint64_t db = sdesc(b0 + (uint32_t)(2 * j * BN * 16), BN * 16);
+                umma(tmem, da, db, IDESC, (u > 0 || j > 0) ? 1u : 0u);
+            }
+            umma_commit(&S.bar[s]);
+        }
+    }
+    const int nu = kt1 - kt0;
+    if (nu > 0 && ok) ok = mbar_wait(&S.bar[(nu - 1) & 1], ((nu - 1) >> 1) & 1);
+    // the other stage's last commit precedes it, so every MMA has completed;
+    // the TMEM loads below are warp-collective, so the decision is block-uniform
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    tc_fence_after();
+    if (nu > 0 && all_ok) {
+        const int m = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 8) {
+            float v[8];
+            tmem_ld8(trow + c, v);
+            ep(m, n0 + c, v);
+        }
+    }
+    if (!ok && err) atomicExch(err, NN_WAIT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+template <int BN, class LA, class LB, class EP>
+cudaError_t gemm_bn(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int splitk, int* err,
+                    cudaStream_t st)
+{
+    const int KT = (K + BK - 1) / BK;
+    splitk = splitk < 1 ? 1 : (splitk > KT ? KT : splitk);
+    const int kt_per = (KT + splitk - 1) / splitk;
+    const int gz = (KT + kt_per - 1) / kt_per;
+    const size_t smem = sizeof(Smem<BN>);
+    static cudaError_t attr =
+        cudaFuncSetAttribute(k_gemm<BN, LA, LB, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
+    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, gz);
+    k_gemm<BN, LA, LB, EP><<<grid, NT, smem, st>>>(la, lb, ep, M, N, K, kt_per, err);
+    return cudaGetLastError();
+}
+
+// N tile: 16 <= BN <= 128, multiple of 16 (tcgen05 M = 128 needs N % 16 == 0)
+template <class LA, class LB, class EP>
+cudaError_t gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int splitk, int* err,
+                 cudaStream_t st)
+{
+    if (N <= 16) return gemm_bn<16>(la, lb, ep, M, N, K, splitk, err, st);
+    if (N <= 32) return gemm_bn<32>(la, lb, ep, M, N, K, splitk, err, st);
+    if (N <= 64) return gemm_bn<64>(la, lb, ep, M, N, K, splitk, err, st);
+    return gemm_bn<128>(la, lb, ep, M, N, K, splitk, err, st);
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels
+// ---------------------------------------------------------------------------
+// 2x2 max pooling of an NHWC view into a dense NHWC output with C channels
+__global__ void k_pool_fwd(Act x, bf16* y, long long n)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % x.c);
+        long long t = q / x.c;
+        const int j = (int)(t % (x.w / 2));
+        t /= (x.w / 2);
+        const int i = (int)(t % (x.h / 2)), nb = (int)(t / (x.h / 2));
+        float m = -3.0e38f;
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++)
+                m = fmaxf(m, __bfloat162float(x.p[((long long)(nb * x.h + 2 * i + a) * x.w + 2 * j + b) * x.cs + x.off + c]));
+        y[q] = __float2bfloat16(m);
+    }
+}
+
+// max pooling backward: the gradient goes to the first maximum of each 2x2 window;
+// adds into dx (NHWC view), masked by the ReLU of x when mask != 0
+__global__ void k_pool_bwd(Act x, const bf16* dy, bf16* dx, long long n, int mask)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % x.c);
+        long long t = q / x.c;
+        const int j = (int)(t % (x.w / 2));
+        t /= (x.w / 2);
+        const int i = (int)(t % (x.h / 2)), nb = (int)(t / (x.h / 2));
+        float m = -3.0e38f;
+        long long best = -1;
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) {
+                const long long e = ((long long)(nb * x.h + 2 * i + a) * x.w + 2 * j + b) * x.cs + x.off + c;
+                const float v = __bfloat162float(x.p[e]);
+                if (v > m) { m = v; best = e; }
+            }
+        const float g = __bfloat162float(dy[q]);
+        if (best >= 0 && (!mask || m > 0.f)) dx[best] = __float2bfloat16(__bfloat162float(dx[best]) + g);
+    }
+}
+
+// bias gradient: db[o] += sum over pixels of dy[p][off + o]
+__global__ void k_bias_grad(Act dy, long long P, float* db)
+{
+    const int o = blockIdx.y;
+    float s = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+        s += __bfloat162float(dy.p[p * dy.cs + dy.off + o]);
+    for (int k = 16; k; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        atomicAdd(db + o, t);
+    }
+}
+
+// mean-squared-error gradient of an FP32 NHWC output against a target, first C
+// channels of cs: g = scale (y - t) (BF16, cs channels, zero in the padding);
+// loss += sum (y - t)^2
+__global__ void k_mse(const float* y, const float* t, int cs, int C, long long P, float scale, bf16* g, float* loss)
+{
+    float acc = 0.f;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P * cs; q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % cs);
+        float d = 0.f;
+        if (c < C) {
+            d = y[q] - t[(q / cs) * C + c];
+            acc += d * d;
+        }
+        g[q] = __float2bfloat16(scale * d);
+    }
+    for (int k = 16; k; k >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, k);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
+}
+
+// Adam on FP32 master weights; writes the BF16 copy used by the GEMMs
+__global__ void k_adam(float* w, const float* g, float* m, float* v, bf16* wb, long long n, float lr, float b1,
+                       float b2, float eps, float c1, float c2)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.f - b1) * gq;
+        const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        const float wq = w[q] - lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+        w[q] = wq;
+        wb[q] = __float2bfloat16(wq);
+    }
+}
+
+// weight re-layouts for the input gradients:
+//  conv3: W[o][tap][c] (K = 9 Ci) -> Wf[c][8 - tap][o] (K = 9 Co)
+//  up2:   U[(a*2+b)*Co + o][c] (K = Ci) -> Ut[c][(a*2+b)*Co + o] (K = 4 Co)
+__global__ void k_flip3(const bf16* w, bf16* wf, int co, int ci)
+{
+    const long long n = (long long)co * 9 * ci;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % ci), tap = (int)((q / ci) % 9), o = (int)(q / (9LL * ci));
+        wf[((long long)c * 9 + (8 - tap)) * co + o] = w[q];
+    }
+}
+__global__ void k_transpose(const bf16* a, bf16* t, int rows, int cols)
+{
+    const long long n = (long long)rows * cols;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % cols), r = (int)(q / cols);
+        t[(long long)c * rows + r] = a[q];
+    }
+}
+__global__ void k_f32_to_bf16(const float* a, bf16* b, long long n)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        b[q] = __float2bfloat16(a[q]);
+}
+
+int grid_of(long long n) { return (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16); }
+
+int rc_of(cudaError_t e) { return e == cudaSuccess ? ERTM_OK : ERTM_ECUDA; }
+
+Act act_of(const ertm_nn_act* a)
+{
+    return Act{reinterpret_cast<const bf16*>(a->data), a->n, a->h, a->w, a->cstride, a->coff, a->c};
+}
+
+bool act_ok(const ertm_nn_act* a)
+{
+    return a && a->data && a->n > 0 && a->h > 0 && a->w > 0 && a->c > 0 && a->c % 8 == 0 && a->coff % 8 == 0 &&
+           a->cstride % 8 == 0 && a->coff + a->c <= a->cstride && ((uintptr_t)a->data % 16) == 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int ertm_nn_gemm(const void* a, const void* b, float* d, int M, int N, int K, int* err, void* stream)
+{
+    if (!a || !b || !d || M < 1 || N < 1 || K < 1 || K % 8) return ERTM_EINVAL;
+    LoadRows la{reinterpret_cast<const bf16*>(a), M, K, K};
+    LoadRows lb{reinterpret_cast<const bf16*>(b), N, K, K};
+    EpiF32 ep{d, N, N, M, nullptr};
+    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, (cudaStream_t)stream));
+}
+
+int ertm_nn_conv3x3(const ertm_nn_act* x, const void* w, const float* bias, const ertm_nn_act* y, int relu,
+                    float* y32, int* err, void* stream)
+{
+    if (!act_ok(x) || !w || !y || (!y32 && !act_ok(y))) return ERTM_EINVAL;
+    if (y->n != x->n || y->h != x->h || y->w != x->w) return ERTM_EINVAL;
+    const int M = x->n * x->h * x->w, N = y->c, K = 9 * x->c;
+    LoadConv3 la{act_of(x), M, K};
+    LoadRows lb{reinterpret_cast<const bf16*>(w), N, K, K};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (y32) {
+        EpiF32 ep{y32, y->cstride, N, M, bias};
+        return rc_of(gemm(la, lb, ep, M, N, K, 1, err, st));
+    }
+    EpiAct ep{reinterpret_cast<bf16*>(const_cast<void*>(y->data)), y->cstride, y->coff, N, M, bias, relu};
+    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, st));
+}
+
+int ertm_nn_conv3x3_dgrad(const ertm_nn_act* dy, const void* wflip, const ertm_nn_act* dx, const ertm_nn_act* mask,
+                          int* err, void* stream)
+{
+    if (!act_ok(dy) || !wflip || !act_ok(dx)) return ERTM_EINVAL;
+    const int M = dy->n * dy->h * dy->w, N = dx->c, K = 9 * dy->c;
+    LoadConv3 la{act_of(dy), M, K};
+    LoadRows lb{reinterpret_cast<const bf16*>(wflip), N, K, K};
+    EpiGrad ep{reinterpret_cast<bf16*>(const_cast<void*>(dx->data)), dx->cstride, dx->coff, N, M,
+               mask ? reinterpret_cast<const bf16*>(mask->data) : nullptr};
+    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, (cudaStream_t)stream));
+}
+
+int ertm_nn_conv3x3_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* dw, int splitk, int* err, void* stream)
+{
+    if (!act_ok(x) || !act_ok(dy) || !dw) return ERTM_EINVAL;
+    const int P = x->n * x->h * x->w;
+    const int M = dy->c, N = 9 * x->c, K = (P + 7) / 8 * 8;
+    LoadChanT la{act_of(dy), M, P};
+    LoadConv3T lb{act_of(x), N, P};
+    EpiAtomic ep{dw, N, N, M};
+    return rc_of(gemm(la, lb, ep, M, N, K, splitk, err, (cudaStream_t)stream));
+}
+
+int ertm_nn_up2(const ertm_nn_act* x, const void* u, const float* bias, const ertm_nn_act* y, int relu, int* err,
+                void* stream)
+{
+    if (!act_ok(x) || !u || !act_ok(y) || y->h != 2 * x->h || y->w != 2 * x->w || y->n != x->n) return ERTM_EINVAL;
+    const int M = x->n * x->h * x->w, N = 4 * y->c, K = x->c;
+    Act xa = act_of(x);
+    // a plain-rows view of x works only for dense channels; use the 1x1 gather otherwise
+    LoadRows lb{reinterpret_cast<const bf16*>(u), N, K, K};
+    EpiUp2 ep{reinterpret_cast<bf16*>(const_cast<void*>(y->data)), y->cstride, y->coff, y->c, x->h, x->w, M, bias,
+              relu};
+    if (x->coff == 0 && x->cstride == x->c) {
+        LoadRows la{xa.p, M, K, K};
+        return rc_of(gemm(la, lb, ep, M, N, K, 1, err, (cudaStream_t)stream));
+    }
+    return ERTM_EINVAL;
+}
+
+int ertm_nn_up2_dgrad(const ertm_nn_act* dy, const void* ut, const ertm_nn_act* dx, const ertm_nn_act* mask,
+                      int* err, void* stream)
+{
+    if (!act_ok(dy) || !ut || !act_ok(dx) || dy->h != 2 * dx->h || dy->w != 2 * dx->w) return ERTM_EINVAL;
+    const int M = dx->n * dx->h * dx->w, N = dx->c, K = 4 * dy->c;
+    LoadUp2 la{act_of(dy), M, K};
+    LoadRows lb{reinterpret_cast<const bf16*>(ut), N, K, K};
+    EpiGrad ep{reinterpret_cast<bf16*>(const_cast<void*>(dx->data)), dx->cstride, dx->coff, N, M,
+               mask ? reinterpret_cast<const bf16*>(mask->data) : nullptr};
+    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, (cudaStream_t)stream));
+}
+
+int ertm_nn_up2_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* du, int splitk, int* err, void* stream)
+{
+    if (!act_ok(x) || !act_ok(dy) || !du || dy->h != 2 * x->h || dy->w != 2 * x->w) return ERTM_EINVAL;
+    const int P = x->n * x->h * x->w;
+    const int M = 4 * dy->c, N = x->c, K = (P + 7) / 8 * 8;
+    LoadUp2T la{act_of(dy), M, P};
+    LoadChanT lb{act_of(x), N, P};
+    EpiAtomic ep{du, N, N, M};
+    return rc_of(gemm(la, lb, ep, M, N, K, splitk, err, (cudaStream_t)stream));
+}
+
+int ertm_nn_pool2(const ertm_nn_act* x, void* y, void* stream)
+{
+    if (!act_ok(x) || !y || x->h % 2 || x->w % 2) return ERTM_EINVAL;
+    const long long n = (long long)x->n * (x->h / 2) * (x->w / 2) * x->c;
+    k_pool_fwd<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(act_of(x), reinterpret_cast<bf16*>(y), n);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_pool2_bwd(const ertm_nn_act* x, const void* dy, const ertm_nn_act* dx, int relu_mask, void* stream)
+{
+    if (!act_ok(x) || !dy || !act_ok(dx) || x->h % 2 || x->w % 2) return ERTM_EINVAL;
+    if (dx->cstride != x->cstride || dx->coff != x->coff || dx->c != x->c) return ERTM_EINVAL;
+    const long long n = (long long)x->n * (x->h / 2) * (x->w / 2) * x->c;
+    // the gradient lands at the same offsets as x's elements (same view layout)
+    Act xa = act_of(x);
+    bf16* dxp = reinterpret_cast<bf16*>(const_cast<void*>(dx->data));
+    k_pool_bwd<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(xa, reinterpret_cast<const bf16*>(dy), dxp, n,
+                                                             relu_mask);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_bias_grad(const ertm_nn_act* dy, float* db, void* stream)
+{
+    if (!act_ok(dy) || !db) return ERTM_EINVAL;
+    const long long P = (long long)dy->n * dy->h * dy->w;
+    dim3 grid((unsigned)std::min<long long>((P + 255) / 256, 64), dy->c);
+    k_bias_grad<<<grid, 256, 0, (cudaStream_t)stream>>>(act_of(dy), P, db);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_mse(const float* y, const float* target, int cstride, int c, long long pixels, float scale, void* grad,
+                float* loss, void* stream)
+{
+    if (!y || !target || !grad || !loss || c > cstride || cstride % 8) return ERTM_EINVAL;
+    k_mse<<<grid_of(pixels * cstride), 256, 0, (cudaStream_t)stream>>>(y, target, cstride, c, pixels, scale,
+                                                                     reinterpret_cast<bf16*>(grad), loss);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_adam(float* w, const float* g, float* m, float* v, void* wb, long long n, float lr, float b1, float b2,
+                 float eps, int step, void* stream)
+{
+    if (!w || !g || !m || !v || !wb || n < 0 || step < 1) return ERTM_EINVAL;
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    k_adam<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, reinterpret_cast<bf16*>(wb), n, lr, b1, b2, eps,
+                                                         c1, c2);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_flip3(const void* w, void* wf, int co, int ci, void* stream)
+{
+    if (!w || !wf || co < 1 || ci < 1) return ERTM_EINVAL;
+    k_flip3<<<grid_of((long long)co * 9 * ci), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const bf16*>(w),
+                                                                             reinterpret_cast<bf16*>(wf), co, ci);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_transpose(const void* a, void* t, int rows, int cols, void* stream)
+{
+    if (!a || !t || rows < 1 || cols < 1) return ERTM_EINVAL;
+    k_transpose<<<grid_of((long long)rows * cols), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const bf16*>(a), reinterpret_cast<bf16*>(t), rows, cols);
+    return rc_of(cudaGetLastError());
+}
+
+int ertm_nn_to_bf16(const float* a, void* b, long long n, void* stream)
+{
+    if (!a || !b || n < 0) return ERTM_EINVAL;
+    k_f32_to_bf16<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(a, reinterpret_cast<bf16*>(b), n);
+    return rc_of(cudaGetLastError());
+}
+
+}  // extern "C"

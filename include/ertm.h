@@ -267,6 +267,63 @@ int ertm_forward_together_using_real_model_noalloc(const ertm_config *cfg, const
                                                    void *cuda_stream, char *errbuf,
                                                    size_t errlen);
 
+/* ---- learned LSRTM preconditioner: tensor-core network kernels --------
+ * No counterpart in the reference (its LSRTM has no learned part).  Building
+ * blocks of a 2D U-Net: BF16 NHWC activations, FP32 accumulation in tensor
+ * memory (tcgen05.mma), FP32 master weights.  All pointers are device
+ * pointers; calls are asynchronous on `stream` (NULL: the legacy stream).
+ * `err` (device int, may be NULL) is set non-zero if a kernel's bounded wait
+ * gave up.  Channel counts, offsets and strides are multiples of 8. */
+typedef struct {
+    const void *data;        /* BF16, pixel p = (n*h + y)*w + x at data + p*cstride + coff */
+    int n, h, w;             /* batch, height, width */
+    int cstride, coff, c;    /* channels per pixel in memory, first channel, channels used */
+} ertm_nn_act;
+
+/* D[M][N] = A[M][K] B[N][K]^T, A and B BF16 row-major (K contiguous, K % 8 == 0), D FP32 */
+int ertm_nn_gemm(const void *a, const void *b, float *d, int M, int N, int K, int *err, void *stream);
+/* 3x3 convolution, zero padding 1: y = relu?(conv(x, w) + bias); w BF16 [y.c][9][x.c];
+ * output into the BF16 view y, or FP32 y32[pixel][y.cstride] when y32 != NULL */
+int ertm_nn_conv3x3(const ertm_nn_act *x, const void *w, const float *bias, const ertm_nn_act *y,
+                    int relu, float *y32, int *err, void *stream);
+/* input gradient through a 3x3 convolution: dx = conv(dy, wflip) (* (mask > 0) when mask);
+ * wflip from ertm_nn_flip3 */
+int ertm_nn_conv3x3_dgrad(const ertm_nn_act *dy, const void *wflip, const ertm_nn_act *dx,
+                          const ertm_nn_act *mask, int *err, void *stream);
+/* weight gradient of a 3x3 convolution, accumulated: dw[dy.c][9][x.c] += ... (split-K) */
+int ertm_nn_conv3x3_wgrad(const ertm_nn_act *x, const ertm_nn_act *dy, float *dw, int splitk,
+                          int *err, void *stream);
+/* 2x2 stride-2 transposed convolution: y[2i+a][2j+b][o] = relu?(sum_c x[i][j][c] u[(2a+b)*y.c+o][c]
+ * + bias[o]); x dense (coff 0, cstride c) */
+int ertm_nn_up2(const ertm_nn_act *x, const void *u, const float *bias, const ertm_nn_act *y,
+                int relu, int *err, void *stream);
+/* input gradient of ertm_nn_up2 (ut = u transposed, [x.c][4 y.c]), optional ReLU mask */
+int ertm_nn_up2_dgrad(const ertm_nn_act *dy, const void *ut, const ertm_nn_act *dx,
+                      const ertm_nn_act *mask, int *err, void *stream);
+/* weight gradient of ertm_nn_up2, accumulated: du[4 dy.c][x.c] += ... */
+int ertm_nn_up2_wgrad(const ertm_nn_act *x, const ertm_nn_act *dy, float *du, int splitk, int *err,
+                      void *stream);
+/* 2x2 max pooling into a dense BF16 output [n][h/2][w/2][x.c] */
+int ertm_nn_pool2(const ertm_nn_act *x, void *y, void *stream);
+/* its backward: adds dy into dx at the first maximum of each window (dx has x's layout);
+ * relu_mask: only where that maximum is positive */
+int ertm_nn_pool2_bwd(const ertm_nn_act *x, const void *dy, const ertm_nn_act *dx, int relu_mask,
+                      void *stream);
+/* db[o] += sum over pixels of dy[..][o] */
+int ertm_nn_bias_grad(const ertm_nn_act *dy, float *db, void *stream);
+/* grad = scale (y - target) over the first c of cstride channels (BF16, padding 0);
+ * *loss += sum (y - target)^2 */
+int ertm_nn_mse(const float *y, const float *target, int cstride, int c, long long pixels,
+                float scale, void *grad, float *loss, void *stream);
+/* Adam step `step` (1-based) on FP32 weights; writes the BF16 copy wb */
+int ertm_nn_adam(float *w, const float *g, float *m, float *v, void *wb, long long n, float lr,
+                 float b1, float b2, float eps, int step, void *stream);
+/* wf[c][8-tap][o] = w[o][tap][c] (BF16) */
+int ertm_nn_flip3(const void *w, void *wf, int co, int ci, void *stream);
+/* t[cols][rows] = a[rows][cols] (BF16) */
+int ertm_nn_transpose(const void *a, void *t, int rows, int cols, void *stream);
+int ertm_nn_to_bf16(const float *a, void *b, long long n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
