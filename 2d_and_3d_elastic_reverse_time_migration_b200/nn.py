@@ -309,8 +309,9 @@ class UNet:
             if l > 0:
                 o.conv_dgrad(gea, P[f"e{l}a"].aux, act(G[f"in{l}"], n, hh, ww))
 
-    def step(self, x, target, lr=1e-3):
-        """One Adam step on the MSE between forward(x) and target ((n, h, w, 3) float32)."""
+    def loss_grad(self, x, target):
+        """Forward, mean-squared error against target ((n, h, w, 3) float32) and backward:
+        fills every p.g and p.bg; returns the loss (device scalar)."""
         t = self.torch
         n, h, w, _ = x.shape
         B, G = self._buffers(n, h, w)
@@ -319,6 +320,11 @@ class UNet:
         cnt = n * h * w * OUT_C
         self.ops.mse(B["out"], target.contiguous(), OUT_C, 2.0 / cnt, G["out"], loss)
         self.backward(G["out"])
+        return loss / cnt
+
+    def step(self, x, target, lr=1e-3):
+        """One Adam step on the MSE between forward(x) and target ((n, h, w, 3) float32)."""
+        loss = self.loss_grad(x, target)
         self.t += 1
         for p in self.params.values():
             self.ops.adam(p.w, p.g, p.m, p.v, p.wb, lr, self.t)
@@ -328,7 +334,7 @@ class UNet:
                 self.ops.flip3(p.wb, p.aux, p.co, p.ci)
             else:
                 self.ops.transpose(p.wb, p.aux, 4 * p.co, p.ci)
-        return loss / cnt
+        return loss
 
     def flops_per_sample(self, h, w):
         """Multiply-adds x 2 of one forward pass on an h x w image."""

@@ -198,3 +198,32 @@ def windows_3d(nshots: int = 64, seed: int = BASE_SEED + 3, n_interior=(200, 256
                           rx0=x0, nrx=(wx + rec_every - 1) // rec_every, drx=rec_every,
                           ry0=y0, nry=(wy + rec_every - 1) // rec_every, dry=rec_every, rz=2))
     return (wl.svp, wl.svs, wl.srho), wins, shots
+
+
+def faulted_2d(seed: int, nz: int = 400, nx: int = 800, h: float = 5.0, vmin: float = 1800.0,
+               vmax: float = 4000.0):
+    """2D layered-and-faulted model (the LSRTM workload's generator): 8-12 layers with
+    seeded tops and Vp increasing with depth in [vmin, vmax], cut by 2-4 dipping normal
+    faults (dip 50-70 degrees, throw 20-80 m, hanging wall down); Vs = Vp/sqrt(3),
+    density 310 Vp^0.25.  Returns (vp, vs, rho), each (nz, 1, nx) float32."""
+    rng = np.random.default_rng(seed)
+    nl = int(rng.integers(8, 13))
+    depth = nz * h
+    tops = np.sort(rng.uniform(0.05 * depth, 0.95 * depth, size=nl - 1))
+    vps = np.sort(rng.uniform(vmin, vmax, size=nl))
+    z = (np.arange(nz) + 0.5) * h
+    x = (np.arange(nx) + 0.5) * h
+    Z = np.broadcast_to(z[:, None], (nz, nx)).copy()
+    for _ in range(int(rng.integers(2, 5))):
+        x0 = rng.uniform(0.15, 0.85) * nx * h
+        dip = np.deg2rad(rng.uniform(50.0, 70.0)) * rng.choice([-1.0, 1.0])
+        throw = rng.uniform(20.0, 80.0)
+        # the fault plane x = x0 + z / tan(dip); cells on the hanging-wall side sample
+        # the layering `throw` shallower (their layers moved down)
+        side = (x[None, :] - (x0 + Z / np.tan(dip))) * np.sign(dip) > 0
+        Z = np.where(side, Z - throw, Z)
+    layer = np.searchsorted(tops, Z)
+    vp = vps[layer].astype(np.float32)[:, None, :]
+    vs = vs_from_vp(vp)
+    rho = gardner(vp)
+    return vp, vs, rho

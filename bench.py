@@ -52,8 +52,12 @@ def parse():
     ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
-    ap.add_argument("--workload", default="shot", choices=["shot", "windows"],
-                    help="windows: the batched aperture-window workload (its own line)")
+    ap.add_argument("--workload", default="shot", choices=["shot", "windows", "unet", "lsrtm"],
+                    help="windows: batched aperture windows; unet: one U-Net training step at "
+                         "256x512, batch 16; lsrtm: learned vs plain CG (each its own line)")
+    ap.add_argument("--train-models", type=int, default=24)
+    ap.add_argument("--test-models", type=int, default=4)
+    ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--shots", type=int, default=64, help="windows workload: shots")
     ap.add_argument("--lanes", type=int, default=4, help="windows workload: shots in flight")
     return ap.parse_args()
@@ -232,12 +236,95 @@ def run_windows(args):
         "clocks": clk}), flush=True)
 
 
+def run_unet(args):
+    """U-Net training step (forward, loss, backward, Adam) on 16 patches of 256 x 512:
+    tensor-core throughput of the learned part, CUDA events on the current stream."""
+    import torch
+    nn = importlib.import_module(PKG + ".nn")
+    dev = torch.device("cuda", 0)
+    net = nn.UNet(dev, seed=0)
+    n, h, w = 16, 256, 512
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.randn(n, h, w, 3, generator=g).to(dev)
+    t = torch.randn(n, h, w, 3, generator=g).to(dev)
+    for _ in range(max(3, args.warmup)):
+        net.step(x, t)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    for _ in range(args.steps):
+        net.step(x, t)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    flops = 3 * n * net.flops_per_sample(h, w)     # forward + input and weight gradients
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    peak = float(json.load(open(peaks_path))["bf16_tflops"]) if os.path.exists(peaks_path) else 1590.0
+    tf = flops / (ms / 1e3) / 1e12
+    print(json.dumps({"metric": "U-Net training step (256x512, batch 16)", "value": round(ms, 3),
+                      "unit": "ms/step", "higher_is_better": False, "dtype": "bf16 (fp32 accumulate)",
+                      "steps": args.steps, "warmup": args.warmup,
+                      "flops_per_step": flops, "tflops": round(tf, 2),
+                      "roofline": {"bound": "tensor", "achieved": round(tf, 2), "peak": peak,
+                                   "unit": "TFLOP/s", "frac": round(tf / peak, 4)},
+                      "forward_gflop_per_patch": round(net.flops_per_sample(h, w) / 1e9, 3)}), flush=True)
+
+
+def run_lsrtm(args):
+    """Learned-preconditioned LSRTM (reduced scale): training pairs from CG on seeded
+    layered-and-faulted models, U-Net training, plain vs learned CG on held-out models."""
+    import numpy as np
+    import torch
+    nn = importlib.import_module(PKG + ".nn")
+    L = importlib.import_module(PKG + ".learned")
+    dev = torch.device("cuda", 0)
+    geo = L.Geometry()
+    t0 = time.perf_counter()
+    pairs = []
+    for k in range(args.train_models):
+        case = L.make_case(1000 + k, geo)
+        pairs.append(L.training_pair(case, cg_iters=10))
+        case.ctx.close()
+    t_data = time.perf_counter() - t0
+    net = nn.UNet(dev, seed=0)
+    log = L.train(net, pairs, steps=args.train_steps, batch=16, patch=(64, 128), lr=1e-3)
+    target, niter = 1e-2, 20
+    rows = []
+    for k in range(args.test_models):
+        case = L.make_case(5000 + k, geo)
+        rows.append(L.compare(case, net, niter=niter, target=target))
+        case.ctx.close()
+    def med(key):
+        v = [r[key] for r in rows if r[key] is not None]
+        return float(np.median(v)) if v else None
+    print(json.dumps({
+        "metric": "LSRTM iterations and wall time to relative data misfit 1e-2: learned vs plain CG",
+        "unit": "iterations / s", "config": {"grid": f"{geo.nxi}x{geo.nzi} + sponge {geo.pml}",
+                                           "shots": geo.nshots, "nt": geo.nt,
+                                           "train_models": args.train_models,
+                                           "test_models": args.test_models,
+                                           "train_steps": args.train_steps, "cg_iters_target": 10},
+        "plain_iters_median": med("plain_iters"), "learned_iters_median": med("learned_iters"),
+        "plain_time_median": med("plain_time_to_target"),
+        "learned_time_median": med("learned_time_to_target"),
+        "model_rel_diff_median": med("model_rel_diff"),
+        "data_seconds": round(t_data, 1), "train_seconds": round(log.seconds, 1),
+        "train_loss": log.loss[::max(1, len(log.loss) // 8)],
+        "cases": [{k: (v if not isinstance(v, list) else [round(float(x), 5) for x in v])
+                   for k, v in r.items()} for r in rows]}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "windows":
         return run_windows(args)
+    if args.workload == "unet":
+        return run_unet(args)
+    if args.workload == "lsrtm":
+        return run_lsrtm(args)
     import numpy as np
     import torch
     import torch.distributed as dist
