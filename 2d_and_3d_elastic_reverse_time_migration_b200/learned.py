@@ -153,9 +153,16 @@ def iters_to(misfit: list, target: float):
     return None
 
 
+def _model_err(m, ref) -> float:
+    num = sum(float(np.sum((a.astype(np.float64) - b) ** 2)) for a, b in zip(m, ref))
+    den = sum(float(np.sum(b.astype(np.float64) ** 2)) for b in ref)
+    return float(np.sqrt(num / max(den, 1e-30)))
+
+
 def compare(case: Case, net, niter: int, target: float):
-    """Plain vs learned-preconditioned CG on one case: misfit curves, iterations and
-    wall time to reach `target`, and the relative model difference of the results."""
+    """Plain vs learned-preconditioned CG on one case: misfit curves; iterations and
+    wall time to reach `target` and to reach plain CG's final (niter-th) misfit;
+    reflectivity errors against the true perturbation."""
     t0 = time.perf_counter()
     plain = _lsrtm.cgls(case.ctx, case.shots, case.data, niter=niter)
     tp = time.perf_counter() - t0
@@ -165,11 +172,16 @@ def compare(case: Case, net, niter: int, target: float):
     tl = time.perf_counter() - t0
     ip, il = iters_to(plain.misfit, target), iters_to(learned.misfit, target)
     per_p, per_l = tp / max(1, len(plain.misfit)), tl / max(1, len(learned.misfit))
-    diff = np.sqrt(sum(float(np.sum((a.astype(np.float64) - b) ** 2)) for a, b in zip(learned.m, plain.m)) /
-                   max(1e-30, sum(float(np.sum(b.astype(np.float64) ** 2)) for b in plain.m)))
+    pfin = plain.misfit[-1]
+    il_fin = iters_to(learned.misfit, pfin)
     return {"plain_misfit": plain.misfit, "learned_misfit": learned.misfit,
             "accepted": learned.accepted, "plain_iters": ip, "learned_iters": il,
             "plain_seconds": tp, "learned_seconds": tl,
             "plain_time_to_target": ip * per_p if ip else None,
             "learned_time_to_target": il * per_l if il else None,
-            "model_rel_diff": diff}
+            "learned_iters_to_plain_final": il_fin,
+            "learned_time_to_plain_final": il_fin * per_l if il_fin else None,
+            "time_ratio_to_plain_final": (il_fin * per_l) / tp if il_fin else None,
+            "plain_model_err": _model_err(plain.m, case.true),
+            "learned_model_err": _model_err(learned.m, case.true),
+            "model_rel_diff": _model_err(learned.m, plain.m)}
