@@ -8,7 +8,7 @@
 // staged in shared memory by all 128 threads through "loaders" that gather 8
 // consecutive K elements (16 bytes) of one row: an implicit im2col for 3x3
 // convolutions on NHWC activations, plain rows of K-major weights, or
-// transposing gathers for the weight gradients.  Two shared-memory stages
+// MN-major gathers (8 channels of one pixel) for the weight gradients.  Two shared-memory stages
 // alternate: while the tensor core works on one, the threads fill the other,
 // and tcgen05.commit on a per-stage mbarrier tells them when a stage is free.
 // After the K loop each warp reads its 32 accumulator rows from TMEM
@@ -125,6 +125,7 @@ struct Act {
 struct LoadConv3 {
     Act x;
     int M, K;
+    static constexpr bool MN = false;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
         if (r >= M || k >= K) return zero4();
@@ -141,6 +142,7 @@ struct LoadConv3 {
 struct LoadRows {
     const bf16* p;
     int rows, K, ld;
+    static constexpr bool MN = false;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
         if (r >= rows || k >= K) return zero4();
@@ -153,6 +155,7 @@ struct LoadRows {
 struct LoadUp2 {
     Act dy;      // high-resolution view (h, w = 2x the rows' grid)
     int M, K;
+    static constexpr bool MN = false;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
         if (r >= M || k >= K) return zero4();
@@ -165,78 +168,51 @@ struct LoadUp2 {
     }
 };
 
-// weight-gradient operands: row = channel index of an activation, k = pixel.
-// Gathers 8 pixels of one channel (strided 2-byte loads).
-__device__ __forceinline__ uint4 pack8(const bf16* v)
-{
-    uint4 u;
-    u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
-    u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
-    u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
-    u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
-    return u;
-}
+// Weight-gradient operands are staged MN-major: one 16-byte chunk holds 8
+// consecutive rows (channels, contiguous in NHWC memory) at one K index (pixel),
+// so the gathers stay coalesced.  operator()(r, k) returns rows r .. r+7 (r % 8 == 0).
 
-// row o of dy^T (dy an NHWC view with C channels), k = pixel
-struct LoadChanT {
+// rows = channels of an NHWC view, k = pixel
+struct LoadChanMN {
     Act a;
-    int rows, P;   // rows = channels used, P = pixels
+    int rows, P;
+    static constexpr bool MN = true;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
-        if (r >= rows) return zero4();
-        bf16 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-            v[q] = (k + q < P) ? a.p[(long long)(k + q) * a.cs + a.off + r] : __float2bfloat16(0.f);
-        return pack8(v);
+        if (r >= rows || k >= P) return zero4();
+        return *reinterpret_cast<const uint4*>(a.p + (long long)k * a.cs + a.off + r);
     }
 };
 
-// row (tap, c) of the 3x3 im2col transposed, k = output pixel
-struct LoadConv3T {
+// rows = (tap, c) of the 3x3 im2col, k = output pixel
+struct LoadConv3MN {
     Act x;
     int rows, P;   // rows = 9 C
+    static constexpr bool MN = true;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
-        if (r >= rows) return zero4();
-        const int tap = r / x.c, c = r - tap * x.c, dy = tap / 3 - 1, dx = tap % 3 - 1;
-        bf16 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            v[q] = __float2bfloat16(0.f);
-            const int p = k + q;
-            if (p < P) {
-                const int xx = p % x.w, t = p / x.w, yy = t % x.h, n = t / x.h;
-                const int sy = yy + dy, sx = xx + dx;
-                if (sy >= 0 && sy < x.h && sx >= 0 && sx < x.w)
-                    v[q] = x.p[((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c];
-            }
-        }
-        return pack8(v);
+        if (r >= rows || k >= P) return zero4();
+        const int tap = r / x.c, c = r - tap * x.c;
+        const int xx = k % x.w, t = k / x.w, yy = t % x.h, n = t / x.h;
+        const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
+        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return zero4();
+        return *reinterpret_cast<const uint4*>(x.p + ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c);
     }
 };
 
-// row (a, b, o) of the 2x2 up-sampling gather of dy transposed, k = low-res pixel
-struct LoadUp2T {
+// rows = (a, b, o) of the 2x2 up-sampling gather of dy (high resolution), k = low-res pixel
+struct LoadUp2MN {
     Act dy;
     int rows, P;   // rows = 4 C
+    static constexpr bool MN = true;
     __device__ __forceinline__ uint4 operator()(int r, int k) const
     {
-        if (r >= rows) return zero4();
+        if (r >= rows || k >= P) return zero4();
         const int ab = r / dy.c, o = r - ab * dy.c;
         const int lw = dy.w / 2, lh = dy.h / 2;
-        bf16 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            v[q] = __float2bfloat16(0.f);
-            const int p = k + q;
-            if (p < P) {
-                const int j = p % lw, t = p / lw, i = t % lh, n = t / lh;
-                const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
-                v[q] = dy.p[((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o];
-            }
-        }
-        return pack8(v);
+        const int j = k % lw, t = k / lw, i = t % lh, n = t / lh;
+        const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
+        return *reinterpret_cast<const uint4*>(dy.p + ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o);
     }
 };
 
@@ -324,10 +300,12 @@ struct EpiUp2 {
     }
 };
 
-// FP32 accumulation (split-K weight gradients): g[m][n] += acc
+// FP32 accumulation (split-K weight gradients): g[m][n] += acc, or g[n][m] += acc
+// when trans (the GEMM ran with the operands swapped)
 struct EpiAtomic {
     float* g;
     int ld, N, M;
+    int trans;
     __device__ __forceinline__ void operator()(int m, int n0, const float* v) const
     {
         if (m >= M) return;
@@ -335,7 +313,7 @@ struct EpiAtomic {
         for (int q = 0; q < 8; q++) {
             const int n = n0 + q;
             if (n >= N) break;
-            atomicAdd(g + (long long)m * ld + n, v[q]);
+            atomicAdd(g + (trans ? (long long)n * ld + m : (long long)m * ld + n), v[q]);
         }
     }
 };
@@ -356,11 +334,23 @@ template <int R, class L>
 __device__ __forceinline__ void stage(uint8_t* dst, const L& ld, int r0, int k0)
 {
     constexpr int CH = R * (BK / 8);   // 16-byte chunks
+    if constexpr (!L::MN) {
+        // K-major: chunk = 8 K elements of one row; core matrix (8 rows x 16 B)
 #pragma unroll 4
-    for (int q = threadIdx.x; q < CH; q += NT) {
-        const int r = q % R, j = q / R;    // consecutive threads take consecutive rows
-        const uint4 v = ld(r0 + r, k0 + j * 8);
-        *reinterpret_cast<uint4*>(dst + ((size_t)j * R + r) * 16) = v;
+        for (int q = threadIdx.x; q < CH; q += NT) {
+            const int r = q % R, j = q / R;    // consecutive threads take consecutive rows
+            const uint4 v = ld(r0 + r, k0 + j * 8);
+            *reinterpret_cast<uint4*>(dst + ((size_t)j * R + r) * 16) = v;
+        }
+    } else {
+        // MN-major: chunk = 8 rows at one K; core matrix (8 K x 16 B), same SBO / LBO
+        constexpr int RG = R / 8;
+#pragma unroll 4
+        for (int q = threadIdx.x; q < CH; q += NT) {
+            const int rg = q % RG, k = q / RG;   // consecutive threads take consecutive row groups
+            const uint4 v = ld(r0 + rg * 8, k0 + k);
+            *reinterpret_cast<uint4*>(dst + ((size_t)(k >> 3) * RG + rg) * 128 + (k & 7) * 16) = v;
+        }
     }
 }
 
@@ -390,7 +380,7 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem;
-    constexpr uint32_t IDESC = idesc_bf16(BN);
+    constexpr uint32_t IDESC = idesc_bf16(BN) | (LA::MN ? 1u << 15 : 0u) | (LB::MN ? 1u << 16 : 0u);
     bool ok = true;
 
     for (int t = kt0; t < kt1; ++t) {
@@ -649,11 +639,17 @@ int ertm_nn_conv3x3_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* dw
 {
     if (!act_ok(x) || !act_ok(dy) || !dw) return ERTM_EINVAL;
     const int P = x->n * x->h * x->w;
-    const int M = dy->c, N = 9 * x->c, K = (P + 7) / 8 * 8;
-    LoadChanT la{act_of(dy), M, P};
-    LoadConv3T lb{act_of(x), N, P};
-    EpiAtomic ep{dw, N, N, M};
-    return rc_of(gemm(la, lb, ep, M, N, K, splitk, err, (cudaStream_t)stream));
+    const int co = dy->c, k9 = 9 * x->c;
+    LoadChanMN ld_dy{act_of(dy), co, P};
+    LoadConv3MN ld_x{act_of(x), k9, P};
+    cudaStream_t st = (cudaStream_t)stream;
+    // the longer of the two operands takes the 128-row side of the MMA
+    if (k9 > co) {
+        EpiAtomic ep{dw, k9, co, k9, 1};
+        return rc_of(gemm(ld_x, ld_dy, ep, k9, co, P, splitk, err, st));
+    }
+    EpiAtomic ep{dw, k9, k9, co, 0};
+    return rc_of(gemm(ld_dy, ld_x, ep, co, k9, P, splitk, err, st));
 }
 
 int ertm_nn_up2(const ertm_nn_act* x, const void* u, const float* bias, const ertm_nn_act* y, int relu, int* err,
@@ -689,11 +685,16 @@ int ertm_nn_up2_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* du, in
 {
     if (!act_ok(x) || !act_ok(dy) || !du || dy->h != 2 * x->h || dy->w != 2 * x->w) return ERTM_EINVAL;
     const int P = x->n * x->h * x->w;
-    const int M = 4 * dy->c, N = x->c, K = (P + 7) / 8 * 8;
-    LoadUp2T la{act_of(dy), M, P};
-    LoadChanT lb{act_of(x), N, P};
-    EpiAtomic ep{du, N, N, M};
-    return rc_of(gemm(la, lb, ep, M, N, K, splitk, err, (cudaStream_t)stream));
+    const int c4 = 4 * dy->c, ci = x->c;
+    LoadUp2MN ld_dy{act_of(dy), c4, P};
+    LoadChanMN ld_x{act_of(x), ci, P};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ci > c4) {
+        EpiAtomic ep{du, ci, c4, ci, 1};
+        return rc_of(gemm(ld_x, ld_dy, ep, ci, c4, P, splitk, err, st));
+    }
+    EpiAtomic ep{du, ci, ci, c4, 0};
+    return rc_of(gemm(ld_dy, ld_x, ep, c4, ci, P, splitk, err, st));
 }
 
 int ertm_nn_pool2(const ertm_nn_act* x, void* y, void* stream)
