@@ -98,6 +98,10 @@ SIGNATURES = {
     "ertm_kernel_launches": (C.c_int64, [_P]),
     "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_write_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
+    "ertm_read_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
+    "ertm_mute_direct": (C.c_int, [C.POINTER(_Shot), _P, C.c_int, C.c_float, C.c_float, C.c_float,
+                                   C.c_float, C.c_float, C.c_int, _P]),
     "ertm_nn_gemm": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "ertm_nn_conv3x3": (C.c_int, [C.POINTER(_NnAct), _P, _P, C.POINTER(_NnAct), C.c_int, _P, _P, _P]),
     "ertm_nn_conv3x3_dgrad": (C.c_int, [C.POINTER(_NnAct), _P, C.POINTER(_NnAct), C.POINTER(_NnAct),
@@ -480,3 +484,62 @@ def rtm_windows(base: Config, vp, vs, rho, windows: list, shots: list, data: lis
     if rc != 0:
         raise ErtmError(rc, buf.value.decode(errors="replace"))
     return tuple(outs)
+
+
+def write_volume_xyz(path: str, vol, cut=None):
+    """Write a (nz, ny, nx) float32 volume in the reference's x-outer, z-inner raw
+    format; cut = (nx, ny, nz, bl, bf, bu) writes only that interior block
+    (output_file_xyz_boundary)."""
+    v = np.ascontiguousarray(vol, np.float32)
+    nzb, nyb, nxb = v.shape
+    nx, ny, nz, bl, bf, bu = cut if cut else (nxb, nyb, nzb, 0, 0, 0)
+    rc = lib().ertm_write_volume_xyz(os.fsencode(path), v.ctypes.data, nxb, nyb, nzb, nx, ny, nz, bl, bf, bu)
+    if rc != 0:
+        raise ErtmError(rc, f"cannot write {path}")
+
+
+def read_volume_xyz(path: str, nx: int, ny: int, nz: int, into=None, offsets=(0, 0, 0)):
+    """Read an x-outer raw float32 volume of nx*ny*nz values into a (nz, ny, nx)
+    array, or into the interior of `into` at offsets (bl, bf, bu)
+    (input_file_xyz_boundary)."""
+    out = np.zeros((nz, ny, nx), np.float32) if into is None else into
+    if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.flags["C_CONTIGUOUS"]):
+        raise ValueError("into must be a C-contiguous float32 array")
+    nzb, nyb, nxb = out.shape
+    bl, bf, bu = offsets
+    rc = lib().ertm_read_volume_xyz(os.fsencode(path), out.ctypes.data, nxb, nyb, nzb, nx, ny, nz, bl, bf, bu)
+    if rc != 0:
+        raise ErtmError(rc, f"cannot read {path}")
+    return out
+
+
+def write_shot_gathers(prefix: str, data):
+    """Recorded data [3][nt][nrec] -> prefix_x.bin, prefix_y.bin, prefix_z.bin, each
+    raw float32 [nrec][nt] (receiver-major, time fastest)."""
+    d = np.asarray(data, np.float32)
+    for c, name in enumerate("xyz"):
+        np.ascontiguousarray(d[c].T).tofile(f"{prefix}_{name}.bin")
+
+
+def read_shot_gathers(prefix: str, nt: int, nrec: int):
+    out = np.zeros((3, nt, nrec), np.float32)
+    for c, name in enumerate("xyz"):
+        out[c] = np.fromfile(f"{prefix}_{name}.bin", np.float32).reshape(nrec, nt).T
+    return out
+
+
+def mute_direct(shot: Shot, data, dt_ms: float, h: tuple, v: float, extra: int = 0, stream_ptr=None):
+    """Zero the direct arrival in recorded data [3][nt][nrec] (numpy or CUDA tensor),
+    in place; h = (dx, dy, dz) in m, v in m/s (see ertm_mute_direct)."""
+    nt = data.shape[1]
+    s = shot.struct()
+    if _is_torch(data):
+        p = _ptr(data, 3 * nt * shot.nrec)
+    else:
+        if not (isinstance(data, np.ndarray) and data.dtype == np.float32 and data.flags["C_CONTIGUOUS"]):
+            raise ValueError("data must be a C-contiguous float32 array")
+        p = data.ctypes.data
+    rc = lib().ertm_mute_direct(C.byref(s), p, nt, h[0], h[1], h[2], dt_ms, v, extra, stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "mute_direct")
+    return data

@@ -267,6 +267,25 @@ int ertm_forward_together_using_real_model_noalloc(const ertm_config *cfg, const
                                                    void *cuda_stream, char *errbuf,
                                                    size_t errlen);
 
+/* ---- files and recorded data (host code) ------------------------------ */
+
+/* Raw float32 volume in the reference's file order, x outer and z inner
+ * (output_file_xyz_boundary / input_file_xyz_boundary, 3D_elastic_RTM/3D_zzzzz:1-139):
+ * the file holds nx*ny*nz values; the array is (nzb, nyb, nxb) with x fastest and
+ * the file's volume sits at offsets (bl, bf, bu) in x, y, z.  Offsets 0 and
+ * full sizes give output_file_xyz / input_file_xyz.  Host arrays. */
+int ertm_write_volume_xyz(const char *path, const float *vol, int nxb, int nyb, int nzb, int nx,
+                          int ny, int nz, int bl, int bf, int bu);
+int ertm_read_volume_xyz(const char *path, float *vol, int nxb, int nyb, int nzb, int nx, int ny,
+                         int nz, int bl, int bf, int bu);
+
+/* Direct-wave mute of recorded data [3][nt][nrx*nry] (host or device), replacing
+ * cut_direct_shot_3D_surface_three_new (3D_forward_or_back_together.cu:135, body
+ * not in the reference tree): zeroes every sample it < ceil(t_d / dt) + shot->nw
+ * + extra, t_d = |receiver - source| / v (straight ray, spacings dx, dy, dz in m). */
+int ertm_mute_direct(const ertm_shot *shot, float *data, int nt, float dx, float dy, float dz,
+                     float dt_ms, float v, int extra, void *stream);
+
 /* ---- learned LSRTM preconditioner: tensor-core network kernels --------
  * No counterpart in the reference (its LSRTM has no learned part).  Building
  * blocks of a 2D U-Net: BF16 NHWC activations, FP32 accumulation in tensor
