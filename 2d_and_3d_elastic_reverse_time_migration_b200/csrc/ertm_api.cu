@@ -827,6 +827,11 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     x->R = c.order / 2;
     x->device = c.device;
     x->g = make_geom(c, x->R);
+    if (x->g.total >= (1LL << 31)) {   // the step kernels index a volume with 32-bit offsets
+        const long long total = x->g.total;
+        delete x;
+        return fail(nullptr, ERTM_EINVAL, "grid too large: %lld floats per padded volume (limit 2^31)", total);
+    }
     int rc = ERTM_OK;
     auto bail = [&](int code) {
         g_create_error = x->err;

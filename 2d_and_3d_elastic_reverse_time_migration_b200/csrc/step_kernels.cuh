@@ -11,7 +11,8 @@
 // `empty` mbarrier.  There is no block-wide barrier in the z loop (warps drift
 // apart by up to S-1 planes) and the issue cost stays off the consumers' path;
 // C-PML memory variables, which live only in the absorbing slabs, come by
-// 4-byte cp.async into a double buffer.
+// 4-byte cp.async into a three-buffer ring, two planes ahead.
+// Cell and slab offsets are 32-bit (a padded volume holds < 2^31 floats).
 // The current plane of the fields that need x or y derivatives is staged in
 // shared memory with an R-wide halo; the z derivatives come from a register
 // queue of 2R+1 planes per field that slides down the column, so every
@@ -84,6 +85,7 @@ __device__ __forceinline__ void cpa4(void* sdst, const void* gsrc)
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
 {
@@ -192,7 +194,7 @@ struct StressShape {
     static constexpr unsigned TX_BYTES = 4u * STAGE;
     static constexpr int PSI = NP * B::C;                       // floats per psi buffer
     static constexpr int NS = 4;                                // ring stages
-    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 2 * PSI) + 16 * NS;
+    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 3 * PSI) + 16 * NS;
 };
 
 template <int R, bool Y, bool CPML, bool PS>
@@ -207,7 +209,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     constexpr int C_TP = NSIG, C_M = NSIG + (PS ? 1 : 0), C_MU = C_M + 1;
     extern __shared__ __align__(128) float sm[];
     float* psibuf = sm + NS * SS::STAGE;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * SS::PSI);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 3 * SS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool leader = (tx == 0 && ty == TYB);
@@ -216,7 +218,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     const int k0 = blockIdx.z * a.kchunk;
     const int k1 = min(k0 + a.kchunk, a.nz);
     const int nk = k1 - k0;
-    const long long sy = a.sy, sz = a.sz;
+    const int sy = (int)a.sy, sz = (int)a.sz;
     const bool act = (i < a.nx) && (j < a.ny);
     const int it = __ldg(a.it_ptr);
     const bool src_on = (it >= 0) && (it < a.nw);
@@ -228,7 +230,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
 
     float* sig[6] = {a.f[F_TXX], a.f[F_TZZ], a.f[F_TXZ], a.f[F_TYY], a.f[F_TXY], a.f[F_TYZ]};
     float* tp = a.f[F_TP];
-    const long long cj = (long long)j * sy + i;
+    const int cj = j * sy + i;
 
     auto issue = [&](int t) {   // leader only: all boxes of iteration t into stage t % S
         const int st = t % NS;
@@ -269,20 +271,20 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         if (!CPML) return;
         float* Ps = psibuf + buf * SS::PSI;
         if (inx) {
-            const long long x = ((long long)p * a.ny + j) * WX + slx;
+            const int x = (p * a.ny + j) * WX + slx;
             cpa4(&Ps[(PX + 0) * CB + cell], a.psi[P_EXX] + x);
             cpa4(&Ps[(PX + 1) * CB + cell], a.psi[P_DXVZ] + x);
             if (Y) cpa4(&Ps[(PX + 2) * CB + cell], a.psi[P_DXVY] + x);
         }
         if (iny) {
-            const long long y = ((long long)p * WY + sly) * a.nx + i;
+            const int y = (p * WY + sly) * a.nx + i;
             cpa4(&Ps[(PY + 0) * CB + cell], a.psi[P_EYY] + y);
             cpa4(&Ps[(PY + 1) * CB + cell], a.psi[P_DYVX] + y);
             cpa4(&Ps[(PY + 2) * CB + cell], a.psi[P_DYVZ] + y);
         }
         if (act && (p < a.w[4] || p >= a.nz - a.w[5])) {
             const int sl = p < a.w[4] ? p : p - a.nz + a.w[4] + a.w[5];
-            const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+            const int z = (sl * a.ny + j) * a.nx + i;
             cpa4(&Ps[(PZ + 0) * CB + cell], a.psi[P_EZZ] + z);
             cpa4(&Ps[(PZ + 1) * CB + cell], a.psi[P_DZVX] + z);
             if (Y) cpa4(&Ps[(PZ + 2) * CB + cell], a.psi[P_DZVY] + z);
@@ -308,23 +310,26 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     float qx[2 * R + 1], qy[2 * R + 1], qz[2 * R + 1];
 #pragma unroll
     for (int q = 0; q < 2 * R; q++) {
-        const long long cc = (long long)(k0 + q - R) * sz + cj;
+        const int cc = (k0 + q - R) * sz + cj;
         qx[q] = vsrc[0][cc];
         qz[q] = vsrc[1][cc];
         if (Y) qy[q] = vsrc[2][cc];
     }
     issue_psi(k0, 0);
-    cpa_wait_all();
+    if (nk > 1) issue_psi(k0 + 1, 1);
+    else cpa_commit();
+    cpa_wait_1();
 
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
         const int st = t % NS;
         if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
-        if (t + 1 < nk) issue_psi(k + 1, (t + 1) & 1);
+        if (t + 2 < nk) issue_psi(k + 2, (t + 2) % 3);
+        else cpa_commit();   // keep one group per iteration
         const float* S = sm + st * SS::STAGE;
         const float* Cc = S + SS::OFF_C;
-        const float* Ps = psibuf + (t & 1) * SS::PSI;
+        const float* Ps = psibuf + (t % 3) * SS::PSI;
         qx[2 * R] = S[SS::OFF_FR + 0 * CB + cell];
         qz[2 * R] = S[SS::OFF_FR + 1 * CB + cell];
         if (Y) qy[2 * R] = S[SS::OFF_FR + 2 * CB + cell];
@@ -351,10 +356,10 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         }
 
         if (act) {
-            const long long c = (long long)k * sz + cj;
+            const int c = k * sz + cj;
             if (CPML) {
                 if (inx) {
-                    const long long x = ((long long)k * a.ny + j) * WX + slx;
+                    const int x = (k * a.ny + j) * WX + slx;
                     float p0 = fmaf(bxf, Ps[(PX + 0) * CB + cell], axf * exx);
                     float p1 = fmaf(bxh, Ps[(PX + 1) * CB + cell], axh * dxvz);
                     a.psi[P_EXX][x] = p0;
@@ -368,7 +373,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
                     }
                 }
                 if (iny) {
-                    const long long y = ((long long)k * WY + sly) * a.nx + i;
+                    const int y = (k * WY + sly) * a.nx + i;
                     float p0 = fmaf(byf, Ps[(PY + 0) * CB + cell], ayf * eyy);
                     float p1 = fmaf(byh, Ps[(PY + 1) * CB + cell], ayh * dyvx);
                     float p2 = fmaf(byh, Ps[(PY + 2) * CB + cell], ayh * dyvz);
@@ -381,7 +386,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
                 }
                 if (k < a.w[4] || k >= a.nz - a.w[5]) {
                     const int sl = k < a.w[4] ? k : k - a.nz + a.w[4] + a.w[5];
-                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    const int z = (sl * a.ny + j) * a.nx + i;
                     const float azf = __ldg(a.pa[2][0] + k), bzf = __ldg(a.pb[2][0] + k);
                     const float azh = __ldg(a.pa[2][1] + k), bzh = __ldg(a.pb[2][1] + k);
                     float p0 = fmaf(bzf, Ps[(PZ + 0) * CB + cell], azf * ezz);
@@ -433,7 +438,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
             qz[q] = qz[q + 1];
             if (Y) qy[q] = qy[q + 1];
         }
-        cpa_wait_all();
+        cpa_wait_1();   // plane t+1's memory variables have landed
         __syncwarp();
         if (tx == 0) mbar_arrive(&bars[NS + st]);   // release the stage
     }
@@ -471,7 +476,7 @@ struct VelShape {
     static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
     static constexpr int PSI = NP * B::C;
     static constexpr int NS = 3;   // ring stages (4 would not leave room for 2 CTAs per SM)
-    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 2 * PSI) + 16 * NS;
+    static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 3 * PSI) + 16 * NS;
 };
 
 template <int R, bool Y, bool CPML, int EPI, bool REC>
@@ -485,7 +490,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     constexpr int TYB = B::TYB, XB = B::XB, XW = B::XW, CB = B::C;
     extern __shared__ __align__(128) float sm[];
     float* psibuf = sm + NS * VS::STAGE;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 2 * VS::PSI);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(psibuf + 3 * VS::PSI);
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool leader = (tx == 0 && ty == TYB);
@@ -494,14 +499,14 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     const int k0 = blockIdx.z * a.kchunk;
     const int k1 = min(k0 + a.kchunk, a.nz);
     const int nk = k1 - k0;
-    const long long sy = a.sy, sz = a.sz;
+    const int sy = (int)a.sy, sz = (int)a.sz;
     const bool act = (i < a.nx) && (j < a.ny);
     const int it = __ldg(a.it_ptr);
     const int rec = ((REC || EPI == EPI_IMAGE) && act) ? receiver_index(a, i, j) : -1;
     const long long nrec = (long long)a.nrx * a.nry;
     const int cell = ty * TX + tx;
     const int gx = i0 + XH, gy = j0 + (Y ? R : 0), gz0 = k0 + R;
-    const long long cj = (long long)j * sy + i;
+    const int cj = j * sy + i;
 
     float* vx = a.f[F_VX];
     float* vy = a.f[F_VY];
@@ -550,20 +555,20 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         if (!CPML) return;
         float* Ps = psibuf + buf * VS::PSI;
         if (inx) {
-            const long long x = ((long long)p * a.ny + j) * WX + slx;
+            const int x = (p * a.ny + j) * WX + slx;
             cpa4(&Ps[(PX + 0) * CB + cell], a.psi[P_DXTXX] + x);
             cpa4(&Ps[(PX + 1) * CB + cell], a.psi[P_DXTXZ] + x);
             if (Y) cpa4(&Ps[(PX + 2) * CB + cell], a.psi[P_DXTXY] + x);
         }
         if (iny) {
-            const long long y = ((long long)p * WY + sly) * a.nx + i;
+            const int y = (p * WY + sly) * a.nx + i;
             cpa4(&Ps[(PY + 0) * CB + cell], a.psi[P_DYTXY] + y);
             cpa4(&Ps[(PY + 1) * CB + cell], a.psi[P_DYTYY] + y);
             cpa4(&Ps[(PY + 2) * CB + cell], a.psi[P_DYTYZ] + y);
         }
         if (act && (p < a.w[4] || p >= a.nz - a.w[5])) {
             const int sl = p < a.w[4] ? p : p - a.nz + a.w[4] + a.w[5];
-            const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+            const int z = (sl * a.ny + j) * a.nx + i;
             cpa4(&Ps[(PZ + 0) * CB + cell], a.psi[P_DZTXZ] + z);
             cpa4(&Ps[(PZ + 1) * CB + cell], a.psi[P_DZTZZ] + z);
             if (Y) cpa4(&Ps[(PZ + 2) * CB + cell], a.psi[P_DZTYZ] + z);
@@ -591,24 +596,27 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     float qxz[2 * R + 1], qyz[2 * R + 1], qzz[2 * R + 1], qtp[2 * R + 1];
 #pragma unroll
     for (int q = 0; q < 2 * R; q++) {
-        const long long cc = (long long)(k0 + q - R) * sz + cj;
+        const int cc = (k0 + q - R) * sz + cj;
         qxz[q] = txz[cc];
         qzz[q] = tzz[cc];
         if (Y) qyz[q] = tyz[cc];
         if (PS) qtp[q] = tp[cc];
     }
     issue_psi(k0, 0);
-    cpa_wait_all();
+    if (nk > 1) issue_psi(k0 + 1, 1);
+    else cpa_commit();
+    cpa_wait_1();
 
     bool ok = true;
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
         const int st = t % NS;
         if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
-        if (t + 1 < nk) issue_psi(k + 1, (t + 1) & 1);
+        if (t + 2 < nk) issue_psi(k + 2, (t + 2) % 3);
+        else cpa_commit();   // keep one group per iteration
         const float* S = sm + st * VS::STAGE;
         const float* Cc = S + VS::O_C;
-        const float* Ps = psibuf + (t & 1) * VS::PSI;
+        const float* Ps = psibuf + (t % 3) * VS::PSI;
         qxz[2 * R] = S[VS::O_FR + 0 * CB + cell];
         qzz[2 * R] = S[VS::O_FR + 1 * CB + cell];
         if (Y) qyz[2 * R] = S[VS::O_FR + VS::FR_TYZ * CB + cell];
@@ -645,10 +653,10 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         }
 
         if (act) {
-            const long long c = (long long)k * sz + cj;
+            const int c = k * sz + cj;
             if (CPML) {
                 if (inx) {
-                    const long long x = ((long long)k * a.ny + j) * WX + slx;
+                    const int x = (k * a.ny + j) * WX + slx;
                     float p0 = fmaf(bxh, Ps[(PX + 0) * CB + cell], axh * dxtxx);
                     float p1 = fmaf(bxf, Ps[(PX + 1) * CB + cell], axf * dxtxz);
                     a.psi[P_DXTXX][x] = p0;
@@ -662,7 +670,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
                     }
                 }
                 if (iny) {
-                    const long long y = ((long long)k * WY + sly) * a.nx + i;
+                    const int y = (k * WY + sly) * a.nx + i;
                     float p0 = fmaf(byf, Ps[(PY + 0) * CB + cell], ayf * dytxy);
                     float p1 = fmaf(byh, Ps[(PY + 1) * CB + cell], ayh * dytyy);
                     float p2 = fmaf(byf, Ps[(PY + 2) * CB + cell], ayf * dytyz);
@@ -675,7 +683,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
                 }
                 if (k < a.w[4] || k >= a.nz - a.w[5]) {
                     const int sl = k < a.w[4] ? k : k - a.nz + a.w[4] + a.w[5];
-                    const long long z = ((long long)sl * a.ny + j) * a.nx + i;
+                    const int z = (sl * a.ny + j) * a.nx + i;
                     const float azf = __ldg(a.pa[2][0] + k), bzf = __ldg(a.pb[2][0] + k);
                     const float azh = __ldg(a.pa[2][1] + k), bzh = __ldg(a.pb[2][1] + k);
                     float p0 = fmaf(bzf, Ps[(PZ + 0) * CB + cell], azf * dztxz);
@@ -776,7 +784,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
             if (Y) qyz[q] = qyz[q + 1];
             if (PS) qtp[q] = qtp[q + 1];
         }
-        cpa_wait_all();
+        cpa_wait_1();   // plane t+1's memory variables have landed
         __syncwarp();
         if (tx == 0) mbar_arrive(&bars[NS + st]);   // release the stage
     }
