@@ -31,6 +31,36 @@ def _dot(a: Sequence[np.ndarray], b: Sequence[np.ndarray]) -> float:
     return float(sum(np.sum(x.astype(np.float64) * y) for x, y in zip(a, b)))
 
 
+class _Sum:
+    """Sums over the ranks of `group` (torch.distributed; identity on one process):
+    the gradient (three volumes) and the scalar norms of CGLS, so every rank holds
+    the same model, direction and step after each iteration."""
+
+    def __init__(self, group):
+        import torch.distributed as dist
+        self.on = dist.is_available() and dist.is_initialized() and \
+            dist.get_world_size(group) > 1
+        self.group = group
+
+    def scalar(self, v: float) -> float:
+        if not self.on:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
+    def volumes(self, g):
+        if not self.on:
+            return g
+        import torch
+        import torch.distributed as dist
+        t = torch.from_numpy(np.stack([x.astype(np.float32) for x in g]))
+        dist.all_reduce(t, group=self.group)
+        return tuple(t[q].numpy().copy() for q in range(len(g)))
+
+
 def _axpy(alpha: float, x, y):
     return tuple((yy + alpha * xx).astype(np.float32) for xx, yy in zip(x, y))
 
@@ -44,17 +74,23 @@ def adjoint_all(ctx, shots, res):
     for s, r in zip(shots, res):
         gs = ctx.born_adjoint(s, r)
         g = gs if g is None else tuple(a + b for a, b in zip(g, gs))
+    if g is None:                      # a rank without shots contributes zero
+        return tuple(np.zeros(ctx.cfg.shape, np.float32) for _ in range(3))
     return tuple(x.astype(np.float32) for x in g)
 
 
 def cgls(ctx, shots: list, data: list, niter: int,
          precond: Callable[[tuple], tuple] | None = None,
-         callback: Callable[[int, float], None] | None = None) -> CGResult:
+         callback: Callable[[int, float], None] | None = None, group=None) -> CGResult:
+    """CGLS on this rank's shots; with torch.distributed initialised, the ranks of
+    `group` each pass their own shots and data, and the gradient (one all-reduce of
+    three volumes per iteration) and the norms are summed over them."""
+    red = _Sum(group)
     shape = ctx.cfg.shape
     m = tuple(np.zeros(shape, np.float32) for _ in range(3))
     r = [d.astype(np.float32).copy() for d in data]            # r = d - F m
-    dnorm = sum(float(np.sum(d.astype(np.float64) ** 2)) for d in data)
-    s = adjoint_all(ctx, shots, r)
+    dnorm = red.scalar(sum(float(np.sum(d.astype(np.float64) ** 2)) for d in data))
+    s = red.volumes(adjoint_all(ctx, shots, r))
     z = precond(s) if precond else s
     p = z
     gamma = _dot(s, z)
@@ -62,12 +98,12 @@ def cgls(ctx, shots: list, data: list, niter: int,
     rnorm = dnorm
     for it in range(niter):
         q = born_all(ctx, shots, p)
-        qq = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q)
+        qq = red.scalar(sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q))
         if qq == 0.0 or gamma == 0.0:
             break
         alpha = gamma / qq
         r_new = [(rr - alpha * qq_).astype(np.float32) for rr, qq_ in zip(r, q)]
-        rn = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new)
+        rn = red.scalar(sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new))
         kind = "precond" if precond else "plain"
         if precond and rn >= rnorm:
             # safeguard: the preconditioned direction did not lower the misfit;
@@ -75,14 +111,14 @@ def cgls(ctx, shots: list, data: list, niter: int,
             p = s
             gamma = _dot(s, s)
             q = born_all(ctx, shots, p)
-            qq = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q)
+            qq = red.scalar(sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q))
             alpha = gamma / qq
             r_new = [(rr - alpha * qq_).astype(np.float32) for rr, qq_ in zip(r, q)]
-            rn = sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new)
+            rn = red.scalar(sum(float(np.sum(x.astype(np.float64) ** 2)) for x in r_new))
             kind = "plain"
         m = _axpy(alpha, p, m)
         r, rnorm = r_new, rn
-        s = adjoint_all(ctx, shots, r)
+        s = red.volumes(adjoint_all(ctx, shots, r))
         z = precond(s) if (precond and kind == "precond") else s
         gamma_new = _dot(s, z)
         beta = gamma_new / gamma if gamma else 0.0
