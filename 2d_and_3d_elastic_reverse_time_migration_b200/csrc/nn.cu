@@ -8,9 +8,10 @@
 // staged in shared memory by all 128 threads through "loaders" that gather 8
 // consecutive K elements (16 bytes) of one row: an implicit im2col for 3x3
 // convolutions on NHWC activations, plain rows of K-major weights, or
-// MN-major gathers (8 channels of one pixel) for the weight gradients.  Two shared-memory stages
-// alternate: while the tensor core works on one, the threads fill the other,
-// and tcgen05.commit on a per-stage mbarrier tells them when a stage is free.
+// MN-major gathers (8 channels of one pixel) for the weight gradients.  The
+// threads copy operand chunks into a ring of 3-4 shared-memory stages with
+// cp.async (zero-fill for padding), several K tiles ahead of the tensor core;
+// tcgen05.commit on a per-stage mbarrier tells them when a stage may be refilled.
 // After the K loop each warp reads its 32 accumulator rows from TMEM
 // (tcgen05.ld 32x32b) and an epilogue functor writes them (bias, ReLU, BF16
 // store, scatter of a transposed convolution, or FP32 atomics for split-K
@@ -109,10 +110,10 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
 }
 
 // ---------------------------------------------------------------------------
-// Operand loaders: 16 bytes = 8 consecutive K elements of row `r` starting at k
-// (k % 8 == 0).  Rows or K past the bounds read zeros.
+// Operand loaders: src(r, k) is the address of 16 bytes = 8 consecutive K
+// elements of row r starting at k (k % 8 == 0), or nullptr where the operand is
+// zero (rows or K past the bounds, convolution padding).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint4 zero4() { return make_uint4(0, 0, 0, 0); }
 
 // NHWC activation view: pixel p = (n*H + y)*W + x, channels [off, off+C) of a
 // pixel stride of cs channels
@@ -126,15 +127,14 @@ struct LoadConv3 {
     Act x;
     int M, K;
     static constexpr bool MN = false;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= M || k >= K) return zero4();
+        if (r >= M || k >= K) return nullptr;
         const int tap = k / x.c, c = k - tap * x.c;
         const int xx = r % x.w, t = r / x.w, yy = t % x.h, n = t / x.h;
         const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
-        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return zero4();
-        const long long q = ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c;
-        return *reinterpret_cast<const uint4*>(x.p + q);
+        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return nullptr;
+        return x.p + ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c;
     }
 };
 
@@ -143,10 +143,10 @@ struct LoadRows {
     const bf16* p;
     int rows, K, ld;
     static constexpr bool MN = false;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= rows || k >= K) return zero4();
-        return *reinterpret_cast<const uint4*>(p + (long long)r * ld + k);
+        if (r >= rows || k >= K) return nullptr;
+        return p + (long long)r * ld + k;
     }
 };
 
@@ -156,15 +156,14 @@ struct LoadUp2 {
     Act dy;      // high-resolution view (h, w = 2x the rows' grid)
     int M, K;
     static constexpr bool MN = false;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= M || k >= K) return zero4();
+        if (r >= M || k >= K) return nullptr;
         const int ab = k / dy.c, o = k - ab * dy.c;
         const int lw = dy.w / 2, lh = dy.h / 2;
         const int j = r % lw, t = r / lw, i = t % lh, n = t / lh;
         const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
-        const long long q = ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o;
-        return *reinterpret_cast<const uint4*>(dy.p + q);
+        return dy.p + ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o;
     }
 };
 
@@ -177,10 +176,10 @@ struct LoadChanMN {
     Act a;
     int rows, P;
     static constexpr bool MN = true;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= rows || k >= P) return zero4();
-        return *reinterpret_cast<const uint4*>(a.p + (long long)k * a.cs + a.off + r);
+        if (r >= rows || k >= P) return nullptr;
+        return a.p + (long long)k * a.cs + a.off + r;
     }
 };
 
@@ -189,14 +188,14 @@ struct LoadConv3MN {
     Act x;
     int rows, P;   // rows = 9 C
     static constexpr bool MN = true;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= rows || k >= P) return zero4();
+        if (r >= rows || k >= P) return nullptr;
         const int tap = r / x.c, c = r - tap * x.c;
         const int xx = k % x.w, t = k / x.w, yy = t % x.h, n = t / x.h;
         const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
-        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return zero4();
-        return *reinterpret_cast<const uint4*>(x.p + ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c);
+        if (sy < 0 || sy >= x.h || sx < 0 || sx >= x.w) return nullptr;
+        return x.p + ((long long)(n * x.h + sy) * x.w + sx) * x.cs + x.off + c;
     }
 };
 
@@ -205,14 +204,14 @@ struct LoadUp2MN {
     Act dy;
     int rows, P;   // rows = 4 C
     static constexpr bool MN = true;
-    __device__ __forceinline__ uint4 operator()(int r, int k) const
+    __device__ __forceinline__ const bf16* src(int r, int k) const
     {
-        if (r >= rows || k >= P) return zero4();
+        if (r >= rows || k >= P) return nullptr;
         const int ab = r / dy.c, o = r - ab * dy.c;
         const int lw = dy.w / 2, lh = dy.h / 2;
         const int j = k % lw, t = k / lw, i = t % lh, n = t / lh;
         const int y = 2 * i + (ab >> 1), x = 2 * j + (ab & 1);
-        return *reinterpret_cast<const uint4*>(dy.p + ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o);
+        return dy.p + ((long long)(n * dy.h + y) * dy.w + x) * dy.cs + dy.off + o;
     }
 };
 
@@ -321,13 +320,31 @@ struct EpiAtomic {
 // ---------------------------------------------------------------------------
 // The GEMM kernel
 // ---------------------------------------------------------------------------
+// ring depth: four stages up to BN = 64 (up to 72 KB), three at BN = 128 (96 KB)
+template <int BN>
+struct Ring {
+    static constexpr int N = BN >= 128 ? 3 : 4;
+};
 template <int BN>
 struct Smem {
-    alignas(128) uint8_t a[2][BM * BK * 2];
-    alignas(128) uint8_t b[2][BN * BK * 2];
-    uint64_t bar[2];
+    static constexpr int NS = Ring<BN>::N;
+    alignas(128) uint8_t a[NS][BM * BK * 2];
+    alignas(128) uint8_t b[NS][BN * BK * 2];
+    uint64_t bar[NS];
     uint32_t tmem;
 };
+
+__device__ __forceinline__ void cp16(void* sdst, const void* gsrc)
+{
+    // 16 bytes global -> shared, asynchronous; a null source zero-fills
+    const uint32_t n = gsrc ? 16u : 0u;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(su32(sdst)),
+                 "l"(gsrc ? gsrc : sdst), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // stage one operand tile: rows [r0, r0 + R), K chunk [k0, k0 + 64)
 template <int R, class L>
@@ -339,8 +356,7 @@ __device__ __forceinline__ void stage(uint8_t* dst, const L& ld, int r0, int k0)
 #pragma unroll 4
         for (int q = threadIdx.x; q < CH; q += NT) {
             const int r = q % R, j = q / R;    // consecutive threads take consecutive rows
-            const uint4 v = ld(r0 + r, k0 + j * 8);
-            *reinterpret_cast<uint4*>(dst + ((size_t)j * R + r) * 16) = v;
+            cp16(dst + ((size_t)j * R + r) * 16, ld.src(r0 + r, k0 + j * 8));
         }
     } else {
         // MN-major: chunk = 8 rows at one K; core matrix (8 K x 16 B), same SBO / LBO
@@ -348,8 +364,7 @@ __device__ __forceinline__ void stage(uint8_t* dst, const L& ld, int r0, int k0)
 #pragma unroll 4
         for (int q = threadIdx.x; q < CH; q += NT) {
             const int rg = q % RG, k = q / RG;   // consecutive threads take consecutive row groups
-            const uint4 v = ld(r0 + rg * 8, k0 + k);
-            *reinterpret_cast<uint4*>(dst + ((size_t)(k >> 3) * RG + rg) * 128 + (k & 7) * 16) = v;
+            cp16(dst + ((size_t)(k >> 3) * RG + rg) * 128 + (k & 7) * 16, ld.src(r0 + rg * 8, k0 + k));
         }
     }
 }
@@ -365,9 +380,9 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
     const int KT = (K + BK - 1) / BK;
     const int kt0 = blockIdx.z * kt_per, kt1 = min(KT, kt0 + kt_per);
 
+    constexpr int NS = Smem<BN>::NS;
     if (threadIdx.x == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
+        for (int q = 0; q < NS; q++) mbar_init(&S.bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -382,17 +397,26 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
     const uint32_t tmem = S.tmem;
     constexpr uint32_t IDESC = idesc_bf16(BN) | (LA::MN ? 1u << 15 : 0u) | (LB::MN ? 1u << 16 : 0u);
     bool ok = true;
-
-    for (int t = kt0; t < kt1; ++t) {
-        const int u = t - kt0, s = u & 1;
-        if (u >= 2 && ok) ok = mbar_wait(&S.bar[s], ((u >> 1) - 1) & 1);   // MMAs of u-2 done
-        stage<BM>(S.a[s], la, m0, t * BK);
-        stage<BN>(S.b[s], lb, n0, t * BK);
-        proxy_fence();
-        __syncthreads();
+    const int nu = kt1 - kt0;
+    // every thread copies its chunks of K tile u into slot u % NS with cp.async, one
+    // commit group per tile (empty groups keep the count uniform)
+    auto issue = [&](int u) {
+        if (u < nu) {
+            const int sl = u % NS;
+            stage<BM>(S.a[sl], la, m0, (kt0 + u) * BK);
+            stage<BN>(S.b[sl], lb, n0, (kt0 + u) * BK);
+        }
+        cp_commit();
+    };
+    for (int u = 0; u < NS - 1; u++) issue(u);
+    for (int u = 0; u < nu; ++u) {
+        cp_wait<NS - 2>();        // this thread's copies of tile u have landed
+        proxy_fence();            // ... and are visible to the tensor core's async proxy
+        __syncthreads();          // ... for every thread's chunks
+        const int sl = u % NS;
         if (threadIdx.x == 0 && ok) {
             tc_fence_after();
-            const uint32_t a0 = su32(S.a[s]), b0 = su32(S.b[s]);
+            const uint32_t a0 = su32(S.a[sl]), b0 = su32(S.b[sl]);
 #pragma unroll
             for (int j = 0; j < BK / 16; j++) {
                 // K step j covers the core-matrix columns 2j, 2j+1
@@ -400,11 +424,15 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
                 const uint64_t db = sdesc(b0 + (uint32_t)(2 * j * BN * 16), BN * 16);
                 umma(tmem, da, db, IDESC, (u > 0 || j > 0) ? 1u : 0u);
             }
-            umma_commit(&S.bar[s]);
+            umma_commit(&S.bar[sl]);
         }
+        // refill slot (u - 1) % NS with tile u + NS - 1 once tile u-1's MMAs read it
+        const int un = u + NS - 1;
+        if (un < nu && u >= 1 && ok) ok = mbar_wait(&S.bar[(u - 1) % NS], ((u - 1) / NS) & 1);
+        issue(ok ? un : nu);
     }
-    const int nu = kt1 - kt0;
-    if (nu > 0 && ok) ok = mbar_wait(&S.bar[(nu - 1) & 1], ((nu - 1) >> 1) & 1);
+    cp_wait<0>();
+    if (nu > 0 && ok) ok = mbar_wait(&S.bar[(nu - 1) % NS], ((nu - 1) / NS) & 1);
     // the other stage's last commit precedes it, so every MMA has completed;
     // the TMEM loads below are warp-collective, so the decision is block-uniform
     const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
