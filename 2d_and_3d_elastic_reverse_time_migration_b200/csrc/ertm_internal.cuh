@@ -19,7 +19,7 @@ namespace ertm {
 constexpr int TX = 32;        // x tile = one warp
 constexpr int TY3 = 8;        // y tile of the 3D kernels
 constexpr int CTAS3 = 2;      // resident CTAs per SM of the 3D step kernels
-constexpr int TY2 = 4;        // y (= independent 2D shot) tile of the 2D kernels
+constexpr int TY2 = 1;        // y tile of the 2D kernels (a 2D grid has one y row)
 constexpr int XH = 8;         // allocated x halo, floats (>= R, 32-byte aligned)
 
 enum Field {

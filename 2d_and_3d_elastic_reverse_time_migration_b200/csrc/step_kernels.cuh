@@ -138,7 +138,7 @@ __device__ __forceinline__ void tma3(float* dst, const CUtensorMap* map, int x, 
         : "memory");
 }
 
-// Box geometry of the staged tiles (all sizes multiples of 128 bytes)
+// Box geometry of the staged tiles
 template <int R, bool Y>
 struct Boxes {
     static constexpr int TYB = Y ? TY3 : TY2;
@@ -150,6 +150,11 @@ struct Boxes {
     static constexpr int YH = TYB + 2 * YB;                     // y-halo box height
     static constexpr int Yb = TX * YH;
     static constexpr int XY = XW * YH;
+    // shared-memory slot sizes: a TMA box must land on a 128-byte boundary, so
+    // slots round up to 32 floats (a no-op for the 3D tiles; one-row 2D tiles
+    // have 40- or 48-float halo boxes)
+    static constexpr int XP = (X + 31) / 32 * 32;
+    static constexpr int XYP = (XY + 31) / 32 * 32;
 };
 
 // Stage ring of NS stages: plane t goes to stage t % NS.  bars[s] ("full")
@@ -188,10 +193,12 @@ struct StressShape {
     static constexpr int NC = NSIG + (PS ? 1 : 0) + 2;          // + tp + M + MU
     static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
     // stage: v tiles (XY), fronts (C), cells (C)
-    static constexpr int OFF_FR = NV * B::XY;
+    static constexpr int OFF_FR = NV * B::XYP;
     static constexpr int OFF_C = OFF_FR + NV * B::C;
     static constexpr int STAGE = OFF_C + NC * B::C;             // floats
-    static constexpr unsigned TX_BYTES = 4u * STAGE;
+    static constexpr unsigned TX_BYTES = 4u * (NV * B::XY + NV * B::C + NC * B::C);   // box bytes
+    static_assert(B::C % 32 == 0 && OFF_FR % 32 == 0 && OFF_C % 32 == 0 && STAGE % 32 == 0,
+                  "TMA boxes must start on 128-byte boundaries");
     static constexpr int PSI = NP * B::C;                       // floats per psi buffer
     static constexpr int NS = 4;                                // ring stages
     static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 3 * PSI) + 16 * NS;
@@ -240,7 +247,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         mbar_expect_tx(bar, SS::TX_BYTES);
 #pragma unroll
         for (int f = 0; f < NV; f++) {
-            tma3(S + f * B::XY, &maps.v[f], gx - XB, gy - B::YB, z, bar);
+            tma3(S + f * B::XYP, &maps.v[f], gx - XB, gy - B::YB, z, bar);
             tma3(S + SS::OFF_FR + f * CB, &maps.vc[f], gx, gy, z + R, bar);
         }
 #pragma unroll
@@ -334,9 +341,9 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         qz[2 * R] = S[SS::OFF_FR + 1 * CB + cell];
         if (Y) qy[2 * R] = S[SS::OFF_FR + 2 * CB + cell];
         // tiles: (TX+2XB) wide, (TYB+2YB) high; the cell sits at row ty+YB, column tx+XB
-        const float* Tx = S + 0 * B::XY + (ty + B::YB) * XW + tx + XB;
-        const float* Tz = S + 1 * B::XY + (ty + B::YB) * XW + tx + XB;
-        const float* Ty = S + 2 * B::XY + (ty + B::YB) * XW + tx + XB;
+        const float* Tx = S + 0 * B::XYP + (ty + B::YB) * XW + tx + XB;
+        const float* Tz = S + 1 * B::XYP + (ty + B::YB) * XW + tx + XB;
+        const float* Ty = S + 2 * B::XYP + (ty + B::YB) * XW + tx + XB;
 
         float exx = 0.f, dxvz = 0.f, dxvy = 0.f, eyy = 0.f, dyvx = 0.f, dyvz = 0.f;
         float ezz = 0.f, dzvx = 0.f, dzvy = 0.f;
@@ -454,12 +461,12 @@ struct VelShape {
     static constexpr bool PS = (EPI != EPI_NONE);
     // tiles: txx (X), txz (X), txy (XY), tyy (Y), tyz (Y), tp (XY; X in 2D)
     static constexpr int O_TXX = 0;
-    static constexpr int O_TXZ = O_TXX + B::X;
-    static constexpr int O_TXY = O_TXZ + B::X;
-    static constexpr int O_TYY = O_TXY + (Y ? B::XY : 0);
+    static constexpr int O_TXZ = O_TXX + B::XP;
+    static constexpr int O_TXY = O_TXZ + B::XP;
+    static constexpr int O_TYY = O_TXY + (Y ? B::XYP : 0);
     static constexpr int O_TYZ = O_TYY + (Y ? B::Yb : 0);
     static constexpr int O_TP = O_TYZ + (Y ? B::Yb : 0);
-    static constexpr int O_FR = O_TP + (PS ? B::XY : 0);
+    static constexpr int O_FR = O_TP + (PS ? B::XYP : 0);
     // fronts: txz, tzz, (tyz), (tp)
     static constexpr int NFR = 2 + (Y ? 1 : 0) + (PS ? 1 : 0);
     static constexpr int FR_TYZ = 2, FR_TP = Y ? 3 : 2;
@@ -472,7 +479,12 @@ struct VelShape {
     static constexpr int NC = C_B + 1 + (PS ? 1 : 0);
     static constexpr int O_C = O_FR + NFR * B::C;
     static constexpr int STAGE = O_C + NC * B::C;
-    static constexpr unsigned TX_BYTES = 4u * STAGE;
+    static constexpr unsigned TX_BYTES =    // box bytes (slots may be padded)
+        4u * (2 * B::X + (Y ? B::XY + 2 * B::Yb : 0) + (PS ? B::XY : 0) + NFR * B::C + NC * B::C);
+    static_assert(B::C % 32 == 0 && O_TXZ % 32 == 0 && O_TXY % 32 == 0 && O_TYY % 32 == 0 &&
+                      O_TYZ % 32 == 0 && O_TP % 32 == 0 && O_FR % 32 == 0 && O_C % 32 == 0 &&
+                      STAGE % 32 == 0,
+                  "TMA boxes must start on 128-byte boundaries");
     static constexpr int NP = CPML ? (Y ? 9 : 4) : 0;
     static constexpr int PSI = NP * B::C;
     static constexpr int NS = 3;   // ring stages (4 would not leave room for 2 CTAs per SM)
