@@ -1336,9 +1336,9 @@ void visco_fit(int nm, double qp, double qs, double f0, double* tau_sigma, doubl
 
 int born_check(ertm_ctx* c, const ertm_shot* s)
 {
-    if (!c->g.two_d) return fail(c, ERTM_ENOTSUP, "Born operators: 2D grids only in this build");
+    if (!c->g.two_d) return fail(c, ERTM_ENOTSUP, "Born operators support 2D grids only");
     if (c->cfg.boundary == ERTM_BOUNDARY_CPML)
-        return fail(c, ERTM_ENOTSUP, "Born operators: sponge boundaries only in this build");
+        return fail(c, ERTM_ENOTSUP, "Born operators support sponge boundaries only");
     if (!c->model_set[1]) return fail(c, ERTM_ESTATE, "migration model not set");
     int rc = validate_shot(c, s, true);
     if (rc) return rc;

@@ -11,8 +11,7 @@ hand-written kernels too.  Torch only allocates the buffers (plumbing) and
 calls nothing but the library on them.
 
 Activations are NHWC BF16; channel counts are padded to multiples of 8 (input
-3 -> 8, output 3 -> 16).  The reference has no learned component; this is the
-north star's pattern (c).
+3 -> 8, output 3 -> 16).  The reference has no learned component.
 """
 from __future__ import annotations
 

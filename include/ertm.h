@@ -51,7 +51,7 @@ extern "C" {
 #define ERTM_ENOMEM   -2   /* device or host allocation failed */
 #define ERTM_ECUDA    -3   /* CUDA runtime error */
 #define ERTM_ESTATE   -4   /* call out of order (e.g. receiver pass before source pass) */
-#define ERTM_ENOTSUP  -5   /* configuration not supported by this build */
+#define ERTM_ENOTSUP  -5   /* configuration not supported by the library */
 #define ERTM_EDEVICE  -6   /* a device-side check failed (bounded wait expired, bad index) */
 
 /* absorbing boundary kinds */

@@ -153,7 +153,7 @@ int orc_image_given(long n, const float *ex, const float *ez, const float *rpx, 
 
 /* Threads used by the OpenMP loops (1 if built without OpenMP). */
 int orc_threads(void);
-/* sizeof(REAL) of this build. */
+/* sizeof(REAL) of the loaded library (8 or 4). */
 int orc_real_size(void);
 
 #ifdef __cplusplus

@@ -3,8 +3,8 @@
  * reference's CPU helper files use (alloc/free wrappers, the `complex` struct,
  * PI, warn/err).  SU itself is not vendored in the reference tree.  Only the
  * arithmetic-free plumbing is supplied here; every numeric line that the
- * golden vectors exercise is the reference's own, compiled from
- * /root/reference where it lies.  Used only to generate tests/golden fixtures.
+ * golden vectors exercise is the reference's own, compiled from the
+ * reference tree where it lies.  Used only to generate tests/golden fixtures.
  */
 #pragma once
 #include <math.h>

@@ -40,7 +40,7 @@ int get(float* h, const float* d, size_t n)
 // fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization (viscoelastic_equation.cu:184-325)
 // with tao = strain = 1 (no attenuation: memory variables stay zero) and
 // modul_p = vp^2, modul_s = vs^2: one elastic stress half-step with damping.
-// nx % 32 == 0, nz % 16 == 0.  coe_x = dt/1000/dx (the driver that sets it is absent).
+// nx % 32 == 0, nz % 16 == 0.  coe_x = dt/1000/dx (the reference host code that sets it is absent).
 extern "C" int ref_stress_step(int nx, int nz, float dt_ms, float dx, float dz, const float* coe7,
                                const float* vp, const float* vs, const float* rho, const float* att,
                                const float* vx, const float* vz, const float* txx, const float* tzz,
