@@ -321,9 +321,13 @@ class UNet:
         self.backward(G["out"])
         return loss / cnt
 
-    def step(self, x, target, lr=1e-3):
-        """One Adam step on the MSE between forward(x) and target ((n, h, w, 3) float32)."""
+    def step(self, x, target, lr=1e-3, group=None):
+        """One Adam step on the MSE between forward(x) and target ((n, h, w, 3) float32).
+        With torch.distributed initialised, every rank passes its own batch and the
+        gradients are averaged over the ranks of `group` (data parallel, NCCL) before
+        the update, so the replicas stay identical."""
         loss = self.loss_grad(x, target)
+        average_gradients([t for p in self.params.values() for t in (p.g, p.bg)], group)
         self.t += 1
         for p in self.params.values():
             self.ops.adam(p.w, p.g, p.m, p.v, p.wb, lr, self.t)
@@ -346,6 +350,23 @@ class UNet:
             else:
                 f += 2 * (pix // 4) * 4 * p.co * p.ci
         return f
+
+
+def average_gradients(tensors, group=None):
+    """All-reduce (mean) a list of gradient tensors over the ranks of `group`, as one
+    flat bucket; a no-op on one process."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) < 2:
+        return
+    flat = torch.cat([t.reshape(-1) for t in tensors])
+    dist.all_reduce(flat, group=group)
+    flat /= dist.get_world_size(group)
+    off = 0
+    for t in tensors:
+        n = t.numel()
+        t.copy_(flat[off:off + n].view_as(t))
+        off += n
 
 
 def _out_view(t, n, h, w):

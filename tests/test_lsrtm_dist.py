@@ -86,3 +86,27 @@ def test_distributed_cgls_equals_single_process(tmp_path):
         assert np.allclose(got["misfit"], ref.misfit, rtol=1e-4)
         for a, b in zip(got["m"], ref.m):
             assert np.allclose(a.numpy(), b, rtol=1e-3, atol=1e-5 * np.abs(b).max())
+
+
+def _avg_worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    if REPO not in sys.path:
+        sys.path.insert(0, REPO)
+    nn = importlib.import_module(PKG + ".nn")
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        g = [torch.full((3, 4), float(rank + 1)), torch.arange(5, dtype=torch.float32) * (rank + 1)]
+        nn.average_gradients(g)
+        torch.save(g, f"{out}/g{rank}.pt")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_unet_gradient_averaging_over_two_ranks(tmp_path):
+    mp.spawn(_avg_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    for r in range(2):
+        g = torch.load(f"{tmp_path}/g{r}.pt")
+        assert torch.allclose(g[0], torch.full((3, 4), 1.5))
+        assert torch.allclose(g[1], torch.arange(5, dtype=torch.float32) * 1.5)
