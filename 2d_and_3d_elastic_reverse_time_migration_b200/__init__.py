@@ -100,6 +100,11 @@ SIGNATURES = {
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_write_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
     "ertm_read_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
+    "ertm_laplace_filter": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                      C.c_float]),
+    "ertm_hilbert_z": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int]),
+    "ertm_bell_smooth": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P]),
+    "ertm_taper_x": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P]),
     "ertm_mute_direct": (C.c_int, [C.POINTER(_Shot), _P, C.c_int, C.c_float, C.c_float, C.c_float,
                                    C.c_float, C.c_float, C.c_int, _P]),
     "ertm_nn_gemm": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
@@ -543,3 +548,68 @@ def mute_direct(shot: Shot, data, dt_ms: float, h: tuple, v: float, extra: int =
     if rc != 0:
         raise ErtmError(rc, "mute_direct")
     return data
+
+
+def laplace_filter(img, vp, h: tuple):
+    """Laplacian image filter (see ertm_laplace_filter); returns a new (nz, ny, nx) array."""
+    out = np.array(img, np.float32, order="C", copy=True)
+    v = np.ascontiguousarray(vp, np.float32)
+    if out.ndim != 3 or v.shape != out.shape:
+        raise ValueError("img and vp must be (nz, ny, nx) arrays of one shape")
+    nz, ny, nx = out.shape
+    rc = lib().ertm_laplace_filter(out.ctypes.data, v.ctypes.data, nx, ny, nz, *h)
+    if rc != 0:
+        raise ErtmError(rc, "laplace_filter")
+    return out
+
+
+def hilbert_z(img):
+    """Hilbert transform along depth of every column (see ertm_hilbert_z)."""
+    x = np.ascontiguousarray(img, np.float32)
+    out = np.zeros_like(x)
+    nz, ny, nx = x.shape
+    rc = lib().ertm_hilbert_z(x.ctypes.data, out.ctypes.data, nx, ny, nz)
+    if rc != 0:
+        raise ErtmError(rc, "hilbert_z")
+    return out
+
+
+AXIS_X, AXIS_Y, AXIS_Z = 1, 2, 4
+
+
+def _arr_ptr(a, n):
+    if _is_torch(a):
+        return _ptr(a, n)
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]):
+        raise ValueError("arrays must be C-contiguous float32")
+    if a.size != n:
+        raise ValueError("array size mismatch")
+    return a.ctypes.data
+
+
+def bell_smooth(img, rbell: int, axes: int = AXIS_X | AXIS_Z, stream_ptr=None):
+    """Truncated Gaussian smoothing of an (nz, ny, nx) array (numpy or CUDA tensor)
+    along the named axes (see ertm_bell_smooth); returns a new array."""
+    nz, ny, nx = img.shape
+    n = nx * ny * nz
+    if _is_torch(img):
+        import torch
+        src = img.contiguous()
+        out, work = torch.empty_like(src), torch.empty_like(src)
+    else:
+        src = np.ascontiguousarray(img, np.float32)
+        out, work = np.empty_like(src), np.empty_like(src)
+    rc = lib().ertm_bell_smooth(_arr_ptr(src, n), _arr_ptr(out, n), _arr_ptr(work, n), nx, ny, nz,
+                                rbell, axes, stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "bell_smooth")
+    return out
+
+
+def taper_x(img, left: int, right: int, power: int = 3, stream_ptr=None):
+    """Cosine-power edge taper in x, in place (see ertm_taper_x)."""
+    nz, ny, nx = img.shape
+    rc = lib().ertm_taper_x(_arr_ptr(img, nx * ny * nz), nx, ny, nz, left, right, power, stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "taper_x")
+    return img

@@ -55,7 +55,7 @@ extern "C" {
 #define ERTM_EDEVICE  -6   /* a device-side check failed (bounded wait expired, bad index) */
 
 /* absorbing boundary kinds */
-#define ERTM_BOUNDARY_CPML          0  /* convolutional PML (north-star default) */
+#define ERTM_BOUNDARY_CPML          0  /* convolutional PML (default) */
 #define ERTM_BOUNDARY_SPONGE_COS    1  /* reference 3D damping, 3D_zzzzz:261-369 */
 #define ERTM_BOUNDARY_SPONGE_CUBIC  2  /* reference 2D damping, zzzzz:238-325 */
 
@@ -278,6 +278,32 @@ int ertm_write_volume_xyz(const char *path, const float *vol, int nxb, int nyb, 
                           int ny, int nz, int bl, int bf, int bu);
 int ertm_read_volume_xyz(const char *path, float *vol, int nxb, int nyb, int nzb, int nx, int ny,
                          int nz, int bl, int bf, int bu);
+
+/* Image post-filters (host arrays (nz, ny, nx), x fastest).  Laplacian filter of
+ * cpu_laplace (3D_elastic_RTM/zzzzz:1110-1147; 3D adds the y term): in place,
+ * img <- vp^2 (-laplacian(img)) / 4 with the reference's edge handling.  Hilbert
+ * transform along depth of suhilbt (3D_elastic_RTM/zzzzz:1018-1066) into out.  Both
+ * work on the image interior the reference cuts out of its padded arrays. */
+int ertm_laplace_filter(float *img, const float *vp, int nx, int ny, int nz, float dx, float dy,
+                        float dz);
+int ertm_hilbert_z(const float *img, float *out, int nx, int ny, int nz);
+
+/* Gradient post-filters, host or device arrays (nz, ny, nx).  Truncated Gaussian
+ * smoothing with weights exp(-i^2 / (2 rbell)), |i| <= rbell <= 64, renormalised
+ * where the window leaves the array, one pass per axis in `axes` (z, then y, then x)
+ * — cuda_bell_smoothz_new / cuda_bell_smoothx_new / cuda_bell_smooth_2d
+ * (2D_elastic_RTM/viscoelastic_equation.cu:2528-2604).  `work` (n floats, same
+ * memory space) is needed with two or more axes; `in` may equal `out` with exactly
+ * two.  Device arrays run on `stream`; the call returns when the passes are done. */
+#define ERTM_AXIS_X 1
+#define ERTM_AXIS_Y 2
+#define ERTM_AXIS_Z 4
+int ertm_bell_smooth(const float *in, float *out, float *work, int nx, int ny, int nz, int rbell,
+                     int axes, void *stream);
+/* Cosine-power edge taper in x of cuda_attenuation_truncation
+ * (viscoelastic_equation.cu:2881-2926; there left = offset_left/3, right =
+ * offset_right/3, power 3), in place, host or device. */
+int ertm_taper_x(float *img, int nx, int ny, int nz, int left, int right, int power, void *stream);
 
 /* Direct-wave mute of recorded data [3][nt][nrx*nry] (host or device), replacing
  * cut_direct_shot_3D_surface_three_new (3D_forward_or_back_together.cu:135, body

@@ -59,3 +59,4 @@ def test_direct_wave_mute_on_the_device_matches_the_host(ertm):
     dev = torch.from_numpy(d).cuda()
     ertm.mute_direct(shot, dev, 0.5, (5.0, 5.0, 5.0), 1800.0, extra=3)
     assert np.array_equal(dev.cpu().numpy(), host)
+
