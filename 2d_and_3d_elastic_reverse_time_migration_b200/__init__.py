@@ -92,6 +92,11 @@ SIGNATURES = {
     "ertm_rtm_batch": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(_P), _P, _P, _P]),
     "ertm_get_wavefield": (C.c_int, [_P, C.c_int, _P]),
     "ertm_get_excitation": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "ertm_set_angles": (C.c_int, [_P, C.c_int]),
+    "ertm_get_angles": (C.c_int, [_P, _P, _P]),
+    "ertm_angle_compensate": (C.c_int, [_P, _P, _P, _P, C.c_longlong, C.c_int, _P]),
+    "ertm_adcig_bin": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                 C.c_int, C.c_float, _P]),
     "ertm_divcurl": (C.c_int, [_P, C.c_int, _P, _P, _P, _P]),
     "ertm_propagate": (C.c_int, [_P, C.c_int, C.POINTER(_Shot), C.c_int]),
     "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
@@ -384,6 +389,19 @@ class Context:
                                              *[_ptr(e, n, True) for e in ev]))
         return {"amp": amp, "time": t, "evx": ev[0], "evy": ev[1], "evz": ev[2], "etp": ev[3]}
 
+    def set_angles(self, on: bool = True):
+        """Capture source / receiver P-wave propagation angles at the excitation
+        time in the following passes (2D; see ertm_set_angles)."""
+        self._ck(self._L.ertm_set_angles(self._h, 1 if on else 0))
+
+    def get_angles(self, src: bool = True, rcv: bool = True):
+        """(source angle, receiver angle) in degrees, (nz, 1, nx); None where not asked."""
+        n = self.ncell
+        a = np.zeros(self.cfg.shape, np.float32) if src else None
+        b = np.zeros(self.cfg.shape, np.float32) if rcv else None
+        self._ck(self._L.ertm_get_angles(self._h, _ptr(a, n, True), _ptr(b, n, True)))
+        return a, b
+
     def divcurl(self, which: int = MIGRATION_MODEL):
         n = self.ncell
         outs = [np.zeros(self.cfg.shape, np.float32) for _ in range(4)]
@@ -613,3 +631,51 @@ def taper_x(img, left: int, right: int, power: int = 3, stream_ptr=None):
     if rc != 0:
         raise ErtmError(rc, "taper_x")
     return img
+
+
+COMP_PP, COMP_PS, COMP_PP_SIGN, COMP_PS_SIGN = 0, 1, 2, 3
+
+
+def angle_compensate(img, src_angle, rcv_angle, kind: int = COMP_PP, stream_ptr=None):
+    """Angle-dependent compensation of a PP or PS image (see ertm_angle_compensate);
+    numpy arrays or CUDA tensors of one shape; returns a new array."""
+    n = int(np.prod(img.shape))
+    if _is_torch(img):
+        import torch
+        out = torch.empty_like(img)
+    else:
+        img = np.ascontiguousarray(img, np.float32)
+        src_angle = np.ascontiguousarray(src_angle, np.float32)
+        rcv_angle = np.ascontiguousarray(rcv_angle, np.float32)
+        out = np.empty_like(img)
+    rc = lib().ertm_angle_compensate(_arr_ptr(img, n), _arr_ptr(src_angle, n), _arr_ptr(rcv_angle, n),
+                                     _arr_ptr(out, n), n, kind, stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "angle_compensate")
+    return out
+
+
+def adcig_bin(img, angle, nang: int, dangle: float, sx: int, zmin: int = 50, slope: float = 1.2,
+              normal=None, cig=None, stream_ptr=None):
+    """Add one shot's image to angle-domain common-image gathers
+    cig[2*nang+1][nz][nx] (see ertm_adcig_bin); img and angle are (nz, 1, nx) or
+    (nz, nx).  Returns cig (allocated when None)."""
+    nz, nx = img.shape[0], img.shape[-1]
+    n = nx * nz
+    if cig is None:
+        if _is_torch(img):
+            import torch
+            cig = torch.zeros((2 * nang + 1, nz, nx), dtype=torch.float32, device=img.device)
+        else:
+            cig = np.zeros((2 * nang + 1, nz, nx), np.float32)
+    if not _is_torch(img):
+        img = np.ascontiguousarray(img, np.float32)
+        angle = np.ascontiguousarray(angle, np.float32)
+        normal = None if normal is None else np.ascontiguousarray(normal, np.float32)
+    rc = lib().ertm_adcig_bin(_arr_ptr(img, n), _arr_ptr(angle, n),
+                              None if normal is None else _arr_ptr(normal, n),
+                              _arr_ptr(cig, (2 * nang + 1) * n), nx, nz, nang, dangle, sx, zmin, slope,
+                              stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "adcig_bin")
+    return cig

@@ -97,6 +97,40 @@ __global__ void k_axpy(long long n, const float* __restrict__ x, float* __restri
 }
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
+// P-wave propagation angle at the cells whose excitation time is the current step
+// (caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM,
+// 2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284), from the Poynting vector of
+// sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
+// cells around the cell, sxz = sum px pz and szz = sum pz^2 (products in float,
+// sums in double, as the reference), angle = atan(sxz / szz) in degrees from the
+// z axis, written only where szz != 0.  2D grids: the x halo (XH >= 2) and the z
+// halo (R >= 2) hold zeros, so the window needs no bounds checks.  Runs after the
+// velocity kernel of the step and before the step counter advances.
+__global__ void k_angle(Geom g, KArgs a, float* __restrict__ ang)
+{
+    const int it = *a.it_ptr;
+    const float* tp = a.f[F_TP];
+    const float* vxp = a.f[F_VXP];
+    const float* vzp = a.f[F_VZP];
+    const long long n = (long long)g.nx * g.nz;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n;
+         m += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(m % g.nx), k = (int)(m / g.nx);
+        const long long c = k * g.sz + i;
+        if (a.ex_time[c] != it) continue;
+        double sxz = 0.0, szz = 0.0;
+        for (int dk = -2; dk <= 2; dk++)
+            for (int di = -2; di <= 2; di++) {
+                const long long q = c + dk * g.sz + di;
+                const float t = tp[q];
+                const float px = -t * vxp[q], pz = -t * vzp[q];
+                sxz += (double)(px * pz);
+                szz += (double)(pz * pz);
+            }
+        if (szz != 0.0) ang[c] = (float)(atan(sxz / szz) * (180.0 / 3.14159265358979323846));
+    }
+}
+
 template <int R>
 __device__ __forceinline__ float dplus(const float* f, long long c, long long s, const float* cf)
 {
@@ -212,6 +246,12 @@ cudaError_t launch_advance(int* it_ptr, int delta, cudaStream_t s)
 cudaError_t launch_set_int(int* p, int v, cudaStream_t s)
 {
     k_set_int<<<1, 1, 0, s>>>(p, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_angle(const Geom& g, const KArgs& a, float* ang, cudaStream_t s)
+{
+    k_angle<<<grid_for((long long)g.nx * g.nz), 256, 0, s>>>(g, a, ang);
     return cudaGetLastError();
 }
 

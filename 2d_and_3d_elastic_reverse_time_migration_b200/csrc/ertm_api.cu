@@ -74,6 +74,11 @@ struct ertm_ctx {
     float* ex_v_base[3] = {nullptr};
     float* ex_tp_base = nullptr;
     float* img_base[3] = {nullptr};
+    // propagation angles at the excitation time (2D, ertm_set_angles): [0] source
+    // wavefield, written by the source pass; [1] receiver wavefield, receiver pass
+    float* ang_base[2] = {nullptr, nullptr};
+    bool angles = false;
+    bool have_src_angle = false, have_rcv_angle = false;
     bool have_excitation = false;
     int last_shot_key = 0;
 
@@ -715,9 +720,13 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
     }
     const StressMaps sm = stress_maps(c, which);
     const VelMaps vm = vel_maps(c, which, epi);
+    float* ang = nullptr;
+    if (c->angles && mode == MODE_SOURCE) ang = c->ang_base[0] + c->g.off0;
+    if (c->angles && mode == MODE_RECEIVER) ang = c->ang_base[1] + c->g.off0;
     auto one_step = [&]() -> cudaError_t {
         cudaError_t e = launch_stress(R, c->g, a, sm, cpml, psplit, c->stream);
         if (e == cudaSuccess) e = launch_velocity(R, c->g, a, vm, cpml, epi, record, c->stream);
+        if (e == cudaSuccess && ang) e = launch_angle(c->g, a, ang, c->stream);
         if (e == cudaSuccess) e = launch_advance(c->it_d, dir, c->stream);
         return e;
     };
@@ -748,7 +757,7 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
         if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "graph time loop: %s", cudaGetErrorString(e));
     }
     for (; done < nsteps; done++) CK(c, one_step());
-    c->launches += 3LL * nsteps;
+    c->launches += (ang ? 4LL : 3LL) * nsteps;
     return check_device_error(c);
 }
 
@@ -936,6 +945,8 @@ int ertm_destroy(ertm_ctx* c)
         cudaFree(c->img_base[q]);
     }
     cudaFree(c->ex_tp_base);
+    cudaFree(c->ang_base[0]);
+    cudaFree(c->ang_base[1]);
     cudaFree(c->stage);
     cudaFree(c->traces);
     cudaFree(c->wavelet);
@@ -997,7 +1008,40 @@ int ertm_set_grid(ertm_ctx* c, int nx, int ny, int nt, int src_steps)
     c->att_ready = false;
     c->model_set[0] = c->model_set[1] = false;
     c->have_excitation = false;
+    c->have_src_angle = c->have_rcv_angle = false;
     c->born.ready = false;
+    return ERTM_OK;
+}
+
+int ertm_set_angles(ertm_ctx* c, int on)
+{
+    if (!c) return ERTM_EINVAL;
+    if (on != 0 && on != 1) return fail(c, ERTM_EINVAL, "on = %d", on);
+    if (on && !c->g.two_d) return fail(c, ERTM_ENOTSUP, "propagation angles need a 2D grid");
+    CK(c, cudaSetDevice(c->device));
+    if (on && !c->ang_base[0]) {
+        float* dummy;
+        for (int q = 0; q < 2; q++) {
+            int rc = alloc_volume(c, &c->ang_base[q], &dummy);
+            if (rc) return rc;
+        }
+    }
+    if (!on) c->have_src_angle = c->have_rcv_angle = false;
+    c->angles = on != 0;
+    return ERTM_OK;
+}
+
+int ertm_get_angles(ertm_ctx* c, float* src_angle, float* rcv_angle)
+{
+    if (!c) return ERTM_EINVAL;
+    if (!c->angles) return fail(c, ERTM_ESTATE, "angle capture is off");
+    if (src_angle && !c->have_src_angle) return fail(c, ERTM_ESTATE, "no source pass with angles has run");
+    if (rcv_angle && !c->have_rcv_angle) return fail(c, ERTM_ESTATE, "no receiver pass with angles has run");
+    CK(c, cudaSetDevice(c->device));
+    int rc = copy_out_volume(c, c->ang_base[0] + c->g.off0, src_angle);
+    if (rc == ERTM_OK) rc = copy_out_volume(c, c->ang_base[1] + c->g.off0, rcv_angle);
+    if (rc) return rc;
+    CK(c, cudaStreamSynchronize(c->stream));
     return ERTM_OK;
 }
 
@@ -1075,11 +1119,14 @@ int ertm_forward_together_using_smoothed_model(ertm_ctx* c, const ertm_shot* s)
     for (int q = 0; q < 3; q++)
         if (c->ex_v_base[q]) CK(c, cudaMemsetAsync(c->ex_v_base[q], 0, sizeof(float) * g.total, c->stream));
     CK(c, cudaMemsetAsync(c->ex_tp_base, 0, sizeof(float) * g.total, c->stream));
+    if (c->angles) CK(c, cudaMemsetAsync(c->ang_base[0], 0, sizeof(float) * g.total, c->stream));
     int nsrc = c->cfg.src_steps > 0 ? c->cfg.src_steps : 2 * c->cfg.nt / 3;
     c->have_excitation = false;
+    c->have_src_angle = false;
     if ((rc = run_pass(c, 1, s, MODE_SOURCE, nsrc, nullptr))) return rc;
     CK(c, cudaStreamSynchronize(c->stream));
     c->have_excitation = true;
+    c->have_src_angle = c->angles;
     return ERTM_OK;
 }
 
@@ -1095,6 +1142,8 @@ int ertm_backward_together_using_smoothed_model(ertm_ctx* c, const ertm_shot* s,
     if ((rc = ensure_images(c))) return rc;
     const Geom& g = c->g;
     for (int q = 0; q < 3; q++) CK(c, cudaMemsetAsync(c->img_base[q], 0, sizeof(float) * g.total, c->stream));
+    c->have_rcv_angle = false;
+    if (c->angles) CK(c, cudaMemsetAsync(c->ang_base[1], 0, sizeof(float) * g.total, c->stream));
     const long long nrec = nrec_of(s);
     const size_t nd = 3 * (size_t)c->cfg.nt * nrec;
     float* traces = nullptr;
@@ -1107,6 +1156,7 @@ int ertm_backward_together_using_smoothed_model(ertm_ctx* c, const ertm_shot* s,
         }
     }
     if ((rc = run_pass(c, 1, s, MODE_RECEIVER, c->cfg.nt, traces))) return rc;
+    c->have_rcv_angle = c->angles;
     float* outs[3] = {img_pp, img_ps, img_tp};
     for (int q = 0; q < 3; q++)
         if ((rc = copy_out_volume(c, c->img_base[q] + g.off0, outs[q]))) return rc;

@@ -10,7 +10,8 @@
 // kernels on its gradients, 2D_elastic_RTM/viscoelastic_equation.cu:2528-2988):
 // the truncated Gaussian "bell" smoothing of cuda_bell_smooth{x,z}_new /
 // cuda_bell_smooth_2d, and the cosine-power edge taper of
-// cuda_attenuation_truncation.
+// cuda_attenuation_truncation; the angle-dependent compensation of PP/PS images and
+// the angle-domain common-image gathers of 2D_elastic_RTM/elastic_2D_kernel_3.cu.
 //
 // Arrays are (nz, ny, nx), x fastest; ny = 1 is a 2D section.
 #include <cuda_runtime.h>
@@ -87,6 +88,63 @@ __global__ void k_taper(float* img, long long n, int nx, int left, int right, in
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
          c += (long long)gridDim.x * blockDim.x)
         img[c] *= taper_at((int)(c % nx), nx, left, right, power);
+}
+
+// Angle-dependent amplitude compensation of one cell (open angle d = src - rcv, degrees)
+__host__ __device__ inline float compensate(float img, float src, float rcv, int kind)
+{
+    const double rad = 3.14159265358979323846 / 180.0;
+    const float d = src - rcv;
+    switch (kind) {
+    case ERTM_COMP_PP: {
+        const float den = (fabsf(d) >= 87.5f && fabsf(d) <= 92.5f) ? 0.1f : (float)cos(d * rad);
+        return img / (den + 0.0001f);
+    }
+    case ERTM_COMP_PS: {
+        const float den = fabsf(d) <= 2.5f ? 0.1f : (float)sin(fabs(d * rad));
+        return img / (den + 0.0001f);
+    }
+    case ERTM_COMP_PP_SIGN: {
+        const float den = (float)cos(d * rad);
+        const float v = den <= 0.f ? -img : img;
+        return -v / (fabsf(den) + 0.03f);
+    }
+    default: {   // ERTM_COMP_PS_SIGN
+        const float den = (float)fabs(sin(d * rad)) + 0.1f;
+        return -img / den;
+    }
+    }
+}
+
+__global__ void k_compensate(const float* img, const float* src, const float* rcv, float* out, long long n,
+                             int kind)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+        out[c] = compensate(img[c], src[c], rcv[c], kind);
+}
+
+// Angle bin of cell (ix, iz), or -1 when the cell is masked out or its angle is past
+// the last bin.
+__host__ __device__ inline int adcig_bin(float ang, int ix, int iz, int nang, float dangle, int sx, int zmin,
+                                         float slope)
+{
+    if (!(iz > zmin && iz > slope * (ix - sx) && iz > slope * (sx - ix))) return -1;
+    const int r = (int)((fabsf(ang) + 0.5f) / dangle);
+    if (r >= nang) return -1;
+    return ang >= 0.f ? nang + r : nang - r;
+}
+
+__global__ void k_adcig(const float* img, const float* ang, const float* normal, float* cig, int nx, int nz,
+                        int nang, float dangle, int sx, int zmin, float slope)
+{
+    const long long n = (long long)nx * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        const float a = ang[c] - (normal ? normal[c] : 0.f);
+        const int b = adcig_bin(a, (int)(c % nx), (int)(c / nx), nang, dangle, sx, zmin, slope);
+        if (b >= 0) cig[b * n + c] += img[c];   // one cell per thread: no two threads share an address
+    }
 }
 
 int grid_for(long long n)
@@ -250,6 +308,65 @@ int ertm_taper_x(float* img, int nx, int ny, int nz, int left, int right, int po
     std::vector<float> f(nx);
     for (int i = 0; i < nx; i++) f[i] = taper_at(i, nx, left, right, power);
     for (long long c = 0; c < n; c++) img[c] *= f[c % nx];
+    return ERTM_OK;
+}
+
+// Angle-dependent compensation of a PP or PS image (2D_elastic_RTM/elastic_2D_kernel_3.cu):
+// with d = src_angle - rcv_angle in degrees,
+//   ERTM_COMP_PP       img / (cos d + 1e-4), cos d replaced by 0.1 for 87.5 <= |d| <= 92.5
+//                      (imaging_pp_compensate_dependent_angle_2D, :622-648)
+//   ERTM_COMP_PS       img / (sin |d| + 1e-4), sin |d| replaced by 0.1 for |d| <= 2.5
+//                      (imaging_ps_compensate_dependent_angle_2D, :650-676)
+//   ERTM_COMP_PP_SIGN  -sign(cos d) img / (|cos d| + 0.03), sign(0) = -1
+//                      (cuda_ex_com_pp_ps_sign + imaging_pp_compensate_dependent_angle_2D_new,
+//                      :698-741)
+//   ERTM_COMP_PS_SIGN  -img / (|sin d| + 0.1)  (imaging_ps_compensate_dependent_angle_2D_new,
+//                      :743-761)
+// The reference applies them cell by cell at the cell's excitation time, when the
+// cell's image and both angles are final; here they run on the finished arrays.
+int ertm_angle_compensate(const float* img, const float* src_angle, const float* rcv_angle, float* out,
+                          long long n, int kind, void* stream)
+{
+    if (!img || !src_angle || !rcv_angle || !out || n < 0 || kind < ERTM_COMP_PP || kind > ERTM_COMP_PS_SIGN)
+        return ERTM_EINVAL;
+    const bool dev = on_device(img);
+    if (on_device(src_angle) != dev || on_device(rcv_angle) != dev || on_device(out) != dev) return ERTM_EINVAL;
+    if (n == 0) return ERTM_OK;
+    if (dev) {
+        k_compensate<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(img, src_angle, rcv_angle, out, n, kind);
+        if (cudaGetLastError() != cudaSuccess) return ERTM_ECUDA;
+        return cudaStreamSynchronize((cudaStream_t)stream) == cudaSuccess ? ERTM_OK : ERTM_ECUDA;
+    }
+    for (long long c = 0; c < n; c++) out[c] = compensate(img[c], src_angle[c], rcv_angle[c], kind);
+    return ERTM_OK;
+}
+
+// Angle-domain common-image gathers of one shot (set_adcigs_for_ex,
+// 2D_elastic_RTM/elastic_2D_kernel_3.cu:489-511): the angle of a cell is
+// angle - normal (normal may be NULL: 0); r = (int)((|angle| + 0.5) / dangle); cells
+// with r < nang, iz > zmin and iz > slope |ix - sx| add their image value to bin
+// nang + r (angle >= 0) or nang - r (angle < 0) of cig [2 nang + 1][nz][nx], so bin b
+// holds angles near (b - nang) dangle.  The reference's mask uses zmin 50, slope 1.2.
+// Accumulates into cig; host or device arrays.
+int ertm_adcig_bin(const float* img, const float* angle, const float* normal, float* cig, int nx, int nz,
+                   int nang, float dangle, int sx, int zmin, float slope, void* stream)
+{
+    if (!img || !angle || !cig || nx < 1 || nz < 1 || nang < 1 || !(dangle > 0)) return ERTM_EINVAL;
+    const bool dev = on_device(img);
+    if (on_device(angle) != dev || on_device(cig) != dev || (normal && on_device(normal) != dev))
+        return ERTM_EINVAL;
+    const long long n = (long long)nx * nz;
+    if (dev) {
+        k_adcig<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(img, angle, normal, cig, nx, nz, nang, dangle, sx,
+                                                              zmin, slope);
+        if (cudaGetLastError() != cudaSuccess) return ERTM_ECUDA;
+        return cudaStreamSynchronize((cudaStream_t)stream) == cudaSuccess ? ERTM_OK : ERTM_ECUDA;
+    }
+    for (long long c = 0; c < n; c++) {
+        const float a = angle[c] - (normal ? normal[c] : 0.f);
+        const int b = adcig_bin(a, (int)(c % nx), (int)(c / nx), nang, dangle, sx, zmin, slope);
+        if (b >= 0) cig[b * n + c] += img[c];
+    }
     return ERTM_OK;
 }
 

@@ -305,6 +305,36 @@ int ertm_bell_smooth(const float *in, float *out, float *work, int nx, int ny, i
  * offset_right/3, power 3), in place, host or device. */
 int ertm_taper_x(float *img, int nx, int ny, int nz, int left, int right, int power, void *stream);
 
+/* Propagation angles (2D grids).  With capture on, the source pass records at each
+ * cell the P-wave propagation angle of the source wavefield at the cell's
+ * excitation time, and the receiver pass that of the receiver wavefield at the
+ * same time: Poynting vector p = -tp (vxp, vzp), angle = atan(sum px pz / sum pz^2)
+ * over the 5 x 5 cells around the cell, in degrees from the z axis; a cell whose
+ * window sum of pz^2 is zero keeps 0.  Replaces caculate_ex_angle_pp_only_RTM /
+ * caculate_ex_angle_rp_only_RTM on sum_poynting's vectors
+ * (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284, elastic_2D_kernel_2.cu:8-30).
+ * One extra kernel per step while on; ERTM_ENOTSUP on 3D grids.  ertm_get_angles
+ * copies either array out (NULL skips; host or device pointers, (nz, 1, nx)). */
+int ertm_set_angles(ertm_ctx *ctx, int on);
+int ertm_get_angles(ertm_ctx *ctx, float *src_angle, float *rcv_angle);
+
+/* Angle-dependent compensation of a PP or PS image from the two angle arrays
+ * (elastic_2D_kernel_3.cu:622-761), n cells, host or device arrays (all alike). */
+#define ERTM_COMP_PP       0  /* img / (cos d + 1e-4), 0.1 near 90 degrees */
+#define ERTM_COMP_PS       1  /* img / (sin|d| + 1e-4), 0.1 near 0 degrees */
+#define ERTM_COMP_PP_SIGN  2  /* -sign(cos d) img / (|cos d| + 0.03) */
+#define ERTM_COMP_PS_SIGN  3  /* -img / (|sin d| + 0.1) */
+int ertm_angle_compensate(const float *img, const float *src_angle, const float *rcv_angle,
+                          float *out, long long n, int kind, void *stream);
+
+/* Angle-domain common-image gathers of one shot, accumulated into
+ * cig[2*nang+1][nz][nx] (set_adcigs_for_ex, elastic_2D_kernel_3.cu:489-511): a cell
+ * with iz > zmin and iz > slope*|ix - sx| adds its image value to bin
+ * nang +/- (int)((|angle - normal| + 0.5) / dangle) when that offset is below nang.
+ * normal may be NULL.  The reference uses zmin = 50, slope = 1.2. */
+int ertm_adcig_bin(const float *img, const float *angle, const float *normal, float *cig, int nx,
+                   int nz, int nang, float dangle, int sx, int zmin, float slope, void *stream);
+
 /* Direct-wave mute of recorded data [3][nt][nrx*nry] (host or device), replacing
  * cut_direct_shot_3D_surface_three_new (3D_forward_or_back_together.cu:135, body
  * not in the reference tree): zeroes every sample it < ceil(t_d / dt) + shot->nw

@@ -439,6 +439,44 @@ static long rec_cell(const orc_state *S, const orc_shot *s, int r, int *ok)
 static int image_pp_ps(real ex, real ey, real ez, real px, real py, real pz, real sx, real sy,
                        real sz, real *pp, real *ps);
 
+/* P-wave propagation angle at cell (i, k) of a 2D state, restating
+ * caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM
+ * (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284) on the Poynting vector of
+ * sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
+ * cells around (i, k) (cells outside the grid count as zero), sxz = sum px pz and
+ * szz = sum pz^2, angle = atan(sxz / szz) in degrees from the z axis.  Returns 0
+ * and leaves *out alone where szz == 0, as the reference does. */
+static int window_angle(const orc_state *S, int i, int k, float *out)
+{
+    const orc_grid *g = &S->g;
+    double sxz = 0.0, szz = 0.0;
+    for (int dk = -2; dk <= 2; dk++)
+        for (int di = -2; di <= 2; di++) {
+            int ii = i + di, kk = k + dk;
+            if (ii < 0 || ii >= g->nx || kk < 0 || kk >= g->nz) continue;
+            long c = AT(S, ii, 0, kk);
+            double tp = S->f[F_TP][c];
+            double px = -tp * S->f[F_VXP][c], pz = -tp * S->f[F_VZP][c];
+            sxz += px * pz;
+            szz += pz * pz;
+        }
+    if (szz == 0.0) return 0;
+    *out = (float)(atan(sxz / szz) * 180.0 / SU_PI);
+    return 1;
+}
+
+static void capture_angles(const orc_state *S, const orc_excitation *ex, int it, float *angle)
+{
+    const orc_grid *g = &S->g;
+    if (!S->two_d || !angle) return;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < g->nz; k++)
+        for (int i = 0; i < g->nx; i++) {
+            long m = (long)k * g->nx + i;
+            if (ex->time[m] == it) window_angle(S, i, k, &angle[m]);
+        }
+}
+
 /* One time step `it` of a pass, in the order of
  * 3D_elastic_RTM/3D_forward_or_back_together.cu:25-154 (model), :173-289 (source),
  * :310-452 (receiver). */
@@ -507,6 +545,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                         ex->second2[m] = (float)a2;
                     }
                 }
+        capture_angles(S, ex, it, ex->src_angle);
     }
     if (mode == ORC_MODE_RECEIVER && ex) {
         /* imaging_inner_product_ex / imaging_correlation_ex, restating
@@ -530,6 +569,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                     real et = ex->etp[m];
                     if (ptp && et != 0) ptp[m] = (float)(S->f[F_TP][c] / et);
                 }
+        capture_angles(S, ex, it, ex->rcv_angle);
     }
 }
 
@@ -568,6 +608,8 @@ int orc_run_pass(const orc_grid *g, const float *vp, const float *vs, const floa
     orc_state *S = state_new(g, vp, vs, rho);
     if (!S) return -2;
     long n = (long)g->nx * g->ny * g->nz;
+    if (mode == ORC_MODE_SOURCE && ex && ex->src_angle) memset(ex->src_angle, 0, sizeof(float) * n);
+    if (mode == ORC_MODE_RECEIVER && ex->rcv_angle) memset(ex->rcv_angle, 0, sizeof(float) * n);
     if (mode == ORC_MODE_SOURCE && ex) {
         memset(ex->amp2, 0, sizeof(float) * n);
         memset(ex->second2, 0, sizeof(float) * n);

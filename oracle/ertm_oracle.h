@@ -78,6 +78,10 @@ typedef struct {
     float *amp2, *second2;
     int   *time;
     float *evx, *evy, *evz, *etp;
+    /* 2D only, optional (NULL = off): P-wave propagation angle in degrees at the
+     * excitation time, of the source wavefield (written by the source pass) and of
+     * the receiver wavefield (written by the receiver pass); see orc_window_angle. */
+    float *src_angle, *rcv_angle;
 } orc_excitation;
 
 /* ---- model-independent helpers --------------------------------------- */

@@ -45,7 +45,8 @@ class Excitation(C.Structure):
     _fields_ = [("amp2", C.POINTER(C.c_float)), ("second2", C.POINTER(C.c_float)),
                 ("time", C.POINTER(C.c_int)), ("evx", C.POINTER(C.c_float)),
                 ("evy", C.POINTER(C.c_float)), ("evz", C.POINTER(C.c_float)),
-                ("etp", C.POINTER(C.c_float))]
+                ("etp", C.POINTER(C.c_float)), ("src_angle", C.POINTER(C.c_float)),
+                ("rcv_angle", C.POINTER(C.c_float))]
 
 
 _libs: dict[int, C.CDLL] = {}
@@ -184,7 +185,12 @@ def make_shot(sx, sy, sz, wavelet, rx0=0, nrx=1, drx=1, ry0=0, nry=1, dry=1, rz=
 
 
 class ExcitationArrays:
-    def __init__(self, shape):
+    """Excitation state; with angles=True (2D) also the source and receiver P-wave
+    propagation angles at the excitation time."""
+
+    def __init__(self, shape, angles: bool = False):
+        self.src_angle = np.zeros(shape, np.float32) if angles else None
+        self.rcv_angle = np.zeros(shape, np.float32) if angles else None
         self.amp2 = np.zeros(shape, np.float32)
         self.second2 = np.zeros(shape, np.float32)
         self.time = np.zeros(shape, np.int32)
@@ -198,6 +204,7 @@ class ExcitationArrays:
         e.amp2, e.second2 = _fp(self.amp2), _fp(self.second2)
         e.time = self.time.ctypes.data_as(C.POINTER(C.c_int))
         e.evx, e.evy, e.evz, e.etp = _fp(self.evx), _fp(self.evy), _fp(self.evz), _fp(self.etp)
+        e.src_angle, e.rcv_angle = _fp(self.src_angle), _fp(self.rcv_angle)
         return e
 
 
