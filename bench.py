@@ -52,9 +52,10 @@ def parse():
     ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
-    ap.add_argument("--workload", default="shot", choices=["shot", "windows", "unet", "lsrtm"],
+    ap.add_argument("--workload", default="shot", choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op"],
                     help="windows: batched aperture windows; unet: one U-Net training step at "
-                         "256x512, batch 16; lsrtm: learned vs plain CG (each its own line)")
+                         "256x512, batch 16; lsrtm: learned vs plain CG (each its own line); "
+                         "lsrtm-op: Born forward + adjoint per shot on the 880x480 GSLS-3 LSRTM grid")
     ap.add_argument("--train-models", type=int, default=48)
     ap.add_argument("--test-models", type=int, default=6)
     ap.add_argument("--train-steps", type=int, default=1500)
@@ -318,6 +319,69 @@ def run_lsrtm(args):
         "cases": [_fmt_case(r) for r in rows]}), flush=True)
 
 
+def run_lsrtm_op(args):
+    """LSRTM operators at the LSRTM workload's size: 880 x 480 cells (800 x 400 interior +
+    40-cell sponge) at 5 m, GSLS with 3 mechanisms (Qp 100, Qs 50, f0 15 Hz), dt 0.5 ms,
+    4000 steps, 800 receivers, checkpoints every 200 steps.  Times the Born forward and
+    its adjoint (one CG iteration's work per shot) over `--shots` shots of the 40-shot
+    layout and projects one 40-shot iteration and the 20-iteration run."""
+    import numpy as np
+    import torch
+    L = importlib.import_module(PKG + ".learned")
+    syn = importlib.import_module(PKG + ".synthetic")
+    ertm = importlib.import_module(PKG)
+    nshots = max(1, min(args.shots, 40))
+    g = L.Geometry(nzi=400, nxi=800, h=5.0, pml=40, nt=4000, dt_ms=0.5, nshots=40, f0=15.0,
+                   sigma=10.0, visco=(3, 100.0, 50.0, 15.0))
+    vp, vs, rho = syn.faulted_2d(20261203, g.nzi, g.nxi, g.h)
+    pads = (g.pml, g.pml, 0, 0, g.pml, g.pml)
+    vp, vs, rho = (syn.pad_edges(a, pads) for a in (vp, vs, rho))
+    svp, svs, srho = (syn.gaussian_smooth(a, g.sigma) for a in (vp, vs, rho))
+    true = tuple((a / b - 1.0).astype(np.float32) for a, b in ((vp, svp), (vs, svs), (rho, srho)))
+    nz, _, nx = vp.shape
+    cfg = ertm.Config(nx=nx, ny=1, nz=nz, dx=g.h, dy=g.h, dz=g.h, dt_ms=g.dt_ms, nt=g.nt, order=8,
+                      boundary=ertm.BOUNDARY_SPONGE_CUBIC, pml=pads, sponge_coef=150.0,
+                      checkpoint_every=200, visco_nmech=3, visco_qp=100.0, visco_qs=50.0, visco_f0=15.0)
+    ctx = ertm.Context(cfg)
+    ctx.set_model(ertm.MIGRATION_MODEL, svp, svs, srho)
+    w = syn.ricker(g.f0, g.dt_ms / 1000.0)
+    xs = np.linspace(g.pml + 4, nx - g.pml - 5, 40).round().astype(int)
+    rz = g.pml + 2
+    shots = [ertm.Shot(int(x), 0, rz, wavelet=w, rx0=g.pml, nrx=nx - 2 * g.pml, drx=1, rz=rz)
+             for x in xs[np.linspace(0, 39, nshots).round().astype(int)]]
+    # warm-up: one forward and one adjoint on the first shot (allocations, graphs)
+    d0 = ctx.born_forward(shots[0], *true)
+    ctx.born_adjoint(shots[0], d0)
+    torch.cuda.synchronize()
+    tf = ta = 0.0
+    data = []
+    for s in shots:
+        t0 = time.perf_counter()
+        d = ctx.born_forward(s, *true)
+        tf += time.perf_counter() - t0
+        data.append(d)
+    for s, d in zip(shots, data):
+        t0 = time.perf_counter()
+        ctx.born_adjoint(s, d)
+        ta += time.perf_counter() - t0
+    cell_steps = float(nx * nz) * g.nt
+    per_shot = (tf + ta) / nshots
+    print(json.dumps({
+        "metric": "LSRTM operator throughput (Born forward + adjoint, GSLS-3)",
+        "value": round(2 * cell_steps * nshots / (tf + ta) / 1e9, 3), "unit": "Gcell-steps/s",
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "LSRTM 880x480 (800x400 + 40-cell sponge), dx 5 m, GSLS-3 Qp 100 Qs 50 "
+                               "f0 15 Hz, dt 0.5 ms, nt 4000, 800 receivers, checkpoints every 200 steps",
+                   "shots_timed": nshots},
+        "forward_s_per_shot": round(tf / nshots, 3), "adjoint_s_per_shot": round(ta / nshots, 3),
+        "forward_gcell_steps_s": round(cell_steps * nshots / tf / 1e9, 3),
+        "adjoint_gcell_steps_s": round(cell_steps * nshots / ta / 1e9, 3),
+        "projected_cg_iteration_40_shots_s": round(40 * per_shot, 1),
+        "projected_20_iterations_s": round(20 * 40 * per_shot, 1),
+        "timing": "host wall clock around each synchronous call, host arrays in and out"}), flush=True)
+    ctx.close()
+
+
 def _fmt_case(r):
     out = {}
     for k, v in r.items():
@@ -339,6 +403,8 @@ def main():
         return run_unet(args)
     if args.workload == "lsrtm":
         return run_lsrtm(args)
+    if args.workload == "lsrtm-op":
+        return run_lsrtm_op(args)
     import numpy as np
     import torch
     import torch.distributed as dist
