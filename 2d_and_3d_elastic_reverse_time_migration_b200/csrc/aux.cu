@@ -101,8 +101,10 @@ __global__ void k_set_int(int* p, int v) { *p = v; }
 // (caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM,
 // 2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284), from the Poynting vector of
 // sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
-// cells around the cell, sxz = sum px pz and szz = sum pz^2 (products in float,
-// sums in double, as the reference), angle = atan(sxz / szz) in degrees from the
+// cells around the cell, sxz = sum px pz and szz = sum pz^2 (p in float, products
+// and sums in double, as the reference: its Poynting arrays are float and it forms
+// 1.0 * px * pz; a float product would underflow where the receiver wavefield is
+// still only the stencil's numerical precursor), angle = atan(sxz / szz) in degrees from the
 // z axis, written only where szz != 0.  2D grids: the x halo (XH >= 2) and the z
 // halo (R >= 2) hold zeros, so the window needs no bounds checks.  Runs after the
 // velocity kernel of the step and before the step counter advances.
@@ -124,8 +126,8 @@ __global__ void k_angle(Geom g, KArgs a, float* __restrict__ ang)
                 const long long q = c + dk * g.sz + di;
                 const float t = tp[q];
                 const float px = -t * vxp[q], pz = -t * vzp[q];
-                sxz += (double)(px * pz);
-                szz += (double)(pz * pz);
+                sxz += (double)px * (double)pz;
+                szz += (double)pz * (double)pz;
             }
         if (szz != 0.0) ang[c] = (float)(atan(sxz / szz) * (180.0 / 3.14159265358979323846));
     }

@@ -439,17 +439,18 @@ static long rec_cell(const orc_state *S, const orc_shot *s, int r, int *ok)
 static int image_pp_ps(real ex, real ey, real ez, real px, real py, real pz, real sx, real sy,
                        real sz, real *pp, real *ps);
 
-/* P-wave propagation angle at cell (i, k) of a 2D state, restating
+/* P-wave propagation angle at cell (i, k) of a 2D state (and, when asked, the
+ * window's P energy), restating
  * caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM
  * (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284) on the Poynting vector of
  * sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
  * cells around (i, k) (cells outside the grid count as zero), sxz = sum px pz and
  * szz = sum pz^2, angle = atan(sxz / szz) in degrees from the z axis.  Returns 0
  * and leaves *out alone where szz == 0, as the reference does. */
-static int window_angle(const orc_state *S, int i, int k, float *out)
+static int window_angle(const orc_state *S, int i, int k, float *out, float *energy)
 {
     const orc_grid *g = &S->g;
-    double sxz = 0.0, szz = 0.0;
+    double sxz = 0.0, szz = 0.0, sxx = 0.0;
     for (int dk = -2; dk <= 2; dk++)
         for (int di = -2; di <= 2; di++) {
             int ii = i + di, kk = k + dk;
@@ -459,13 +460,16 @@ static int window_angle(const orc_state *S, int i, int k, float *out)
             double px = -tp * S->f[F_VXP][c], pz = -tp * S->f[F_VZP][c];
             sxz += px * pz;
             szz += pz * pz;
+            sxx += px * px;
         }
+    if (energy) *energy = (float)(sxx + szz);
     if (szz == 0.0) return 0;
     *out = (float)(atan(sxz / szz) * 180.0 / SU_PI);
     return 1;
 }
 
-static void capture_angles(const orc_state *S, const orc_excitation *ex, int it, float *angle)
+static void capture_angles(const orc_state *S, const orc_excitation *ex, int it, float *angle,
+                           float *energy)
 {
     const orc_grid *g = &S->g;
     if (!S->two_d || !angle) return;
@@ -473,7 +477,7 @@ static void capture_angles(const orc_state *S, const orc_excitation *ex, int it,
     for (int k = 0; k < g->nz; k++)
         for (int i = 0; i < g->nx; i++) {
             long m = (long)k * g->nx + i;
-            if (ex->time[m] == it) window_angle(S, i, k, &angle[m]);
+            if (ex->time[m] == it) window_angle(S, i, k, &angle[m], energy ? &energy[m] : NULL);
         }
 }
 
@@ -545,7 +549,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                         ex->second2[m] = (float)a2;
                     }
                 }
-        capture_angles(S, ex, it, ex->src_angle);
+        capture_angles(S, ex, it, ex->src_angle, ex->src_energy);
     }
     if (mode == ORC_MODE_RECEIVER && ex) {
         /* imaging_inner_product_ex / imaging_correlation_ex, restating
@@ -569,7 +573,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                     real et = ex->etp[m];
                     if (ptp && et != 0) ptp[m] = (float)(S->f[F_TP][c] / et);
                 }
-        capture_angles(S, ex, it, ex->rcv_angle);
+        capture_angles(S, ex, it, ex->rcv_angle, ex->rcv_energy);
     }
 }
 
@@ -609,7 +613,9 @@ int orc_run_pass(const orc_grid *g, const float *vp, const float *vs, const floa
     if (!S) return -2;
     long n = (long)g->nx * g->ny * g->nz;
     if (mode == ORC_MODE_SOURCE && ex && ex->src_angle) memset(ex->src_angle, 0, sizeof(float) * n);
+    if (mode == ORC_MODE_SOURCE && ex && ex->src_energy) memset(ex->src_energy, 0, sizeof(float) * n);
     if (mode == ORC_MODE_RECEIVER && ex->rcv_angle) memset(ex->rcv_angle, 0, sizeof(float) * n);
+    if (mode == ORC_MODE_RECEIVER && ex->rcv_energy) memset(ex->rcv_energy, 0, sizeof(float) * n);
     if (mode == ORC_MODE_SOURCE && ex) {
         memset(ex->amp2, 0, sizeof(float) * n);
         memset(ex->second2, 0, sizeof(float) * n);
@@ -650,6 +656,9 @@ void orc_state_step(void *st, const orc_shot *s, int mode, int it, int nsteps, f
 }
 
 void orc_state_destroy(void *st) { state_free((orc_state *)st); }
+
+/* All 13 fields of a stepping state, [13][nz][ny][nx] (field order of the enum). */
+void orc_state_fields(const void *st, float *out) { state_export((const orc_state *)st, out); }
 
 /* ----------------------------------------------------------------------
  * Divergence / curl decomposition (decom_new, elastic_2D_kernel_2.cu:671-791)

@@ -82,6 +82,10 @@ typedef struct {
      * excitation time, of the source wavefield (written by the source pass) and of
      * the receiver wavefield (written by the receiver pass); see orc_window_angle. */
     float *src_angle, *rcv_angle;
+    /* optional (NULL = off): the window's P energy sum (px^2 + pz^2) at each angle
+     * capture, to tell cells with a real wavefield from cells that only hold the
+     * stencil's numerical precursor (where the angle means nothing) */
+    float *src_energy, *rcv_energy;
 } orc_excitation;
 
 /* ---- model-independent helpers --------------------------------------- */

@@ -46,7 +46,8 @@ class Excitation(C.Structure):
                 ("time", C.POINTER(C.c_int)), ("evx", C.POINTER(C.c_float)),
                 ("evy", C.POINTER(C.c_float)), ("evz", C.POINTER(C.c_float)),
                 ("etp", C.POINTER(C.c_float)), ("src_angle", C.POINTER(C.c_float)),
-                ("rcv_angle", C.POINTER(C.c_float))]
+                ("rcv_angle", C.POINTER(C.c_float)), ("src_energy", C.POINTER(C.c_float)),
+                ("rcv_energy", C.POINTER(C.c_float))]
 
 
 _libs: dict[int, C.CDLL] = {}
@@ -84,6 +85,7 @@ def lib(bits: int = 64) -> C.CDLL:
         L.orc_state_step.argtypes = [C.c_void_p, P(Shot), C.c_int, C.c_int, C.c_int, f,
                                      P(Excitation), f, f, f]
         L.orc_state_destroy.argtypes = [C.c_void_p]
+        L.orc_state_fields.argtypes = [C.c_void_p, f]
         L.orc_born_forward.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f, f, f, f]
         L.orc_born_forward.restype = C.c_int
         L.orc_born_adjoint.argtypes = [P(Grid), f, f, f, P(Shot), C.c_int, f, f, f, f]
@@ -191,6 +193,8 @@ class ExcitationArrays:
     def __init__(self, shape, angles: bool = False):
         self.src_angle = np.zeros(shape, np.float32) if angles else None
         self.rcv_angle = np.zeros(shape, np.float32) if angles else None
+        self.src_energy = np.zeros(shape, np.float32) if angles else None
+        self.rcv_energy = np.zeros(shape, np.float32) if angles else None
         self.amp2 = np.zeros(shape, np.float32)
         self.second2 = np.zeros(shape, np.float32)
         self.time = np.zeros(shape, np.int32)
@@ -205,6 +209,7 @@ class ExcitationArrays:
         e.time = self.time.ctypes.data_as(C.POINTER(C.c_int))
         e.evx, e.evy, e.evz, e.etp = _fp(self.evx), _fp(self.evy), _fp(self.evz), _fp(self.etp)
         e.src_angle, e.rcv_angle = _fp(self.src_angle), _fp(self.rcv_angle)
+        e.src_energy, e.rcv_energy = _fp(self.src_energy), _fp(self.rcv_energy)
         return e
 
 

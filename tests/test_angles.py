@@ -170,20 +170,19 @@ def test_source_angles_match_the_oracle(ertm, orc):
 
 
 @pytest.mark.gpu
-@pytest.mark.xfail(strict=False, reason="receiver angles: median GPU-oracle difference 3e-5 degrees, but "
-                   "1 % of clearly excited cells differed by up to 28 degrees in the one B200 run; "
-                   "cause not yet found")
 def test_receiver_angles_match_the_oracle(ertm, orc):
+    """Receiver angles are compared where the receiver window holds a wavefield: at
+    about 40 % of the clearly excited cells of this case the back-propagated field
+    has not arrived at the excitation step and the window holds only the stencil's
+    numerical precursor (P energy 1e-70 of the maximum and below), where the angle
+    of float data means nothing (the reference computes it from float Poynting
+    arrays too)."""
     ctx, c, ex, r, _, ra, clear = _gpu_and_oracle_angles(ertm, orc)
-    pml = c["pml"]
-    nz, _, nx = c["shape"]
-    interior = np.zeros(c["shape"], bool)
-    interior[pml[4]:nz - pml[5], :, pml[0]:nx - pml[1]] = True
-    pp = np.abs(r["pp"])
-    m = clear & interior & (pp > 1e-2 * np.percentile(pp[clear], 99))
-    d = np.abs(ra - ex.rcv_angle)
-    assert np.median(d[clear]) < 0.05
-    assert np.percentile(d[m], 99) < ANGLE_TOL_DEG, np.percentile(d[m], 99)
+    e = ex.rcv_energy
+    live = clear & (e > 1e-12 * e[clear].max())
+    assert live.sum() > 0.3 * clear.sum()
+    d = np.abs(ra - ex.rcv_angle)[live]
+    assert np.percentile(d, 99) < ANGLE_TOL_DEG and np.median(d) < 0.05, (np.percentile(d, 99), np.median(d))
 
 
 @pytest.mark.gpu
