@@ -61,6 +61,39 @@ int main()
         arr("pad3d_z_major", v, (long)nxb * nyb * nzb);
         free1float(v);
     }
+    // cpu_laplace (zzzzz:1110-1147) on an image of nx = 12, nz = 9 (nx >= nz keeps the
+    // reference's row-copy loop inside the array), no boundary offsets; layout ix*nz+iz
+    {
+        int nx = 12, nz = 9;
+        float *img = alloc1float((size_t)nx * nz), *vel = alloc1float((size_t)nx * nz);
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                img[ix * nz + iz] = (float)(sin(0.7 * ix + 0.3) * cos(0.45 * iz - 0.2) + 0.05 * ((ix * 7 + iz * 3) % 5));
+                vel[ix * nz + iz] = 2000.f + 25.f * iz + 10.f * ix;
+            }
+        arr("laplace_in_ix_major", img, (long)nx * nz);
+        arr("laplace_vel_ix_major", vel, (long)nx * nz);
+        cpu_laplace(img, vel, nx, nz, nx, nz, 0, 0, 5.f, 4.f);
+        arr("laplace_out_ix_major", img, (long)nx * nz);
+        free1float(img);
+        free1float(vel);
+    }
+    // suhilbt (zzzzz:1018-1066) along z, nx = 5 columns, nz = 16 and nz = 15; layout ix*nz+iz
+    for (int nz = 15; nz <= 16; nz++) {
+        int nx = 5;
+        float *img = alloc1float((size_t)nx * nz), *out = alloc1float((size_t)nx * nz);
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz; iz++)
+                img[ix * nz + iz] = (float)(cos(2 * PI * (ix + 1) * iz / nz + 0.1 * ix) + 0.3 * sin(0.9 * iz * iz / nz) - 0.1 * ix);
+        suhilbt(img, out, nx, nz, nx, nz, 0, 0, 5.f, 5.f);
+        char nm[64];
+        snprintf(nm, sizeof nm, "hilbert_in_nz%d_ix_major", nz);
+        arr(nm, img, (long)nx * nz);
+        snprintf(nm, sizeof nm, "hilbert_out_nz%d_ix_major", nz);
+        arr(nm, out, (long)nx * nz);
+        free1float(img);
+        free1float(out);
+    }
     // vp_set_vs / vp_set_density (zzzzz:1261-1287)
     {
         float vp[4] = {1800.f, 2500.f, 3200.f, 4500.f}, vs[4], rho[4];

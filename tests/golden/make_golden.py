@@ -25,7 +25,8 @@ out = subprocess.run([os.path.join(REPO, "oracle", "_ref", "ref_helpers")], chec
 data = json.loads(out)
 data["_about"] = ("Outputs of the reference's own CPU helpers (make_ricker_new, "
                   "make_coe_optimized_new, make_attenuation_new, coe_attenuation_3d_new2, "
-                  "add_pml_layers_v_h, vp_set_vs, vp_set_density) on the fixed inputs in "
+                  "add_pml_layers_v_h, vp_set_vs, vp_set_density, cpu_laplace, suhilbt) on the "
+                  "fixed inputs in "
                   "oracle/ref_helpers/ref_helpers.cpp; generated by tests/golden/make_golden.py")
 with open(os.path.join(HERE, "ref_helpers.json"), "w") as f:
     json.dump(data, f, indent=0)

@@ -140,3 +140,47 @@ def test_post_filters_on_the_device_match_the_host(ertm):
     host = ertm.taper_x(g.copy(), 20, 13, 3)
     dev = ertm.taper_x(d.clone(), 20, 13, 3).cpu().numpy()
     assert np.allclose(dev, host, rtol=1e-6, atol=1e-7)
+
+
+def _gold():
+    import json
+    import os
+    return json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_helpers.json")))
+
+
+def _ix_major_to_vol(v, nx, nz):
+    return np.asarray(v, np.float32).reshape(nx, nz).T.copy()[:, None, :]
+
+
+def test_laplace_filter_matches_the_reference_cpu_laplace(ertm):
+    """Golden vectors from the reference's own cpu_laplace (12 x 9 image).  Every
+    cell agrees except the reference's row-copy quirk: it copies the top and bottom
+    rows only for columns 0..nz-1 and its corner copies read a raw -r value; those
+    cells hold -r v^2/4 (uncopied) or the corner value in the reference."""
+    G = _gold()
+    nx, nz = 12, 9
+    img = _ix_major_to_vol(G["laplace_in_ix_major"], nx, nz)
+    vel = _ix_major_to_vol(G["laplace_vel_ix_major"], nx, nz)
+    ref = _ix_major_to_vol(G["laplace_out_ix_major"], nx, nz)
+    out = ertm.laplace_filter(img, vel, (5.0, 5.0, 4.0))
+    quirk = np.zeros((nz, 1, nx), bool)
+    quirk[[0, nz - 1], 0, 0] = True
+    quirk[[0, nz - 1], 0, nz:] = True
+    scale = np.abs(ref).max()
+    assert np.allclose(out[~quirk], ref[~quirk], rtol=1e-5, atol=1e-6 * scale)
+    # uncopied row cells keep -r v^2/4; the last column then copies its neighbour's -r
+    for k in (0, nz - 1):
+        assert np.allclose(ref[k, 0, nz:nx - 1], -img[k, 0, nz:nx - 1] * vel[k, 0, nz:nx - 1] ** 2 / 4, rtol=1e-6)
+        assert np.isclose(ref[k, 0, nx - 1], -img[k, 0, nx - 2] * vel[k, 0, nx - 1] ** 2 / 4, rtol=1e-6)
+
+
+@pytest.mark.parametrize("nz", [15, 16])
+def test_hilbert_matches_the_reference_suhilbt(ertm, nz):
+    """Golden vectors from the reference's own suhilbt (5 columns); the reference
+    accumulates its spectrum in float, this library in double."""
+    G = _gold()
+    nx = 5
+    img = _ix_major_to_vol(G[f"hilbert_in_nz{nz}_ix_major"], nx, nz)
+    ref = _ix_major_to_vol(G[f"hilbert_out_nz{nz}_ix_major"], nx, nz)
+    out = ertm.hilbert_z(img)
+    assert np.allclose(out, ref, rtol=0, atol=2e-5 * np.abs(ref).max())
