@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "ertm.h"
@@ -147,6 +148,34 @@ __global__ void k_adcig(const float* img, const float* ang, const float* normal,
     }
 }
 
+// Hilbert transform of columns [c0, c1) (one host thread's share of ertm_hilbert_z)
+void hilbert_columns(const float* img, float* out, int nz, long long sz, long long c0, long long c1,
+                     const double* cs, const double* sn)
+{
+    std::vector<double> col((size_t)nz), re((size_t)nz), im((size_t)nz);
+    for (long long c = c0; c < c1; c++) {
+        for (int t = 0; t < nz; t++) col[t] = img[t * sz + c];
+        for (int w = 0; w < nz; w++) {
+            double r = 0.0, i = 0.0;
+            for (int t = 0; t < nz; t++) {
+                const int q = (int)(((long long)w * t) % nz);
+                r += col[t] * cs[q];
+                i -= col[t] * sn[q];
+            }
+            if (w < nz / 2) { re[w] = i; im[w] = -r; }      // * (-i)
+            else { re[w] = -i; im[w] = r; }                  // * (+i)
+        }
+        for (int t = 0; t < nz; t++) {
+            double v = 0.0;
+            for (int w = 0; w < nz; w++) {
+                const int q = (int)(((long long)w * t) % nz);
+                v += re[w] * cs[q] - im[w] * sn[q];
+            }
+            out[t * sz + c] = (float)(v / nz);
+        }
+    }
+}
+
 int grid_for(long long n)
 {
     const long long b = (n + 255) / 256;
@@ -210,40 +239,31 @@ int ertm_laplace_filter(float* img, const float* vp, int nx, int ny, int nz, flo
 
 // Hilbert transform along depth of every (y, x) column (suhilbt, zzzzz:1018-1066):
 // X = DFT(x) (forward e^{-i w t}), multiplied by -i for w < n/2 and by +i from n/2 on,
-// y = Re(IDFT(X)) / n — the reference's direct O(n^2) transforms, in double.
+// y = Re(IDFT(X)) / n — the reference's direct O(n^2) transforms, in double.  The
+// columns are split over the host's hardware threads.
 int ertm_hilbert_z(const float* img, float* out, int nx, int ny, int nz)
 {
     if (!img || !out || nx < 1 || ny < 1 || nz < 1) return ERTM_EINVAL;
     const double pi = 3.14159265358979323846;
-    std::vector<double> cs((size_t)nz), sn((size_t)nz), col((size_t)nz), re((size_t)nz), im((size_t)nz);
+    std::vector<double> cs((size_t)nz), sn((size_t)nz);
     for (int q = 0; q < nz; q++) {
         cs[q] = std::cos(2.0 * pi * q / nz);
         sn[q] = std::sin(2.0 * pi * q / nz);
     }
     const long long sz = (long long)nx * ny;
-    for (long long c = 0; c < sz; c++) {
-        for (int t = 0; t < nz; t++) col[t] = img[t * sz + c];
-        for (int w = 0; w < nz; w++) {
-            double r = 0.0, i = 0.0;
-            for (int t = 0; t < nz; t++) {
-                const int q = (int)(((long long)w * t) % nz);
-                r += col[t] * cs[q];
-                i -= col[t] * sn[q];
-            }
-            if (w < nz / 2) { re[w] = i; im[w] = -r; }      // * (-i)
-            else { re[w] = -i; im[w] = r; }                  // * (+i)
-        }
-        for (int t = 0; t < nz; t++) {
-            double v = 0.0;
-            for (int w = 0; w < nz; w++) {
-                const int q = (int)(((long long)w * t) % nz);
-                v += re[w] * cs[q] - im[w] * sn[q];
-            }
-            out[t * sz + c] = (float)(v / nz);
-        }
-    }
+    const long long work = sz * (long long)nz * nz;
+    unsigned nth = std::thread::hardware_concurrency();
+    if (nth == 0) nth = 1;
+    if (work < (1LL << 22)) nth = 1;
+    if ((long long)nth > sz) nth = (unsigned)sz;
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nth; t++)
+        pool.emplace_back(hilbert_columns, img, out, nz, sz, sz * t / nth, sz * (t + 1) / nth, cs.data(),
+                          sn.data());
+    for (auto& th : pool) th.join();
     return ERTM_OK;
 }
+
 
 
 // Truncated Gaussian smoothing (cuda_bell_smoothz_new / cuda_bell_smoothx_new,
