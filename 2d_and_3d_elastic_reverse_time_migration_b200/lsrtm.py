@@ -11,9 +11,19 @@ restate.
 used as in preconditioned CGLS, and a preconditioned step is accepted only if
 the Born-modelled data misfit falls, otherwise the plain CG step of the same
 iteration is taken instead (plain CG is the fallback).
+
+`state` (optional) is a path prefix for the iteration state (model, residual,
+gradient, direction, scalars and history), written after every iteration —
+one file per rank, replaced atomically — and read back at the start, so an
+interrupted run continues from its last finished iteration with the same
+numbers as an uninterrupted one.  `log` (optional) is a JSON-lines file that
+gets one record per iteration (misfit, step kind, seconds).
 """
 from __future__ import annotations
 
+import json
+import os
+import time
 from dataclasses import dataclass, field
 from typing import Callable, Sequence
 
@@ -79,24 +89,69 @@ def adjoint_all(ctx, shots, res):
     return tuple(x.astype(np.float32) for x in g)
 
 
+def _state_file(prefix: str, group) -> str:
+    import torch.distributed as dist
+    rank = dist.get_rank(group) if dist.is_available() and dist.is_initialized() else 0
+    return f"{prefix}.rank{rank}.npz"
+
+
+def _save_state(path: str, it: int, m, r, s, p, gamma, rnorm, dnorm, out: "CGResult"):
+    tmp = path + ".tmp.npz"
+    arrs = {"it": np.int64(it), "gamma": np.float64(gamma), "rnorm": np.float64(rnorm),
+            "dnorm": np.float64(dnorm), "misfit": np.asarray(out.misfit, np.float64),
+            "accepted": np.asarray(out.accepted, dtype="U8"), "nres": np.int64(len(r))}
+    for q in range(3):
+        arrs[f"m{q}"], arrs[f"s{q}"], arrs[f"p{q}"] = m[q], s[q], p[q]
+    for k, x in enumerate(r):
+        arrs[f"r{k}"] = x
+    np.savez(tmp, **arrs)
+    os.replace(tmp, path)
+
+
+def _load_state(path: str):
+    with np.load(path) as f:
+        st = {k: f[k] for k in f.files}
+    vol = lambda key: tuple(st[f"{key}{q}"].astype(np.float32) for q in range(3))
+    return (int(st["it"]), vol("m"), [st[f"r{k}"].astype(np.float32) for k in range(int(st["nres"]))],
+            vol("s"), vol("p"), float(st["gamma"]), float(st["rnorm"]), float(st["dnorm"]),
+            [float(x) for x in st["misfit"]], [str(x) for x in st["accepted"]])
+
+
 def cgls(ctx, shots: list, data: list, niter: int,
          precond: Callable[[tuple], tuple] | None = None,
-         callback: Callable[[int, float], None] | None = None, group=None) -> CGResult:
+         callback: Callable[[int, float], None] | None = None, group=None,
+         state: str | None = None, log: str | None = None) -> CGResult:
     """CGLS on this rank's shots; with torch.distributed initialised, the ranks of
     `group` each pass their own shots and data, and the gradient (one all-reduce of
-    three volumes per iteration) and the norms are summed over them."""
+    three volumes per iteration) and the norms are summed over them.  `state` and
+    `log`: see the module docstring."""
     red = _Sum(group)
     shape = ctx.cfg.shape
-    m = tuple(np.zeros(shape, np.float32) for _ in range(3))
-    r = [d.astype(np.float32).copy() for d in data]            # r = d - F m
-    dnorm = red.scalar(sum(float(np.sum(d.astype(np.float64) ** 2)) for d in data))
-    s = red.volumes(adjoint_all(ctx, shots, r))
-    z = precond(s) if precond else s
-    p = z
-    gamma = _dot(s, z)
-    out = CGResult(m=m)
-    rnorm = dnorm
-    for it in range(niter):
+    out = CGResult(m=None)
+    path = _state_file(state, group) if state else None
+    start = 0
+    have = path is not None and os.path.exists(path)
+    # every rank resumes, or none does (the ranks must take the same steps)
+    if state and red.on and red.scalar(1.0 if have else 0.0) not in (0.0, float(_world(group))):
+        raise RuntimeError(f"CG state {state!r}: some ranks have a state file and some do not")
+    if have:
+        start, m, r, s, p, gamma, rnorm, dnorm, out.misfit, out.accepted = _load_state(path)
+        if len(r) != len(data):
+            raise RuntimeError(f"CG state {path!r} holds {len(r)} residuals for {len(data)} shots")
+        if red.on and red.scalar(float(start)) != float(start) * _world(group):
+            raise RuntimeError(f"CG state {state!r}: ranks stopped at different iterations")
+    else:
+        m = tuple(np.zeros(shape, np.float32) for _ in range(3))
+        r = [d.astype(np.float32).copy() for d in data]            # r = d - F m
+        dnorm = red.scalar(sum(float(np.sum(d.astype(np.float64) ** 2)) for d in data))
+        s = red.volumes(adjoint_all(ctx, shots, r))
+        z = precond(s) if precond else s
+        p = z
+        gamma = _dot(s, z)
+        rnorm = dnorm
+    out.m = m
+    for it in range(start, niter):
+        t0 = time.perf_counter()
         q = born_all(ctx, shots, p)
         qq = red.scalar(sum(float(np.sum(x.astype(np.float64) ** 2)) for x in q))
         if qq == 0.0 or gamma == 0.0:
@@ -126,7 +181,18 @@ def cgls(ctx, shots: list, data: list, niter: int,
         gamma = gamma_new
         out.misfit.append(rnorm / dnorm)
         out.accepted.append(kind)
+        if path:
+            _save_state(path, it + 1, m, r, s, p, gamma, rnorm, dnorm, out)
+        if log:
+            with open(log, "a") as f:
+                f.write(json.dumps({"event": "cg_iteration", "iteration": it, "misfit": rnorm / dnorm,
+                                    "step": kind, "seconds": round(time.perf_counter() - t0, 6)}) + "\n")
         if callback:
             callback(it, rnorm / dnorm)
     out.m = m
     return out
+
+
+def _world(group) -> int:
+    import torch.distributed as dist
+    return dist.get_world_size(group)
