@@ -10,11 +10,18 @@ A single grid is never split across GPUs.
 Before the image collective every rank contributes a status word, so a rank
 whose shots failed makes every rank raise `ShotFailure` (naming the failed
 ranks) instead of leaving the others blocked in the reduction.
+
+`migrate_shots` runs shot by shot: with a `ShotCache` every finished shot's
+images go to their own file (the reference's restart unit is also the per-shot
+image file), so a run that stopped resumes at the shots that have no file yet;
+with `skip_failed` a shot that raises is left out of the stack and reported
+(shot index and message, gathered from every rank) instead of failing the run.
 """
 from __future__ import annotations
 
 import heapq
-from dataclasses import dataclass
+import os
+from dataclasses import dataclass, field
 from typing import Callable, Sequence
 
 
@@ -53,6 +60,7 @@ class StackResult:
     ps: object
     tp: object
     my_shots: list
+    failed: list = field(default_factory=list)   # (shot, message), every rank's (migrate_shots)
 
 
 def migrate(local: Callable[[list[int]], tuple], nshots: int, costs: Sequence[float] | None = None,
@@ -107,6 +115,90 @@ def context_local(ctx, shots: list, data: list) -> Callable[[list[int]], tuple]:
         outs = [torch.zeros(ctx.cfg.shape, dtype=torch.float32, device=dev) for _ in range(3)]
         if idx:
             ctx.rtm_batch([shots[i] for i in idx], [data[i] for i in idx], *outs)
+        return tuple(outs)
+
+    return run
+
+
+class ShotCache:
+    """Per-shot images (pp, ps, tp) on disk, one `.npz` file per shot, written to a
+    temporary name and renamed, so a file that exists is complete."""
+
+    def __init__(self, directory: str):
+        self.dir = directory
+        os.makedirs(directory, exist_ok=True)
+
+    def path(self, shot: int) -> str:
+        return os.path.join(self.dir, f"shot{shot:06d}.npz")
+
+    def has(self, shot: int) -> bool:
+        return os.path.exists(self.path(shot))
+
+    def load(self, shot: int):
+        import numpy as np
+        with np.load(self.path(shot)) as f:
+            return f["pp"], f["ps"], f["tp"]
+
+    def save(self, shot: int, imgs) -> None:
+        import numpy as np
+        host = [x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x) for x in imgs]
+        tmp = self.path(shot) + ".tmp.npz"
+        np.savez(tmp, pp=host[0], ps=host[1], tp=host[2])
+        os.replace(tmp, self.path(shot))
+
+
+def migrate_shots(one_shot: Callable[[int], tuple], nshots: int, shape, costs: Sequence[float] | None = None,
+                  group=None, dst: int | None = None, cache: ShotCache | None = None,
+                  skip_failed: bool = False, device=None) -> StackResult:
+    """`migrate` shot by shot: `one_shot(i)` returns shot i's (pp, ps, tp) tensors of
+    `shape`; cached shots are loaded instead of migrated and new ones are saved;
+    with `skip_failed` a shot that raises is reported in `StackResult.failed` (on
+    every rank) and left out of the stack, otherwise the run fails as in `migrate`."""
+    import torch
+    import torch.distributed as dist
+
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() \
+            else torch.device("cpu")
+    failed_here: list = []
+
+    def local(idx):
+        acc = [torch.zeros(tuple(shape), dtype=torch.float32, device=device) for _ in range(3)]
+        for i in idx:
+            if cache is not None and cache.has(i):
+                imgs = [torch.from_numpy(x).to(device) for x in cache.load(i)]
+            else:
+                try:
+                    imgs = one_shot(i)
+                except Exception as e:
+                    if not skip_failed:
+                        raise
+                    failed_here.append((i, f"{type(e).__name__}: {e}"))
+                    continue
+                if cache is not None:
+                    cache.save(i, imgs)
+            for a, x in zip(acc, imgs):
+                a += torch.as_tensor(x, device=device).reshape(a.shape)
+        return tuple(acc)
+
+    res = migrate(local, nshots, costs, group=group, dst=dst)
+    failed = list(failed_here)
+    if dist.is_initialized() and dist.get_world_size(group) > 1:
+        lists = [None] * dist.get_world_size(group)
+        dist.all_gather_object(lists, failed_here, group=group)
+        failed = [tuple(f) for lst in lists for f in lst]
+    res.failed = sorted(failed)
+    return res
+
+
+def context_shot(ctx, shots: list, data: list) -> Callable[[int], tuple]:
+    """`one_shot` callable for `migrate_shots` over a Context (images on its GPU)."""
+    import torch
+
+    def run(i: int):
+        dev = torch.device("cuda", ctx.cfg.device)
+        outs = [torch.zeros(ctx.cfg.shape, dtype=torch.float32, device=dev) for _ in range(3)]
+        ctx.rtm_shot(shots[i], data[i], *outs)
         return tuple(outs)
 
     return run
