@@ -9,6 +9,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -685,12 +686,21 @@ int upload_wavelet(ertm_ctx* c, const ertm_shot* s)
     return ERTM_OK;
 }
 
+// NVTX range for profilers (no-op unless a tool is attached): one per pass and per
+// Born operator call, so timelines show shots, passes and CG operator calls.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
+
 // One pass of `nsteps` steps.  MODE_MODEL records into `traces` ([3][nt][nrec],
 // device), MODE_RECEIVER injects from it.
 int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, float* traces)
 {
     if (!c->model_set[which])
         return fail(c, ERTM_ESTATE, "%s model not set", which ? "migration" : "true");
+    Range range(mode == MODE_SOURCE ? "ertm source pass" : mode == MODE_RECEIVER ? "ertm receiver pass"
+                                                                               : "ertm modelling pass");
     int rc;
     float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[which];
     if ((rc = upload_profiles(c, vmax))) return rc;
@@ -1519,6 +1529,7 @@ int ertm_born_forward(ertm_ctx* c, const ertm_shot* s, const float* r_vp, const 
                       const float* r_rho, float* data_out)
 {
     if (!c) return ERTM_EINVAL;
+    Range range("ertm born forward");
     if (!r_vp || !r_vs || !r_rho || !data_out) return fail(c, ERTM_EINVAL, "NULL argument");
     CK(c, cudaSetDevice(c->device));
     int rc = born_check(c, s);
@@ -1550,6 +1561,7 @@ int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, fl
                       float* g_vs, float* g_rho)
 {
     if (!c) return ERTM_EINVAL;
+    Range range("ertm born adjoint");
     if (!residual || !g_vp || !g_vs || !g_rho) return fail(c, ERTM_EINVAL, "NULL argument");
     CK(c, cudaSetDevice(c->device));
     int rc = born_check(c, s);
