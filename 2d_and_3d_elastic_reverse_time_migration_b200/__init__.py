@@ -263,8 +263,48 @@ def _ptr(a, n: int | None = None, writable: bool = False):
     return a.ctypes.data
 
 
+def _pass_steps(cfg, name: str) -> int:
+    """Time steps a pass call runs (for the run log's cell-update rates)."""
+    src = cfg.src_steps or (2 * cfg.nt) // 3
+    return {"forward_together_using_real_model": cfg.nt, "forward_together_using_smoothed_model": src,
+            "backward_together_using_smoothed_model": cfg.nt, "rtm_shot": src + cfg.nt,
+            "born_forward": 2 * cfg.nt, "born_adjoint": 3 * cfg.nt}.get(name, 0)
+
+
+def _logged(fn):
+    """Appends one JSON line per call to the context's run log (`Context.set_log`):
+    the call, its wall time (the calls are synchronous), and cell-updates per
+    second over the passes it runs (Born calls count background and scattered
+    wavefields, and the adjoint its background rebuild)."""
+    import functools
+    import json
+    import time
+
+    @functools.wraps(fn)
+    def wrap(self, *a, **k):
+        if not getattr(self, "_log", None):
+            return fn(self, *a, **k)
+        t0 = time.perf_counter()
+        out = fn(self, *a, **k)
+        dt = time.perf_counter() - t0
+        steps = _pass_steps(self.cfg, fn.__name__)
+        rec = {"event": "pass", "call": fn.__name__, "cells": self.ncell, "cell_steps": self.ncell * steps,
+               "seconds": round(dt, 6), "gcell_s": round(self.ncell * steps / dt / 1e9, 4) if dt > 0 else None}
+        with open(self._log, "a") as f:
+            f.write(json.dumps(rec) + "\n")
+        return out
+
+    return wrap
+
+
 class Context:
     """One GPU context: device state of one grid (the reference's GPUdevice)."""
+
+    _log = None
+
+    def set_log(self, path: str | None):
+        """Append a JSON line per pass call to `path` (None stops logging)."""
+        self._log = path
 
     def __init__(self, cfg: Config):
         self.cfg = cfg
@@ -324,6 +364,7 @@ class Context:
         args = [a if _is_torch(a) else np.ascontiguousarray(a, np.float32) for a in args]
         self._ck(self._L.ertm_set_model(self._h, which, *[_ptr(a, n) for a in args]))
 
+    @_logged
     def forward_together_using_real_model(self, shot: Shot, out=None):
         n = 3 * self.cfg.nt * shot.nrec
         if out is None:
@@ -333,10 +374,12 @@ class Context:
                                                                 _ptr(out, n, True)))
         return out
 
+    @_logged
     def forward_together_using_smoothed_model(self, shot: Shot):
         s = shot.struct()
         self._ck(self._L.ertm_forward_together_using_smoothed_model(self._h, C.byref(s)))
 
+    @_logged
     def backward_together_using_smoothed_model(self, shot: Shot, data, pp=None, ps=None, tp=None):
         n = self.ncell
         pp, ps, tp = self._vol(pp), self._vol(ps), self._vol(tp)
@@ -347,6 +390,7 @@ class Context:
             _ptr(ps, n, True), _ptr(tp, n, True)))
         return pp, ps, tp
 
+    @_logged
     def rtm_shot(self, shot: Shot, data, pp=None, ps=None, tp=None):
         n = self.ncell
         pp, ps, tp = self._vol(pp), self._vol(ps), self._vol(tp)
@@ -418,6 +462,7 @@ class Context:
         self._ck(self._L.ertm_time_kernels(self._h, C.byref(s), nsteps, ms))
         return float(ms[0]), float(ms[1])
 
+    @_logged
     def born_forward(self, shot: Shot, r_vp, r_vs, r_rho, out=None):
         """Linearised data (3, nt, nrec) for relative perturbations of the migration model."""
         n = self.ncell
@@ -429,6 +474,7 @@ class Context:
                                            _ptr(out, 3 * self.cfg.nt * shot.nrec, True)))
         return out
 
+    @_logged
     def born_adjoint(self, shot: Shot, residual, g_vp=None, g_vs=None, g_rho=None):
         """Transpose of born_forward applied to residual (3, nt, nrec): (g_vp, g_vs, g_rho)."""
         n = self.ncell

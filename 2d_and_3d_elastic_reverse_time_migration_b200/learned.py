@@ -13,6 +13,7 @@ Born-modelled data misfit falls).
 """
 from __future__ import annotations
 
+import json
 import time
 from dataclasses import dataclass, field
 
@@ -100,15 +101,16 @@ class TrainLog:
 
 
 def train(net, pairs, steps: int, batch: int, patch=(64, 128), lr: float = 1e-3, seed: int = 0,
-          log_every: int = 50) -> TrainLog:
-    """Adam on random patches of the (input, target) image pairs (each (H, W, 3))."""
+          log_every: int = 50, log: str | None = None) -> TrainLog:
+    """Adam on random patches of the (input, target) image pairs (each (H, W, 3));
+    `log` (optional) is a JSON-lines file that gets the loss every `log_every` steps."""
     import torch
     rng = np.random.default_rng(seed)
     dev = net.dev
     X = [torch.from_numpy(x).to(dev) for x, _ in pairs]
     Y = [torch.from_numpy(y).to(dev) for _, y in pairs]
     ph, pw = patch
-    log = TrainLog()
+    tl = TrainLog()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     xb = torch.zeros((batch, ph, pw, 3), device=dev)
@@ -126,11 +128,14 @@ def train(net, pairs, steps: int, batch: int, patch=(64, 128), lr: float = 1e-3,
             yb[b, :hh, :ww] = Y[k][i0:i0 + hh, j0:j0 + ww]
         loss = net.step(xb, yb, lr=lr)
         if it % log_every == 0 or it == steps - 1:
-            log.loss.append((it, float(loss.item())))
+            tl.loss.append((it, float(loss.item())))
+            if log:
+                with open(log, "a") as f:
+                    f.write(json.dumps({"event": "unet_step", "step": it, "loss": tl.loss[-1][1]}) + "\n")
     torch.cuda.synchronize(dev)
-    log.seconds = time.perf_counter() - t0
-    log.steps = steps
-    return log
+    tl.seconds = time.perf_counter() - t0
+    tl.steps = steps
+    return tl
 
 
 def preconditioner(net, shape):

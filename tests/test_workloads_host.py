@@ -46,3 +46,30 @@ def test_image_packing_round_trip():
     assert all(np.array_equal(a, b) for a, b in zip(back, m))
     assert L.iters_to([0.5, 0.2, 0.009, 0.001], 1e-2) == 3
     assert L.iters_to([0.5, 0.2], 1e-2) is None
+
+
+def test_run_log_records_pass_calls(tmp_path):
+    """The per-call JSON-lines log of Context (driven here by a stand-in object, no GPU)."""
+    import json
+    ertm = importlib.import_module(PKG)
+
+    class Fake:
+        cfg = ertm.Config(nx=10, ny=1, nz=8, dx=5.0, dy=5.0, dz=5.0, dt_ms=0.5, nt=30, src_steps=20)
+        ncell = 80
+
+        @ertm._logged
+        def rtm_shot(self, x):
+            return x * 2
+
+        @ertm._logged
+        def born_adjoint(self):
+            return None
+
+    f = Fake()
+    assert f.rtm_shot(3) == 6                  # no log set: plain call
+    f._log = str(tmp_path / "run.jsonl")
+    f.rtm_shot(4)
+    f.born_adjoint()
+    recs = [json.loads(x) for x in open(f._log)]
+    assert [r["call"] for r in recs] == ["rtm_shot", "born_adjoint"]
+    assert recs[0]["cell_steps"] == 80 * (20 + 30) and recs[1]["cell_steps"] == 80 * 90
