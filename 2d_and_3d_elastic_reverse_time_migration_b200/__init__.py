@@ -110,6 +110,8 @@ SIGNATURES = {
     "ertm_hilbert_z": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int]),
     "ertm_bell_smooth": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P]),
     "ertm_taper_x": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P]),
+    "ertm_aperture_taper": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      _P]),
     "ertm_mute_direct": (C.c_int, [C.POINTER(_Shot), _P, C.c_int, C.c_float, C.c_float, C.c_float,
                                    C.c_float, C.c_float, C.c_int, _P]),
     "ertm_nn_gemm": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
@@ -676,6 +678,15 @@ def taper_x(img, left: int, right: int, power: int = 3, stream_ptr=None):
     rc = lib().ertm_taper_x(_arr_ptr(img, nx * ny * nz), nx, ny, nz, left, right, power, stream_ptr)
     if rc != 0:
         raise ErtmError(rc, "taper_x")
+    return img
+
+
+def aperture_taper(img, x0: int, x1: int, width: int, power: int = 2, stream_ptr=None):
+    """Aperture mute in x, in place (see ertm_aperture_taper); -1 leaves a side open."""
+    nz, ny, nx = img.shape
+    rc = lib().ertm_aperture_taper(_arr_ptr(img, nx * ny * nz), nx, ny, nz, x0, x1, width, power, stream_ptr)
+    if rc != 0:
+        raise ErtmError(rc, "aperture_taper")
     return img
 
 

@@ -84,6 +84,31 @@ __host__ __device__ inline float taper_at(int ix, int nx, int left, int right, i
     return (float)f;
 }
 
+// Aperture factor of column ix: 0 outside [x0, x1) (a side whose edge is negative is
+// open), cos(pi/2 m / w)^power on the w columns inside each closed edge (m counts
+// from the inner end of the ramp), 1 elsewhere.
+__host__ __device__ inline float aperture_at(int ix, int x0, int x1, int w, int power)
+{
+    const double hp = 1.57079632679489661923;
+    double f = 1.0;
+    if (x0 >= 0) {
+        if (ix < x0) return 0.f;
+        if (ix < x0 + w) f *= pow(cos(hp * (x0 + w - ix) / w), power);
+    }
+    if (x1 >= 0) {
+        if (ix >= x1) return 0.f;
+        if (ix >= x1 - w) f *= pow(cos(hp * (ix - (x1 - w)) / w), power);
+    }
+    return (float)f;
+}
+
+__global__ void k_aperture(float* img, long long n, int nx, int x0, int x1, int w, int power)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+        img[c] *= aperture_at((int)(c % nx), x0, x1, w, power);
+}
+
 __global__ void k_taper(float* img, long long n, int nx, int left, int right, int power)
 {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
@@ -327,6 +352,30 @@ int ertm_taper_x(float* img, int nx, int ny, int nz, int left, int right, int po
     }
     std::vector<float> f(nx);
     for (int i = 0; i < nx; i++) f[i] = taper_at(i, nx, left, right, power);
+    for (long long c = 0; c < n; c++) img[c] *= f[c % nx];
+    return ERTM_OK;
+}
+
+// Aperture mute of a gradient or image in x (cauda_zero_and_attenuation_truncation,
+// viscoelastic_equation.cu:2928-2988, and its _old form, :2990-3045): columns
+// outside [x0, x1) are zeroed and the w columns inside each edge ramp up with
+// cos^power.  The reference's call: x0 = offset_left - receiver_offset when
+// offset_left > receiver_offset (else open, -1), x1 = offset_left + receiver_offset
+// when offset_right > receiver_offset, w = max(3, receiver_offset / offset_attenuation)
+// and power 2 (the _old form: w = receiver_offset / 3, power 3).
+int ertm_aperture_taper(float* img, int nx, int ny, int nz, int x0, int x1, int w, int power, void* stream)
+{
+    if (!img || nx < 1 || ny < 1 || nz < 1 || w < 1 || power < 0 || x0 < -1 || x1 < -1 ||
+        (x0 >= 0 && x1 >= 0 && x1 < x0))
+        return ERTM_EINVAL;
+    const long long n = (long long)nx * ny * nz;
+    if (on_device(img)) {
+        k_aperture<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(img, n, nx, x0, x1, w, power);
+        if (cudaGetLastError() != cudaSuccess) return ERTM_ECUDA;
+        return cudaStreamSynchronize((cudaStream_t)stream) == cudaSuccess ? ERTM_OK : ERTM_ECUDA;
+    }
+    std::vector<float> f(nx);
+    for (int i = 0; i < nx; i++) f[i] = aperture_at(i, x0, x1, w, power);
     for (long long c = 0; c < n; c++) img[c] *= f[c % nx];
     return ERTM_OK;
 }

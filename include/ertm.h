@@ -304,6 +304,12 @@ int ertm_bell_smooth(const float *in, float *out, float *work, int nx, int ny, i
  * (viscoelastic_equation.cu:2881-2926; there left = offset_left/3, right =
  * offset_right/3, power 3), in place, host or device. */
 int ertm_taper_x(float *img, int nx, int ny, int nz, int left, int right, int power, void *stream);
+/* Aperture mute in x of cauda_zero_and_attenuation_truncation
+ * (viscoelastic_equation.cu:2928-3045): columns outside [x0, x1) become 0 (an edge
+ * of -1 leaves that side open) and the w columns inside each edge ramp with
+ * cos^power; in place, host or device. */
+int ertm_aperture_taper(float *img, int nx, int ny, int nz, int x0, int x1, int w, int power,
+                        void *stream);
 
 /* Propagation angles (2D grids).  With capture on, the source pass records at each
  * cell the P-wave propagation angle of the source wavefield at the cell's

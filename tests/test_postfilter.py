@@ -140,6 +140,9 @@ def test_post_filters_on_the_device_match_the_host(ertm):
     host = ertm.taper_x(g.copy(), 20, 13, 3)
     dev = ertm.taper_x(d.clone(), 20, 13, 3).cpu().numpy()
     assert np.allclose(dev, host, rtol=1e-6, atol=1e-7)
+    host = ertm.aperture_taper(g.copy(), 15, 70, 6, 2)
+    dev = ertm.aperture_taper(d.clone(), 15, 70, 6, 2).cpu().numpy()
+    assert np.allclose(dev, host, rtol=1e-6, atol=1e-7)
 
 
 def _gold():
@@ -184,3 +187,39 @@ def test_hilbert_matches_the_reference_suhilbt(ertm, nz):
     ref = _ix_major_to_vol(G[f"hilbert_out_nz{nz}_ix_major"], nx, nz)
     out = ertm.hilbert_z(img)
     assert np.allclose(out, ref, rtol=0, atol=2e-5 * np.abs(ref).max())
+
+
+def _aperture_ref(g, offset_left, offset_right, receiver_offset, offset_attenuation):
+    """cauda_zero_and_attenuation_truncation (viscoelastic_equation.cu:2928-2988) restated
+    column by column."""
+    g = g.astype(np.float64).copy()
+    nx = g.shape[-1]
+    for ix in range(nx):
+        col = g[..., ix]
+        if offset_left > receiver_offset:
+            if 0 <= ix < offset_left - receiver_offset:
+                col[...] = 0
+            dl = receiver_offset // offset_attenuation
+            dl = 3 if dl <= 2 else dl
+            if offset_left - receiver_offset <= ix < offset_left - receiver_offset + dl and offset_left != 0:
+                m = offset_left - receiver_offset + dl - ix
+                col *= np.cos(np.pi / 2 * m / dl) ** 2
+        if offset_right > receiver_offset:
+            if offset_left + receiver_offset <= ix < nx:
+                col[...] = 0
+            dr = receiver_offset // offset_attenuation
+            dr = 3 if dr <= 2 else dr
+            if offset_left + receiver_offset - dr <= ix < offset_left + receiver_offset and offset_right != 0:
+                m = ix - (offset_left + receiver_offset - dr)
+                col *= np.cos(np.pi / 2 * m / dr) ** 2
+    return g
+
+
+@pytest.mark.parametrize("ol,orr,ro,oa", [(60, 70, 25, 5), (20, 90, 25, 5), (60, 10, 25, 20), (60, 70, 8, 4)])
+def test_aperture_taper_matches_the_reference_kernel(ertm, ol, orr, ro, oa):
+    g = np.random.default_rng(15).standard_normal((6, 1, 130)).astype(np.float32)
+    w = max(3, ro // oa)
+    x0 = ol - ro if ol > ro else -1
+    x1 = ol + ro if orr > ro else -1
+    out = ertm.aperture_taper(g.copy(), x0, x1, w, 2)
+    assert np.allclose(out, _aperture_ref(g, ol, orr, ro, oa), rtol=1e-5, atol=1e-7)
