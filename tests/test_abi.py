@@ -69,3 +69,36 @@ def test_windows_are_validated_before_touching_a_device(ertm):
         with pytest.raises(ertm.ErtmError) as ei:
             ertm.rtm_windows(base, m, m, m, [win], [sh], [d], lanes=1)
         assert ei.value.code == -1 and str(ei.value)
+
+
+def test_header_is_c99_and_a_c_program_links_and_calls_the_library(tmp_path):
+    """The header compiles as strict C99, and a C program linked against libertm.so
+    calls host entry points through the C ABI (no Python, no GPU)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    lib = os.path.join(REPO, "2d_and_3d_elastic_reverse_time_migration_b200", "_lib")
+    src = tmp_path / "drv.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "ertm.h"
+int main(void)
+{
+    float img[5 * 4], vp[5 * 4], h[5 * 4];
+    for (int i = 0; i < 20; i++) { img[i] = (float)((i * 7) % 5) - 2.0f; vp[i] = 2000.0f; }
+    if (ertm_abi_version() != ERTM_ABI_VERSION) return 1;
+    if (ertm_hilbert_z(img, h, 5, 1, 4) != ERTM_OK) return 2;
+    if (ertm_laplace_filter(img, vp, 5, 1, 4, 5.0f, 5.0f, 5.0f) != ERTM_OK) return 3;
+    if (ertm_laplace_filter(img, vp, 2, 1, 4, 5.0f, 5.0f, 5.0f) != ERTM_EINVAL) return 4;
+    if (ertm_taper_x(img, 5, 1, 4, 2, 2, 3, NULL) != ERTM_OK) return 5;
+    printf("ok %g %g\n", img[7], h[3]);
+    return 0;
+}
+''')
+    exe = tmp_path / "drv"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(REPO, "include"),
+                    str(src), "-o", str(exe), "-L", lib, "-lertm", "-Wl,-rpath," + lib], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), (out.returncode, out.stdout, out.stderr)
