@@ -159,6 +159,15 @@ int orc_born_sources_given(long n, double dt_ms, const float *vp, const float *v
 int orc_image_given(long n, const float *ex, const float *ez, const float *rpx, const float *rpz,
                     const float *rsx, const float *rsz, float *pp, float *ps);
 
+/* Stepping state for callers that run a pass one step at a time (the CPU
+ * baseline's timed sample, the angle tests): create, step (same arguments as one
+ * iteration of orc_run_pass), read all 13 fields [13][nz][ny][nx], destroy. */
+void *orc_state_create(const orc_grid *g, const float *vp, const float *vs, const float *rho);
+void orc_state_step(void *st, const orc_shot *s, int mode, int it, int nsteps, float *data,
+                    orc_excitation *ex, float *pp, float *ps, float *ptp);
+void orc_state_fields(const void *st, float *out);
+void orc_state_destroy(void *st);
+
 /* Threads used by the OpenMP loops (1 if built without OpenMP). */
 int orc_threads(void);
 /* sizeof(REAL) of the loaded library (8 or 4). */
