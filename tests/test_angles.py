@@ -203,3 +203,39 @@ def test_angle_products_on_the_device_match_the_host(ertm):
     h = ertm.adcig_bin(img, sa, 20, 3.0, 48, zmin=5)
     d = ertm.adcig_bin(dev[0], dev[1], 20, 3.0, 48, zmin=5).cpu().numpy()
     assert np.array_equal(d, h)
+
+
+def test_oracle_receiver_angle_is_the_window_angle_at_the_excitation_step(orc):
+    """The receiver pass stepped one step at a time: at each step, the cells whose
+    excitation time it is get the window angle of the receiver wavefield of that
+    step, and the window energy the oracle reports."""
+    import ctypes as C
+    n, nt, nsrc = 60, 160, 110
+    g, (vp, vs, rho), shot = _homogeneous(orc, n, (30, 20))
+    rec = orc.make_shot(30, 0, 20, orc.ricker(20.0, 1e-3), rx0=20, nrx=20, drx=1, rz=24)
+    data = np.ascontiguousarray(orc.run_pass(g, vp, vs, rho, rec, orc.MODEL, nt)["data"])
+    ex = orc.ExcitationArrays((n, 1, n), angles=True)
+    orc.run_pass(g, vp, vs, rho, rec, orc.SOURCE, nsrc, ex=ex)
+    L = orc.lib()
+    st = L.orc_state_create(C.byref(g), orc._fp(vp), orc._fp(vs), orc._fp(rho))
+    F = np.zeros((13, n, 1, n), np.float32)
+    exs = ex.struct()
+    checked = 0
+    try:
+        for it in range(nt - 1, -1, -1):
+            L.orc_state_step(st, C.byref(rec), orc.RECEIVER, it, nt, orc._fp(data), C.byref(exs),
+                             None, None, None)
+            cells = np.argwhere(ex.time[:, 0] == it)
+            if len(cells) == 0 or it % 7:
+                continue
+            L.orc_state_fields(st, orc._fp(F))
+            f = {"tp": F[9], "vxp": F[10], "vzp": F[12]}
+            for k, i in cells[:: max(1, len(cells) // 5)]:
+                a = _window_angle(f, i, k)
+                if a is None:
+                    continue
+                assert abs(ex.rcv_angle[k, 0, i] - a) < 1e-4, (it, k, i)
+                checked += 1
+    finally:
+        L.orc_state_destroy(st)
+    assert checked > 20
