@@ -584,6 +584,56 @@ def read_volume_xyz(path: str, nx: int, ny: int, nz: int, into=None, offsets=(0,
     return out
 
 
+def _cut(cfg):
+    bl, _, bf, _, bu, _ = cfg.pml
+    nxi = cfg.nx - cfg.pml[0] - cfg.pml[1]
+    nyi = cfg.ny - cfg.pml[2] - cfg.pml[3]
+    nzi = cfg.nz - cfg.pml[4] - cfg.pml[5]
+    return (nxi, nyi, nzi, bl, bf, bu)
+
+
+def write_shot_results(directory: str, cfg: Config, shot: Shot, pp, ps, tp, vsp: bool = False,
+                       prefix: str = "result"):
+    """One shot's images as the reference writes them (output_3d_result,
+    3D_output_file.cu:309-428): `<prefix>-tp-<sy>-<sx>`, `-pp-`, `-ps-` in
+    `directory`, x-outer raw float32 with the absorbing layers cut off; sx, sy are
+    the shot's interior cell (the padded cell minus boundary_left / the y offset).
+    With vsp the names carry the interior source depth instead (`<prefix>-tp-<sz>`).
+    prefix "compensate-result" gives output_3d_result_compensate's names."""
+    os.makedirs(directory, exist_ok=True)
+    cut = _cut(cfg)
+    sx, sy, sz = shot.sx - cut[3], shot.sy - cut[4], shot.sz - cut[5]
+    tag = f"{sz}" if vsp else f"{sy}-{sx}"
+    paths = []
+    for name, vol in (("tp", tp), ("pp", pp), ("ps", ps)):
+        path = os.path.join(directory, f"{prefix}-{name}-{tag}")
+        write_volume_xyz(path, vol, cut)
+        paths.append(path)
+    return paths
+
+
+def write_excitation_files(directory: str, cfg: Config, shot: Shot, ex: dict):
+    """The excitation arrays of one shot as the reference writes them
+    (output_3d_wavefiled_excitation_amp_time, 3D_output_file.cu:155-250):
+    `ex-time-<sy>-<sx>` (whole padded grid) and `cut-ex-time`, `cut-ex-amp`,
+    `cut-ex-tp`, `cut-ex-vxp`, `cut-ex-vyp`, `cut-ex-vzp` (interior), x-outer raw
+    float32 (the excitation time as a float, as the reference stores it).  `ex` is
+    `Context.get_excitation()`."""
+    os.makedirs(directory, exist_ok=True)
+    cut = _cut(cfg)
+    sx, sy = shot.sx - cut[3], shot.sy - cut[4]
+    tag = f"{sy}-{sx}"
+    t = np.asarray(ex["time"], np.float32)
+    write_volume_xyz(os.path.join(directory, f"ex-time-{tag}"), t)
+    out = [os.path.join(directory, f"ex-time-{tag}")]
+    for name, key in (("time", "time"), ("amp", "amp"), ("tp", "etp"), ("vxp", "evx"), ("vyp", "evy"),
+                      ("vzp", "evz")):
+        path = os.path.join(directory, f"cut-ex-{name}-{tag}")
+        write_volume_xyz(path, np.asarray(ex[key], np.float32), cut)
+        out.append(path)
+    return out
+
+
 def write_shot_gathers(prefix: str, data):
     """Recorded data [3][nt][nrec] -> prefix_x.bin, prefix_y.bin, prefix_z.bin, each
     raw float32 [nrec][nt] (receiver-major, time fastest)."""

@@ -1,4 +1,6 @@
 """File formats of the reference and the direct-wave mute (host code, no GPU)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -60,3 +62,30 @@ def test_direct_wave_mute_on_the_device_matches_the_host(ertm):
     ertm.mute_direct(shot, dev, 0.5, (5.0, 5.0, 5.0), 1800.0, extra=3)
     assert np.array_equal(dev.cpu().numpy(), host)
 
+
+
+def test_reference_output_file_sets(ertm, tmp_path):
+    """Per-shot images and excitation arrays under the reference's file names, cut
+    to the interior, x-outer (output_3d_result / output_3d_wavefiled_excitation_amp_time)."""
+    cfg = ertm.Config(nx=14, ny=9, nz=11, dx=10, dy=10, dz=10, dt_ms=1, nt=10, pml=(3, 2, 1, 2, 4, 1))
+    shot = ertm.Shot(7, 4, 5, wavelet=[1.0])
+    rng = np.random.default_rng(3)
+    pp, ps, tp = (rng.standard_normal(cfg.shape).astype(np.float32) for _ in range(3))
+    paths = ertm.write_shot_results(str(tmp_path), cfg, shot, pp, ps, tp)
+    assert [os.path.basename(p) for p in paths] == ["result-tp-3-4", "result-pp-3-4", "result-ps-3-4"]
+    nxi, nyi, nzi = 14 - 5, 9 - 3, 11 - 5
+    back = ertm.read_volume_xyz(paths[1], nxi, nyi, nzi)
+    assert np.array_equal(back, pp[4:4 + nzi, 1:1 + nyi, 3:3 + nxi])
+    raw = np.fromfile(paths[0], np.float32).reshape(nxi, nyi, nzi)          # x-outer, z-inner
+    assert np.array_equal(raw, tp[4:4 + nzi, 1:1 + nyi, 3:3 + nxi].transpose(2, 1, 0))
+    vsp = ertm.write_shot_results(str(tmp_path), cfg, shot, pp, ps, tp, vsp=True, prefix="compensate-result")
+    assert os.path.basename(vsp[2]) == "compensate-result-ps-1"
+    ex = {"time": rng.integers(0, 9, cfg.shape).astype(np.int32),
+          **{k: rng.standard_normal(cfg.shape).astype(np.float32) for k in ("amp", "etp", "evx", "evy", "evz")}}
+    files = ertm.write_excitation_files(str(tmp_path), cfg, shot, ex)
+    names = [os.path.basename(f) for f in files]
+    assert names[0] == "ex-time-3-4" and "cut-ex-vzp-3-4" in names
+    full = ertm.read_volume_xyz(files[0], 14, 9, 11)
+    assert np.array_equal(full, ex["time"].astype(np.float32))
+    amp = ertm.read_volume_xyz(os.path.join(str(tmp_path), "cut-ex-amp-3-4"), nxi, nyi, nzi)
+    assert np.array_equal(amp, ex["amp"][4:4 + nzi, 1:1 + nyi, 3:3 + nxi])
