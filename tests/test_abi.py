@@ -102,3 +102,33 @@ int main(void)
                     str(src), "-o", str(exe), "-L", lib, "-lertm", "-Wl,-rpath," + lib], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.startswith("ok"), (out.returncode, out.stdout, out.stderr)
+
+
+def test_integration_shim_compiles_against_the_header(tmp_path):
+    """The C shim of INTEGRATION.md (what a maintainer adds to the reference's driver)
+    compiles against include/ertm.h, given declarations of the reference globals it
+    reads (3D_elastic_modeling_parameter)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    doc = open(os.path.join(REPO, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```c\n(.*?)```", doc, re.S)
+    assert blocks, "no C block in INTEGRATION.md"
+    globals_ = """
+typedef struct GPUdevice GPUdevice;
+extern int nnx, nny, nnz, lt, bl, br, bf, bb, bu, bd, wavelet_length;
+extern int gpuid[8], sx_real, sy_real, sz_real, add_receiver_bool;
+extern int receiver_start_x, receiver_num_x, receiver_interval_x;
+extern int receiver_start_y, receiver_num_y, receiver_interval_y, receiver_start_z;
+extern float dx, dy, dz, dt, coe_att;
+extern float *velocity_pml, *velocity1_pml, *density_pml, *s_velocity_pml, *s_velocity1_pml, *s_density_pml;
+extern float *wavelet, *obs_shot_all, *vresult_pp_h, *vresult_ps_h, *vresult_tp_h;
+void err(const char *fmt, ...);
+"""
+    src = tmp_path / "shim.c"
+    body = blocks[0].replace('#include "ertm.h"', '#include "ertm.h"\n' + globals_, 1)
+    src.write_text(body)
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-Wno-unused-function", "-I",
+                    os.path.join(REPO, "include"), "-c", str(src), "-o", str(tmp_path / "shim.o")], check=True)
