@@ -101,6 +101,7 @@ SIGNATURES = {
     "ertm_propagate": (C.c_int, [_P, C.c_int, C.POINTER(_Shot), C.c_int]),
     "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
     "ertm_kernel_launches": (C.c_int64, [_P]),
+    "ertm_set_wait_fault": (C.c_int, [_P, C.c_int, C.c_uint32]),
     "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_write_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
@@ -490,6 +491,13 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self._L.ertm_kernel_launches(self._h))
+
+    def set_wait_fault(self, plane: int = -1, polls: int = 0):
+        """Test hook of the device-error path: the first CTA of each step kernel skips
+        the staged copy of its z plane `plane`, so its bounded wait runs out after
+        `polls` polls (0: default) and the pass raises ErtmError(ERTM_EDEVICE);
+        plane = -1 turns it off."""
+        self._ck(self._L.ertm_set_wait_fault(self._h, int(plane), int(polls)))
 
 
 def forward_together_using_real_model_noalloc(cfg: Config, vp, vs, rho, shot: Shot, out,

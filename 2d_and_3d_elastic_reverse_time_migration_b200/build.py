@@ -17,7 +17,7 @@ OBJ = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libertm.so")
 
-SOURCES = ["ertm_api.cu", "aux.cu", "launch_r4.cu", "launch_r6.cu", "noalloc.cu", "born.cu", "windows.cu", "nn.cu", "io.cu", "postfilter.cu"]
+SOURCES = ["ertm_api.cu", "setup.cu", "aux.cu", "launch_r4.cu", "launch_r6.cu", "noalloc.cu", "born.cu", "windows.cu", "nn.cu", "io.cu", "postfilter.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(REPO, "include"), "-I" + CSRC]

@@ -98,6 +98,10 @@ struct ertm_ctx {
     CUtensorMap mModel[2][3];
     CUtensorMap mExAmp, mExTime;
 
+    // test hook of the device-error path (ertm_set_wait_fault)
+    int skip_plane1 = 0;
+    unsigned wait_polls = 0;
+
     std::string err;
     long long launches = 0;
 
@@ -148,28 +152,6 @@ bool is_device_ptr(const void* p)
 }
 
 long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
-
-Geom make_geom(const ertm_config& c, int R)
-{
-    Geom g{};
-    g.nx = c.nx;
-    g.ny = c.ny;
-    g.nz = c.nz;
-    g.R = R;
-    g.two_d = (c.ny == 1);
-    g.tyb = g.two_d ? TY2 : TY3;
-    g.hx = XH;
-    g.hy = g.two_d ? 0 : R;
-    g.hz = R;
-    g.px = round_up(2LL * g.hx + round_up(c.nx, TX), 32);
-    g.py = 2LL * g.hy + round_up(c.ny, g.tyb);
-    g.pz = 2LL * g.hz + c.nz + 1;
-    g.sy = g.px;
-    g.sz = g.px * g.py;
-    g.off0 = g.hz * g.sz + g.hy * g.sy + g.hx;
-    g.total = g.px * g.py * g.pz;
-    return g;
-}
 
 bool field_used(const Geom& g, int f)
 {
@@ -223,21 +205,7 @@ int upload_profiles(ertm_ctx* c, float vmax)
             for (int h = 0; h < 2; h++) {
                 int stg = h == 0 ? 0 : (ax == 2 ? 1 : -1);
                 std::vector<float> a(n), b(n);
-                for (int i = 0; i < n; i++) {
-                    // C-PML (Komatitsch & Martin 2007), kappa = 1; see orc_cpml_profile
-                    double p = i + 0.5 * stg, dist = 0.0, L = 1.0;
-                    if (w0 > 0 && p < w0 - 1) { dist = (w0 - 1) - p; L = w0; }
-                    else if (w1 > 0 && p > n - w1) { dist = p - (n - w1); L = w1; }
-                    if (dist <= 0.0) { a[i] = 0.f; b[i] = 1.f; continue; }
-                    double Lm = L * hs[ax], x = dist * hs[ax] / Lm;
-                    double d0 = -3.0 * vmax * std::log(rc) / (2.0 * Lm);
-                    double d = d0 * x * x;
-                    double al = M_PI * f0 * (1.0 - x);
-                    if (al < 0) al = 0;
-                    double bb = std::exp(-(d + al) * dts);
-                    b[i] = (float)bb;
-                    a[i] = (float)(d * (bb - 1.0) / (d + al));
-                }
+                cpml_profile(n, w0, w1, stg, hs[ax], vmax, rc, f0, dts, 0, n, a.data(), b.data());
                 if (!c->pa[ax][h]) {
                     const int cap = ax == 0 ? c->cap_nx : ax == 1 ? c->cap_ny : g.nz;
                     CK(c, cudaMalloc(&c->pa[ax][h], sizeof(float) * cap));
@@ -254,37 +222,12 @@ int upload_profiles(ertm_ctx* c, float vmax)
         return ERTM_OK;
     }
     if (c->att_ready) return ERTM_OK;
-    const double pai = 3.1415926;   // 3D_zzzzz:1
     for (int ax = 0; ax < 3; ax++) {
         int n = ns[ax];
         std::vector<float> v(n, 0.f);
-        int w0 = cf.pml[2 * ax], w1 = cf.pml[2 * ax + 1];
-        if (!(ax == 1 && g.two_d)) {
-            float coe = cf.sponge_coef;
-            // coe_attenuation_3d_new2 (3D_zzzzz:261-300) / make_attenuation_new (zzzzz:238-280)
-            for (int i = 0; i < w0 && i < n; i++) {
-                float val;
-                if (cf.boundary == ERTM_BOUNDARY_SPONGE_COS)
-                    val = (float)(coe * (1.0 - std::cos(pai / 2 * (w0 - i - 1) / (w0 - 1))));
-                else {
-                    float x = (float)((w0 - 1.0 - i) / (w0 - 1.0));
-                    val = (float)(coe * std::pow(x * 1.0, 3.0));
-                }
-                v[i] += val;
-            }
-            for (int q = 0; q < w1; q++) {
-                int i = n - w1 + q;
-                if (i < 0) continue;
-                float val;
-                if (cf.boundary == ERTM_BOUNDARY_SPONGE_COS)
-                    val = (float)(coe * (1.0 - std::cos(pai / 2 * q / (w1 - 1))));
-                else {
-                    float x = (float)(q / (w1 - 1.0));
-                    val = (float)(coe * std::pow(x * 1.0, 3.0));
-                }
-                v[i] += val;
-            }
-        }
+        if (!(ax == 1 && g.two_d))
+            sponge_profile(n, cf.pml[2 * ax], cf.pml[2 * ax + 1], cf.boundary, cf.sponge_coef, 0, n,
+                           v.data());
         if (!c->att[ax]) {
             const int cap = ax == 0 ? c->cap_nx : ax == 1 ? c->cap_ny : g.nz;
             CK(c, cudaMalloc(&c->att[ax], sizeof(float) * cap));
@@ -531,6 +474,8 @@ void fill_args(ertm_ctx* c, int which, const ertm_shot* s, KArgs& a)
     }
     a.ex_tp = c->ex_tp_base ? c->ex_tp_base + g.off0 : nullptr;
     a.err = c->err_d;
+    a.skip_plane1 = c->skip_plane1;
+    a.wait_polls = c->wait_polls;
 }
 
 int check_device_error(ertm_ctx* c)
@@ -551,40 +496,6 @@ long long psi_count(const Geom& g, const ertm_config& c, int p)
     const int ax = kPsiAxis[p];
     const long long w = c.pml[2 * ax] + c.pml[2 * ax + 1];
     return ax == 0 ? (long long)g.nz * g.ny * w : ax == 1 ? (long long)g.nz * w * g.nx : w * g.ny * g.nx;
-}
-
-// z planes per CTA.  3D: chunks of about 32 planes, balanced over nz.  Timed on
-// B200 at 480 x 480 x 380 (R = 4, C-PML), the step kernels get faster as the
-// chunk shrinks from the whole column (380 planes) down to 32-48 planes
-// (stress 1.92 -> 1.51 ms, velocity 1.98 -> 1.61 ms per launch), while below
-// ~24 planes the z-queue fill of each chunk starts to cost more than the finer
-// load balance gains.  2D: the chunk count minimises (waves of CTAs) x
-// (planes per chunk + start-up of ~2R planes).
-int choose_kchunk(const ertm_ctx* c)
-{
-    const Geom& g = c->g;
-    if (!g.two_d) {
-        const int target = 32;
-        const int chunks = std::max(1, (g.nz + target / 2) / target);
-        return (g.nz + chunks - 1) / chunks;
-    }
-    long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const long long slots = (long long)sms * 8;
-    const double startup = 2.0 * c->R;
-    int best = g.nz;
-    double best_cost = 1e300;
-    for (int kc = g.nz; kc >= std::min(g.nz, 16); kc--) {
-        long long chunks = (g.nz + kc - 1) / kc;
-        long long waves = (cols * chunks + slots - 1) / slots;
-        double cost = (double)waves * (kc + startup);
-        if (cost < best_cost - 1e-9) {
-            best_cost = cost;
-            best = kc;
-        }
-    }
-    return best;
 }
 
 // Z-chunk autotuner (ertm_config.autotune = 1).  For each grid shape, stencil
@@ -704,7 +615,7 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
     int rc;
     float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[which];
     if ((rc = upload_profiles(c, vmax))) return rc;
-    int kchunk = choose_kchunk(c);
+    int kchunk = choose_kchunk(c->g, c->R, c->device);
     if (c->cfg.autotune == 1 && (rc = autotune_kchunk(c, which, &kchunk))) return rc;
     if ((rc = reset_state(c))) return rc;
     if (mode != MODE_RECEIVER && (rc = upload_wavelet(c, s))) return rc;
@@ -845,7 +756,7 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     x->cfg = c;
     x->R = c.order / 2;
     x->device = c.device;
-    x->g = make_geom(c, x->R);
+    x->g = make_geom(c.nx, c.ny, c.nz, x->R);
     if (x->g.total >= (1LL << 31)) {   // the step kernels index a volume with 32-bit offsets
         const long long total = x->g.total;
         delete x;
@@ -867,33 +778,7 @@ int ertm_create(const ertm_config* cfg, ertm_ctx** out)
     }
     x->stream = x->own_stream;
     // difference coefficients
-    if (c.coef_kind == ERTM_COEF_USER) {
-        for (int n = 0; n < 8; n++) x->coef[n] = n <= x->R ? c.coef[n] : 0.f;
-    } else if (c.coef_kind == ERTM_COEF_REFERENCE12) {
-        const float rc12[7] = {0.0f, 1.2213363647f, -0.096931457519f, 0.017447662353f,
-                               -0.0029672895159f, 0.00035900539822f, -0.00002184781161f};
-        for (int n = 0; n < 7; n++) x->coef[n] = rc12[n];
-    } else {
-        // Taylor coefficients: solve sum_n c_n (2n-1)^(2m-1) = delta_{m1}
-        const int R = x->R;
-        double A[8][9];
-        for (int m = 0; m < R; m++) {
-            for (int n = 0; n < R; n++) A[m][n] = std::pow(2.0 * n + 1.0, 2.0 * m + 1.0);
-            A[m][R] = (m == 0);
-        }
-        for (int cc = 0; cc < R; cc++) {
-            int p = cc;
-            for (int r = cc + 1; r < R; r++) if (std::fabs(A[r][cc]) > std::fabs(A[p][cc])) p = r;
-            for (int k = 0; k <= R; k++) std::swap(A[cc][k], A[p][k]);
-            for (int r = 0; r < R; r++) {
-                if (r == cc) continue;
-                double f = A[r][cc] / A[cc][cc];
-                for (int k = cc; k <= R; k++) A[r][k] -= f * A[cc][k];
-            }
-        }
-        x->coef[0] = 0.f;
-        for (int n = 0; n < R; n++) x->coef[n + 1] = (float)(A[n][R] / A[n][n]);
-    }
+    stencil_coefs(c.coef_kind, c.coef, x->R, x->coef);
     for (int q = 0; q < NFIELD; q++) {
         if (!field_used(x->g, q)) continue;
         if ((rc = alloc_volume(x, &x->f_base[q], &x->f[q]))) return bail(rc);
@@ -1326,7 +1211,7 @@ int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
     if ((rc = upload_wavelet(c, s))) return rc;
     KArgs a;
     fill_args(c, 1, s, a);
-    a.kchunk = choose_kchunk(c);
+    a.kchunk = choose_kchunk(c->g, c->R, c->device);
     const bool cpml = c->cfg.boundary == ERTM_BOUNDARY_CPML;
     cudaEvent_t ev[3];
     for (int q = 0; q < 3; q++) CK(c, cudaEventCreate(&ev[q]));
@@ -1357,6 +1242,15 @@ int ertm_time_kernels(ertm_ctx* c, const ertm_shot* s, int nsteps, float* ms)
 }
 
 int64_t ertm_kernel_launches(const ertm_ctx* c) { return c ? c->launches : 0; }
+
+int ertm_set_wait_fault(ertm_ctx* c, int plane, uint32_t polls)
+{
+    if (!c) return ERTM_EINVAL;
+    if (plane < -1) return fail(c, ERTM_EINVAL, "plane = %d", plane);
+    c->skip_plane1 = plane + 1;
+    c->wait_polls = polls;
+    return ERTM_OK;
+}
 
 }  // extern "C"
 

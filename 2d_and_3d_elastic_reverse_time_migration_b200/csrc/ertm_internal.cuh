@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ertm.h"
+
 namespace ertm {
 
 constexpr int TX = 32;        // x tile = one warp
@@ -80,6 +82,12 @@ struct KArgs {
     float* ex_tp;
     float* img[3];
     int* err;                        // device error word (0 = ok)
+    // test hook of the device-error path (zero = off, so a zeroed KArgs is safe):
+    // with skip_plane1 = t + 1 the first CTA of the grid does not issue the
+    // staged copy of its chunk's plane t, so its consumers' bounded wait
+    // (wait_polls polls; 0 = kWaitPolls) runs out
+    int skip_plane1;
+    unsigned wait_polls;
 };
 
 // Device error codes written to KArgs::err
@@ -107,6 +115,37 @@ struct VelMaps {
 
 // x halo of the staged tiles: >= R and a multiple of 4 floats (16-byte TMA x start)
 constexpr int xb_of(int R) { return R <= 4 ? 4 : 8; }
+
+// Dynamic shared-memory opt-in of kernel `K` (a function attribute of the
+// device's context): made once per device, on the first launch with that
+// device current.  `done` is the kernel's own bit set of devices (one static
+// per kernel instantiation at the call site).
+template <typename KPTR>
+inline cudaError_t smem_opt_in(KPTR K, size_t smem, unsigned long long* done)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (__atomic_load_n(done, __ATOMIC_ACQUIRE) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && bit) __atomic_fetch_or(done, bit, __ATOMIC_RELEASE);
+    return e;
+}
+
+// Host set-up shared by the context path and the no-allocation path (setup.cu).
+Geom make_geom(int nx, int ny, int nz, int R);
+// difference coefficients c_0..c_R (c_0 = 0) for ERTM_COEF_* `coef_kind`
+void stencil_coefs(int coef_kind, const float* user, int R, float coef[8]);
+// C-PML a/b coefficients of one axis of n cells at integer (stg 0) or half points
+// (stg +1 or -1), for cells i0 .. i0+m-1 into a[0..m), b[0..m)
+void cpml_profile(int n, int w0, int w1, int stg, double h, double vmax, double rcoef, double f0,
+                  double dts, int i0, int m, float* a, float* b);
+// sponge damping (1/s, ERTM_BOUNDARY_SPONGE_COS or _CUBIC ramps) of one axis of n
+// cells, for cells i0 .. i0+m-1 into v[0..m)
+void sponge_profile(int n, int w0, int w1, int kind, float coe, int i0, int m, float* v);
+// z planes per CTA of the step kernels for grid g on `device`
+int choose_kchunk(const Geom& g, int R, int device);
 
 // Launchers (one translation unit per stencil radius).
 cudaError_t launch_stress(int R, const Geom& g, const KArgs& a, const StressMaps& m, bool cpml,

@@ -28,6 +28,7 @@
 #include <algorithm>
 
 #include "ertm.h"
+#include "ertm_internal.cuh"
 
 namespace {
 
@@ -463,8 +464,8 @@ cudaError_t gemm_bn(const LA& la, const LB& lb, const EP& ep, int M, int N, int 
     const int kt_per = (KT + splitk - 1) / splitk;
     const int gz = (KT + kt_per - 1) / kt_per;
     const size_t smem = sizeof(Smem<BN>);
-    static cudaError_t attr =
-        cudaFuncSetAttribute(k_gemm<BN, LA, LB, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static unsigned long long opted = 0;   // devices with the opt-in made
+    cudaError_t attr = ertm::smem_opt_in(k_gemm<BN, LA, LB, EP>, smem, &opted);
     if (attr != cudaSuccess) return attr;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, gz);
     k_gemm<BN, LA, LB, EP><<<grid, NT, smem, st>>>(la, lb, ep, M, N, K, kt_per, err);

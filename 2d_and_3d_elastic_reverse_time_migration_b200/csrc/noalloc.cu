@@ -16,8 +16,9 @@
 //    does not fit is rejected with ERTM_EINVAL and a message giving the need;
 //  * every GPU that loads this file's module holds the array until exit;
 //  * the array's device address is looked up once per device, on the first
-//    call made with that device current (cudaGetSymbolAddress); make that
-//    first call before any stream capture on the device;
+//    call made with that device current (cudaGetSymbolAddress), and again
+//    after the device's context changed (a device reset); make that first
+//    call before any stream capture on the device;
 //  * all calls share the array: calls that overlap on the GPU (two streams,
 //    two host threads) race and give wrong results; the caller serialises them;
 //  * the state is cleared at the start of every call, so the array's previous
@@ -47,6 +48,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_scratch_mu;
 void* g_scratch_ptr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};
 
 thread_local char g_noalloc_err[512];
 
@@ -59,23 +61,48 @@ int nfail(int code, const char* fmt, ...)
     return code;
 }
 
-// device address of the scratch array on the current device (looked up once per device)
+// the CUDA context current on this thread (driver entry point, no -lcuda needed)
+CUcontext current_context()
+{
+    static PFN_cuCtxGetCurrent_v4000 get = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return (PFN_cuCtxGetCurrent_v4000)p;
+    }();
+    CUcontext ctx = nullptr;
+    if (!get || get(&ctx) != CUDA_SUCCESS) return nullptr;
+    return ctx;
+}
+
+// Device address of the scratch array in the current context of device `dev`.
+// The lookup (cudaGetSymbolAddress) is cached per device together with the
+// context it was made in: after the caller resets the device, its new primary
+// context loads the module afresh and the lookup is repeated.
 int scratch_base(int dev, unsigned char** out)
 {
     if (dev < 0 || dev >= kMaxDevices) return nfail(ERTM_EINVAL, "device %d not supported", dev);
+    const CUcontext ctx = current_context();
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return nfail(ERTM_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
         g_scratch_ptr[dev] = p;
+        g_scratch_ctx[dev] = ctx;
     }
     *out = static_cast<unsigned char*>(g_scratch_ptr[dev]);
     return ERTM_OK;
 }
 
-bool on_device(const void* p)
+// a pointer the kernels on `dev` may use: device memory of that GPU, or managed memory
+bool on_device(const void* p, int dev)
 {
     if (!p) return false;
     cudaPointerAttributes at;
@@ -83,10 +110,9 @@ bool on_device(const void* p)
         cudaGetLastError();
         return false;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
-
-long long rup(long long v, long long m) { return (v + m - 1) / m * m; }
 
 // bump allocator over the scratch array (256-byte aligned sub-buffers)
 struct Carve {
@@ -178,25 +204,18 @@ int run_noalloc(const ertm_config* cfg, const float* vp, const float* vs, const 
     if (two_d && (s->nry > 1 || s->ry0 != 0 || s->sy != 0))
         return nfail(ERTM_EINVAL, "2D grid: receivers and source must sit at y = 0");
     const long long nrec = (long long)s->nrx * s->nry;
-    if (!on_device(vp) || !on_device(vs) || !on_device(rho) || (nrec > 0 && !on_device(data_out)) ||
-        (s->nw > 0 && !on_device(s->wavelet)))
-        return nfail(ERTM_EINVAL, "vp, vs, rho, wavelet and data_out must be device pointers");
     if (c.device < 0) return nfail(ERTM_EINVAL, "device %d", c.device);
+    const int dv = c.device;
+    if (!on_device(vp, dv) || !on_device(vs, dv) || !on_device(rho, dv) ||
+        (nrec > 0 && !on_device(data_out, dv)) || (s->nw > 0 && !on_device(s->wavelet, dv)))
+        return nfail(ERTM_EINVAL, "vp, vs, rho, wavelet and data_out must be memory of device %d "
+                     "(cudaMalloc on that device, or managed)", dv);
     NCK(cudaSetDevice(c.device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // geometry of the padded volumes (same layout as the context path)
     const int R = c.order / 2;
-    Geom g{};
-    g.nx = c.nx; g.ny = c.ny; g.nz = c.nz; g.R = R; g.two_d = two_d;
-    g.tyb = two_d ? TY2 : TY3;
-    g.hx = XH; g.hy = two_d ? 0 : R; g.hz = R;
-    g.px = rup(2LL * g.hx + rup(c.nx, TX), 32);
-    g.py = 2LL * g.hy + rup(c.ny, g.tyb);
-    g.pz = 2LL * g.hz + c.nz + 1;
-    g.sy = g.px; g.sz = g.px * g.py;
-    g.off0 = g.hz * g.sz + g.hy * g.sy + g.hx;
-    g.total = g.px * g.py * g.pz;
+    const Geom g = make_geom(c.nx, c.ny, c.nz, R);
 
     // scratch plan: wavefields, model products, profiles, memory variables, counters
     static const int kAxis[NPSI] = {0, 1, 2, 1, 0, 2, 0, 2, 1, 0, 1, 2, 0, 1, 2, 0, 1, 2};
@@ -272,33 +291,10 @@ int run_noalloc(const ertm_config* cfg, const float* vp, const float* vs, const 
     }
 
     // difference coefficients
-    float coef[8] = {0};
-    if (c.coef_kind == ERTM_COEF_USER) {
-        for (int n = 0; n <= R; n++) coef[n] = c.coef[n];
-    } else if (c.coef_kind == ERTM_COEF_REFERENCE12) {
-        const float r12[7] = {0.0f, 1.2213363647f, -0.096931457519f, 0.017447662353f,
-                              -0.0029672895159f, 0.00035900539822f, -0.00002184781161f};
-        for (int n = 0; n < 7; n++) coef[n] = r12[n];
-    } else {
-        double A[8][9];
-        for (int m = 0; m < R; m++) {
-            for (int n = 0; n < R; n++) A[m][n] = std::pow(2.0 * n + 1.0, 2.0 * m + 1.0);
-            A[m][R] = (m == 0);
-        }
-        for (int cc = 0; cc < R; cc++) {
-            int p = cc;
-            for (int r = cc + 1; r < R; r++) if (std::fabs(A[r][cc]) > std::fabs(A[p][cc])) p = r;
-            for (int k = 0; k <= R; k++) { double t = A[cc][k]; A[cc][k] = A[p][k]; A[p][k] = t; }
-            for (int r = 0; r < R; r++) {
-                if (r == cc) continue;
-                double f = A[r][cc] / A[cc][cc];
-                for (int k = cc; k <= R; k++) A[r][k] -= f * A[cc][k];
-            }
-        }
-        for (int n = 0; n < R; n++) coef[n + 1] = (float)(A[n][R] / A[n][n]);
-    }
+    float coef[8];
+    stencil_coefs(c.coef_kind, c.coef, R, coef);
 
-    // boundary profiles (host arrays on the stack-owned std::vector-free path: fixed chunks)
+    // boundary profiles, computed in stack chunks and copied synchronously
     const double dts = c.dt_ms / 1000.0;
     const double hs[3] = {c.dx, c.dy, c.dz};
     for (int ax = 0; ax < 3; ax++) {
@@ -308,56 +304,17 @@ int run_noalloc(const ertm_config* cfg, const float* vp, const float* vs, const 
         float chunk[4][256];
         for (int i0 = 0; i0 < n; i0 += 256) {
             const int m = n - i0 < 256 ? n - i0 : 256;
-            for (int q = 0; q < m; q++) {
-                const int i = i0 + q;
-                if (cpml) {
-                    const double rcoef = c.pml_r > 0 ? c.pml_r : 1e-3;
-                    const double f0 = c.pml_f0 > 0 ? c.pml_f0 : 10.0;
-                    for (int h = 0; h < 2; h++) {
-                        const int stg = h == 0 ? 0 : (ax == 2 ? 1 : -1);
-                        double p = i + 0.5 * stg, dist = 0.0, L = 1.0;
-                        if (w0 > 0 && p < w0 - 1) { dist = (w0 - 1) - p; L = w0; }
-                        else if (w1 > 0 && p > n - w1) { dist = p - (n - w1); L = w1; }
-                        float av = 0.f, bv = 1.f;
-                        if (dist > 0.0) {
-                            double Lm = L * hs[ax], x = dist * hs[ax] / Lm;
-                            double d = -3.0 * vmax * std::log(rcoef) / (2.0 * Lm) * x * x;
-                            double al = M_PI * f0 * (1.0 - x);
-                            if (al < 0) al = 0;
-                            double bb = std::exp(-(d + al) * dts);
-                            bv = (float)bb;
-                            av = (float)(d * (bb - 1.0) / (d + al));
-                        }
-                        chunk[2 * h][q] = av;
-                        chunk[2 * h + 1][q] = bv;
-                    }
-                } else {
-                    const double pai = 3.1415926;
-                    float v = 0.f;
-                    if (!(ax == 1 && two_d)) {
-                        const float coe = c.sponge_coef;
-                        if (i < w0) {
-                            if (c.boundary == ERTM_BOUNDARY_SPONGE_COS)
-                                v += (float)(coe * (1.0 - std::cos(pai / 2 * (w0 - i - 1) / (w0 - 1))));
-                            else {
-                                float x = (float)((w0 - 1.0 - i) / (w0 - 1.0));
-                                v += (float)(coe * std::pow(x * 1.0, 3.0));
-                            }
-                        }
-                        if (i >= n - w1) {
-                            const int q1 = i - (n - w1);
-                            if (c.boundary == ERTM_BOUNDARY_SPONGE_COS)
-                                v += (float)(coe * (1.0 - std::cos(pai / 2 * q1 / (w1 - 1))));
-                            else {
-                                float x = (float)(q1 / (w1 - 1.0));
-                                v += (float)(coe * std::pow(x * 1.0, 3.0));
-                            }
-                        }
-                    }
-                    chunk[0][q] = v;
+            if (cpml) {
+                const double rcoef = c.pml_r > 0 ? c.pml_r : 1e-3;
+                const double f0 = c.pml_f0 > 0 ? c.pml_f0 : 10.0;
+                for (int h = 0; h < 2; h++) {
+                    const int stg = h == 0 ? 0 : (ax == 2 ? 1 : -1);
+                    cpml_profile(n, w0, w1, stg, hs[ax], vmax, rcoef, f0, dts, i0, m, chunk[2 * h],
+                                 chunk[2 * h + 1]);
                 }
+            } else {
+                sponge_profile(n, w0, w1, c.boundary, c.sponge_coef, i0, m, chunk[0]);
             }
-            // synchronous copies from this stack chunk (pageable host memory)
             for (int h = 0; h < (cpml ? 4 : 1); h++)
                 NCK(cudaMemcpyAsync(prof[ax][h] + i0, chunk[h], 4 * m, cudaMemcpyHostToDevice, st));
             NCK(cudaStreamSynchronize(st));
@@ -399,21 +356,8 @@ int run_noalloc(const ertm_config* cfg, const float* vp, const float* vs, const 
     a.it_ptr = counters;
     a.err = counters + 4;
 
-    // z planes per CTA (same rule as the context path)
-    {
-        long long cols = (long long)((g.nx + TX - 1) / TX) * ((g.ny + g.tyb - 1) / g.tyb);
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-        const long long slots = (long long)sms * (two_d ? 8 : CTAS3);
-        int best = g.nz;
-        double best_cost = 1e300;
-        for (int kc = g.nz; kc >= (g.nz < 16 ? g.nz : 16); kc--) {
-            long long chunks = (g.nz + kc - 1) / kc;
-            double cost = (double)((cols * chunks + slots - 1) / slots) * (kc + 2.0 * R);
-            if (cost < best_cost - 1e-9) { best_cost = cost; best = kc; }
-        }
-        a.kchunk = best;
-    }
+    // z planes per CTA: the context path's rule
+    a.kchunk = choose_kchunk(g, R, c.device);
 
     // tensor maps over the scratch volumes
     StressMaps sm;

@@ -116,11 +116,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
 // Bounded wait on a stage: gives up after a fixed number of polls (each poll
 // may suspend the thread for a while), so a lost copy cannot hang the GPU.
 constexpr unsigned kWaitPolls = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
+                                                  unsigned polls = kWaitPolls)
 {
-    for (unsigned n = 0; n < kWaitPolls; n++)
+    for (unsigned n = 0; n < polls; n++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+// the consumers' budget: the test hook's, else the default
+__device__ __forceinline__ unsigned consumer_polls(const KArgs& a)
+{
+    return a.wait_polls ? a.wait_polls : kWaitPolls;
+}
+// the test hook's skipped copy: plane t of the first CTA of the grid
+__device__ __forceinline__ bool skip_plane(const KArgs& a, int t)
+{
+    return a.skip_plane1 == t + 1 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
@@ -165,20 +176,25 @@ struct Boxes {
 // previous plane is released.  Every wait is bounded; before returning it
 // waits (bounded) for the copies still in flight, so the block never exits
 // with a TMA write into its shared memory pending.  False if a wait gave up.
+// A consumer whose wait on a stage gives up stops at once without releasing
+// that stage, so a stage is refilled only after every consumer saw its
+// previous copy land: no copy is ever issued into a stage whose last copy is
+// still pending.
 template <int NS, class Issue>
-__device__ __forceinline__ bool produce_planes(uint64_t* bars, int nk, Issue issue)
+__device__ __forceinline__ bool produce_planes(uint64_t* bars, int nk, unsigned polls, Issue issue)
 {
     bool ok = true;
-    int t = 0;
+    int t = 0, skipped = -1;
     for (; t < nk; ++t) {
-        if (t >= NS && !mbar_wait_bounded(&bars[NS + t % NS], ((t / NS) - 1) & 1)) {
+        if (t >= NS && !mbar_wait_bounded(&bars[NS + t % NS], ((t / NS) - 1) & 1, polls)) {
             ok = false;
             break;
         }
-        issue(t);
+        if (!issue(t)) skipped = t;
     }
+    // drain: every copy issued into the ring has landed before the block exits
     for (int u = (t > NS ? t - NS : 0); u < t; ++u)
-        if (!mbar_wait_bounded(&bars[u % NS], (u / NS) & 1)) ok = false;
+        if (u != skipped && !mbar_wait_bounded(&bars[u % NS], (u / NS) & 1)) ok = false;
     return ok;
 }
 
@@ -239,7 +255,8 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     float* tp = a.f[F_TP];
     const int cj = j * sy + i;
 
-    auto issue = [&](int t) {   // leader only: all boxes of iteration t into stage t % S
+    auto issue = [&](int t) -> bool {   // leader only: all boxes of iteration t into stage t % S
+        if (skip_plane(a, t)) return false;
         const int st = t % NS;
         float* S = sm + st * SS::STAGE;
         uint64_t* bar = &bars[st];
@@ -255,6 +272,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
         if (PS) tma3(S + SS::OFF_C + C_TP * CB, &maps.tp, gx, gy, z, bar);
         tma3(S + SS::OFF_C + C_M * CB, &maps.M, gx, gy, z, bar);
         tma3(S + SS::OFF_C + C_MU * CB, &maps.MU, gx, gy, z, bar);
+        return true;
     };
 
     // C-PML: slab membership and profile coefficients of this column
@@ -308,7 +326,8 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     }
     __syncthreads();
     if (ty == TYB) {   // producer warp
-        if (leader && !produce_planes<NS>(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        if (leader && !produce_planes<NS>(bars, nk, consumer_polls(a), issue) && a.err)
+            atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -328,10 +347,15 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     cpa_wait_1();
 
     bool ok = true;
+    const unsigned polls = consumer_polls(a);
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
         const int st = t % NS;
-        if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
+        if (!mbar_wait_bounded(&bars[st], (t / NS) & 1, polls)) {
+            ok = false;          // stop here: the stage stays unreleased
+            cpa_wait_all();
+            break;
+        }
         if (t + 2 < nk) issue_psi(k + 2, (t + 2) % 3);
         else cpa_commit();   // keep one group per iteration
         const float* S = sm + st * SS::STAGE;
@@ -527,7 +551,8 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     float* vyp = a.f[F_VYP];
     float* vzp = a.f[F_VZP];
 
-    auto issue = [&](int t) {
+    auto issue = [&](int t) -> bool {
+        if (skip_plane(a, t)) return false;
         const int st = t % NS;
         float* S = sm + st * VS::STAGE;
         uint64_t* bar = &bars[st];
@@ -545,6 +570,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
         for (int f = 0; f < VS::NFR; f++) tma3(S + VS::O_FR + f * CB, &maps.fr[f], gx, gy, z + R, bar);
 #pragma unroll
         for (int q = 0; q < VS::NC; q++) tma3(S + VS::O_C + q * CB, &maps.c[q], gx, gy, z, bar);
+        return true;
     };
 
     const int WX = a.w[0] + a.w[1], WY = a.w[2] + a.w[3];
@@ -597,7 +623,8 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     }
     __syncthreads();
     if (ty == TYB) {   // producer warp
-        if (leader && !produce_planes<NS>(bars, nk, issue) && a.err) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+        if (leader && !produce_planes<NS>(bars, nk, consumer_polls(a), issue) && a.err)
+            atomicExch(a.err, DEV_WAIT_TIMEOUT);
         return;
     }
 
@@ -620,10 +647,15 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     cpa_wait_1();
 
     bool ok = true;
+    const unsigned polls = consumer_polls(a);
     for (int t = 0; t < nk; ++t) {
         const int k = k0 + t;
         const int st = t % NS;
-        if (ok) ok = mbar_wait_bounded(&bars[st], (t / NS) & 1);
+        if (!mbar_wait_bounded(&bars[st], (t / NS) & 1, polls)) {
+            ok = false;          // stop here: the stage stays unreleased
+            cpa_wait_all();
+            break;
+        }
         if (t + 2 < nk) issue_psi(k + 2, (t + 2) % 3);
         else cpa_commit();   // keep one group per iteration
         const float* S = sm + st * VS::STAGE;
@@ -807,13 +839,13 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
 // Launch helpers (instantiated per R in launch_r4.cu / launch_r6.cu)
 // ---------------------------------------------------------------------------
 // One instantiation per kernel, so the shared-memory opt-in below is made for
-// each kernel separately (the kernels share their function types).
+// each kernel separately (the kernels share their function types), once per device.
 template <typename MAPS, void (*K)(MAPS, KArgs)>
 static cudaError_t launch_dyn(dim3 grid, dim3 block, size_t smem, const MAPS& m, const KArgs& a,
                               cudaStream_t st)
 {
-    static cudaError_t attr = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
+    static unsigned long long opted = 0;
+    cudaError_t attr = smem_opt_in(K, smem, &opted);
     if (attr != cudaSuccess) return attr;
     K<<<grid, block, smem, st>>>(m, a);
     return cudaGetLastError();

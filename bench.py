@@ -52,10 +52,13 @@ def parse():
     ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
-    ap.add_argument("--workload", default="shot", choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op"],
+    ap.add_argument("--workload", default="shot",
+                    choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op", "refstep"],
                     help="windows: batched aperture windows; unet: one U-Net training step at "
                          "256x512, batch 16; lsrtm: learned vs plain CG (each its own line); "
-                         "lsrtm-op: Born forward + adjoint per shot on the 880x480 GSLS-3 LSRTM grid")
+                         "lsrtm-op: Born forward + adjoint per shot on the 880x480 GSLS-3 LSRTM grid; "
+                         "refstep: the reference's own 2D CUDA step kernels against this "
+                         "library's 2D step on the same grids and GPU")
     ap.add_argument("--train-models", type=int, default=48)
     ap.add_argument("--test-models", type=int, default=6)
     ap.add_argument("--train-steps", type=int, default=1500)
@@ -382,6 +385,66 @@ def run_lsrtm_op(args):
     ctx.close()
 
 
+def run_refstep(args):
+    """The reference's own 2D CUDA time step (its stress kernel
+    fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization and its velocity kernels
+    adjoint_fwd_vx/vz_viscoelastic, 2D_elastic_RTM/viscoelastic_equation.cu:184-325,
+    :1827-2122, compiled from the reference tree into oracle/_ref/libref2d.so) against
+    this library's 2D step (k_stress + k_velocity, source-pass variant with the P
+    stress, the reference's 12th-order coefficients and cubic sponge) on the same
+    interior grids, CUDA events around every launch, after warm-up steps.  One line
+    per grid.  The reference kernels also carry one memory-variable set per cell
+    (viscoelastic form; tao = strain = 1 makes it elastic), so they move more bytes."""
+    import numpy as np
+    import torch
+    ertm = importlib.import_module(PKG)
+    lib_path = os.path.join(REPO, "oracle", "_ref", "libref2d.so")
+    if not os.path.exists(lib_path):
+        print(json.dumps({"workload": "refstep", "unavailable": "oracle/_ref/libref2d.so not built "
+                          "(the reference tree is needed to build it)"}), flush=True)
+        return
+    L = C.CDLL(lib_path)
+    coe = np.array([0.0, 1.2213363647, -0.096931457519, 0.017447662353, -0.0029672895159,
+                    0.00035900539822, -0.00002184781161], np.float32)
+    dt_ms, h = 0.5, 5.0
+    steps, warm = max(args.kernel_steps, 20), 5
+    for nx, nz in ((704, 384), (896, 480), (4096, 2048)):
+        ms = (C.c_float * 3)()
+        rc = L.ref_time_step(nx, nz, steps, warm, C.c_float(dt_ms), C.c_float(h), C.c_float(h),
+                             coe.ctypes.data_as(C.POINTER(C.c_float)), ms)
+        if rc != 0:
+            raise RuntimeError(f"ref_time_step {nx}x{nz}: CUDA error {rc}")
+        ref_ms = [m / steps for m in ms]
+        cfg = ertm.Config(nx=nx, ny=1, nz=nz, dx=h, dy=h, dz=h, dt_ms=dt_ms, nt=steps, order=12,
+                          coef_kind=ertm.COEF_REFERENCE12, boundary=ertm.BOUNDARY_SPONGE_CUBIC,
+                          pml=(40, 40, 0, 0, 40, 40), sponge_coef=150.0)
+        vp = np.full((nz, 1, nx), 2500.0, np.float32)
+        vs = (vp / np.sqrt(3)).astype(np.float32)
+        rho = np.full_like(vp, 2200.0)
+        with ertm.Context(cfg) as ctx:
+            ctx.set_model(ertm.MIGRATION_MODEL, vp, vs, rho)
+            shot = ertm.Shot(nx // 2, 0, 45, wavelet=np.ones(8, np.float32) * 1e-3, rx0=40,
+                             nrx=nx - 80, rz=45)
+            ctx.time_kernels(shot, warm)
+            ours = [m / steps for m in ctx.time_kernels(shot, steps)]
+        cells = nx * nz
+        ref_step, our_step = sum(ref_ms), sum(ours)
+        print(json.dumps({
+            "workload": "refstep", "grid": f"{nx}x{nz}", "cells": cells, "steps_timed": steps,
+            "metric": "Gcell-updates/s (2D elastic time step, same GPU)", "unit": UNIT,
+            "reference": {"value": round(cells / (ref_step / 1e3) / 1e9, 3),
+                          "ms_per_step": round(ref_step, 4),
+                          "kernels_ms": {"fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization":
+                                         round(ref_ms[0], 4),
+                                         "adjoint_fwd_vx_viscoelastic": round(ref_ms[1], 4),
+                                         "adjoint_fwd_vz_viscoelastic": round(ref_ms[2], 4)},
+                          "build": "reference 2D kernels, nvcc -O2 sm_100a, tiles 32x16 (inferred)"},
+            "ours": {"value": round(cells / (our_step / 1e3) / 1e9, 3), "ms_per_step": round(our_step, 4),
+                     "kernels_ms": {"k_stress": round(ours[0], 4), "k_velocity": round(ours[1], 4)},
+                     "scheme": "R=6 reference coefficients, cubic sponge 40, P stress + P velocity"},
+            "speedup": round(ref_step / our_step, 2)}), flush=True)
+
+
 def _fmt_case(r):
     out = {}
     for k, v in r.items():
@@ -405,6 +468,8 @@ def main():
         return run_lsrtm(args)
     if args.workload == "lsrtm-op":
         return run_lsrtm_op(args)
+    if args.workload == "refstep":
+        return run_refstep(args)
     import numpy as np
     import torch
     import torch.distributed as dist

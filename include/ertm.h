@@ -244,6 +244,16 @@ int ertm_time_kernels(ertm_ctx *ctx, const ertm_shot *shot, int nsteps, float *m
 /* Number of kernels this context has launched (for launch accounting). */
 int64_t ertm_kernel_launches(const ertm_ctx *ctx);
 
+/* Test hook of the device-error path.  No counterpart in the reference (it
+ * aborts on any CUDA error, 3D_forward_or_back_together.cu:34).  With
+ * plane >= 0 the first CTA of every step-kernel launch does not issue the
+ * staged copy of its z plane `plane` (a copy that never lands), so the bounded
+ * wait of its consumers runs out after `polls` polls (0: the default budget);
+ * the kernel then stops writing, its producer waits (bounded) for the copies it
+ * did issue, and the pass returns ERTM_EDEVICE with the context still usable.
+ * plane = -1 turns the hook off (the default). */
+int ertm_set_wait_fault(ertm_ctx *ctx, int plane, uint32_t polls);
+
 /* ---- modelling without device allocation ------------------------------
  * No counterpart in the reference: an addition of this library.
  *
@@ -251,14 +261,17 @@ int64_t ertm_kernel_launches(const ertm_ctx *ctx);
  * callers that must not allocate GPU memory when they call in (a plugin host
  * whose execute step forbids it, a real-time pipeline whose memory is fixed at
  * start-up, a framework whose own allocator owns the device).  No context is
- * created and nothing is allocated: the caller passes device pointers for vp,
- * vs, rho (nz*ny*nx), shot->wavelet and data_out ([3][nt][nrec]), and the
- * wavefields live in one fixed 64 MiB device array inside the library, held by
- * every GPU that loads it until the process exits.  A grid whose state does
- * not fit returns ERTM_EINVAL with the needed size in errbuf.  The first call
- * on a device looks up that array's address (make it before any stream capture
- * on that device).  Calls share the array: calls that overlap on the GPU race,
- * so serialise them; each call clears the state it uses.  Work is ordered on
+ * created and nothing is allocated: the caller passes pointers to memory of
+ * GPU cfg->device (or managed memory) for vp, vs, rho (nz*ny*nx),
+ * shot->wavelet and data_out ([3][nt][nrec]); memory of another GPU is
+ * refused with ERTM_EINVAL.  The wavefields live in one fixed 64 MiB device
+ * array inside the library, held by every GPU that loads it until the process
+ * exits.  A grid whose state does not fit returns ERTM_EINVAL with the needed
+ * size in errbuf.  The first call on a device looks up that array's address,
+ * and so does the first call after the device's context changed
+ * (cudaDeviceReset); make such a call before any stream capture on that
+ * device.  Calls share the array: calls that overlap on the GPU race, so
+ * serialise them; each call clears the state it uses.  Work is ordered on
  * `cuda_stream` (NULL: the legacy default stream) and is complete on return.
  * errbuf (may be NULL) receives a message on failure. */
 int ertm_forward_together_using_real_model_noalloc(const ertm_config *cfg, const float *vp,

@@ -125,3 +125,74 @@ extern "C" int ref_dem_sources(int nx, int nz, float dt_ms, const float* vp, con
     err |= get(out + 2 * n, dall + 2 * n, 3 * n);
     return err;
 }
+
+// Device time of the reference's own 2D time step on an nx x nz interior
+// (radius-padded, ix-major layout): the stress kernel
+// fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization
+// (viscoelastic_equation.cu:184-325) then the velocity kernels
+// adjoint_fwd_vx_viscoelastic and adjoint_fwd_vz_viscoelastic (:1827-2122),
+// launched with the reference's tiles (32 x 16) and time-level ping-pong, as its
+// driver would.  Inputs are smooth nonzero fields (the timing does not depend on
+// the values); no result is read back.  nx % 32 == 0, nz % 16 == 0.
+// ms[0], ms[1], ms[2]: total CUDA-event time of each kernel over nsteps steps
+// (warm-up steps excluded).  Only bench.py calls it.
+extern "C" int ref_time_step(int nx, int nz, int nsteps, int warmup, float dt_ms, float dx, float dz,
+                             const float* coe7, float* ms)
+{
+    if (nx % 32 || nz % 16 || nsteps < 1) return -1;
+    const size_t n = (size_t)(nx + 2 * radius) * (nz + 2 * radius);
+    Dev D;
+    std::vector<float> h(n);
+    auto smooth = [&](float a, float b) {
+        for (size_t i = 0; i < n; i++) h[i] = a + b * (float)((i * 2654435761u) % 1000u) / 1000.f;
+        return D.put(h.data(), n);
+    };
+    float *vx[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float *vz[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float *txx[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float *tzz[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float *txz[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float *tp[2] = {smooth(0.f, 1e-3f), smooth(0.f, 1e-3f)};
+    float* mem[2][4];
+    for (int t = 0; t < 2; t++)
+        for (int q = 0; q < 4; q++) mem[t][q] = D.put(nullptr, n);
+    float *vp = smooth(2500.f, 500.f), *vs = smooth(1400.f, 300.f), *rho = smooth(2200.f, 100.f);
+    float *mp = smooth(6.25e6f, 1e6f), *msd = smooth(1.96e6f, 4e5f), *att = smooth(0.f, 10.f);
+    float *tao = D.fill(1.f, n), *sp = D.fill(1.f, n), *ss = D.fill(1.f, n);
+    float* coe = D.put(coe7, 7);
+    const float coe_x = dt_ms / 1000.f / dx, coe_z = dt_ms / 1000.f / dz;
+    const dim3 grid(nx / 32, nz / 16), block(32, 16);
+    cudaEvent_t ev[4];
+    for (int q = 0; q < 4; q++) cudaEventCreate(&ev[q]);
+    float tot[3] = {0.f, 0.f, 0.f};
+    for (int s = 0; s < warmup + nsteps; s++) {
+        const int a = s & 1, b = a ^ 1;   // time level a -> b
+        cudaEventRecord(ev[0]);
+        fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization<<<grid, block>>>(
+            tp[b], tp[a], txx[b], txx[a], tzz[b], tzz[a], txz[b], txz[a], vx[a], vz[a], mp, msd, att,
+            dt_ms, coe, coe_x, coe_z, nx, nz, rho, mem[b][0], mem[a][0], mem[b][1], mem[a][1],
+            mem[b][2], mem[a][2], mem[b][3], mem[a][3], vp, vs, tao, sp, ss);
+        cudaEventRecord(ev[1]);
+        adjoint_fwd_vx_viscoelastic<<<grid, block>>>(vx[b], vx[a], txx[b], txz[b], tzz[b], att, dx, dz,
+                                                     dt_ms, coe, coe_x, coe_z, nx, nz, mp, msd, rho,
+                                                     mem[b][0], mem[b][1], mem[b][2], mem[b][3], vp, vs,
+                                                     tao, sp, ss);
+        cudaEventRecord(ev[2]);
+        adjoint_fwd_vz_viscoelastic<<<grid, block>>>(vz[b], vz[a], txx[b], txz[b], tzz[b], att, dx, dz,
+                                                     dt_ms, coe, coe_x, coe_z, nx, nz, mp, msd, rho,
+                                                     mem[b][0], mem[b][1], mem[b][2], mem[b][3], vp, vs,
+                                                     tao, sp, ss);
+        cudaEventRecord(ev[3]);
+        cudaEventSynchronize(ev[3]);
+        if (s >= warmup) {
+            float t;
+            for (int q = 0; q < 3; q++) {
+                cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+                tot[q] += t;
+            }
+        }
+    }
+    for (int q = 0; q < 4; q++) cudaEventDestroy(ev[q]);
+    for (int q = 0; q < 3; q++) ms[q] = tot[q];
+    return (int)cudaGetLastError();
+}

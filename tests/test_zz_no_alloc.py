@@ -62,5 +62,14 @@ def test_noalloc_rejects_oversize_and_host_pointers(ertm):
     with pytest.raises(ertm.ErtmError) as ei:
         ertm.forward_together_using_real_model_noalloc(small, host, host, host, shot2,
                                                        torch.zeros((3, 10, 4), device="cuda"))
-    assert ei.value.code == -1 and "device pointers" in str(ei.value)
+    assert ei.value.code == -1 and "memory of device 0" in str(ei.value)
+    # buffers of device 0 handed to a call configured for device 1: refused before any
+    # work is queued, whether or not a second GPU exists
+    other = ertm.Config(nx=40, ny=1, nz=40, dx=5, dy=5, dz=5, dt_ms=0.5, nt=10, device=1)
+    d = torch.ones(40 * 40, device="cuda:0")
+    shot3 = ertm.Shot(20, 0, 5, wavelet=torch.ones(3, device="cuda:0"), rx0=0, nrx=4, rz=5)
+    with pytest.raises(ertm.ErtmError) as ei:
+        ertm.forward_together_using_real_model_noalloc(other, d, d, d, shot3,
+                                                       torch.zeros((3, 10, 4), device="cuda:0"))
+    assert ei.value.code == -1 and "memory of device 1" in str(ei.value)
     del n
