@@ -100,15 +100,16 @@ __global__ void k_set_int(int* p, int v) { *p = v; }
 // P-wave propagation angle at the cells whose excitation time is the current step
 // (caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM,
 // 2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284), from the Poynting vector of
-// sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
-// cells around the cell, sxz = sum px pz and szz = sum pz^2 (p in float, products
-// and sums in double, as the reference: its Poynting arrays are float and it forms
-// 1.0 * px * pz; a float product would underflow where the receiver wavefield is
-// still only the stencil's numerical precursor), angle = atan(sxz / szz) in degrees from the
-// z axis, written only where szz != 0.  2D grids: the x halo (XH >= 2) and the z
-// halo (R >= 2) hold zeros, so the window needs no bounds checks.  Runs after the
-// velocity kernel of the step and before the step counter advances.
-__global__ void k_angle(Geom g, KArgs a, float* __restrict__ ang)
+// sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the
+// (2 hw + 1)^2 cells around the cell (the reference's 5 x 5 source window, hw = 2,
+// and 9 x 9 receiver window, hw = 4; cells outside the grid count as zero),
+// sxz = sum px pz and szz = sum pz^2 (p in float, products and sums in double, as the
+// reference: its Poynting arrays are float and it forms 1.0 * px * pz; a float product
+// would underflow where the receiver wavefield is still only the stencil's numerical
+// precursor), angle = atan(sxz / szz) in degrees from the z axis, rounded as the
+// reference rounds it, written only where szz != 0.  Runs after the velocity kernel
+// of the step and before the step counter advances.
+__global__ void k_angle(Geom g, KArgs a, float* __restrict__ ang, int hw)
 {
     const int it = *a.it_ptr;
     const float* tp = a.f[F_TP];
@@ -121,15 +122,24 @@ __global__ void k_angle(Geom g, KArgs a, float* __restrict__ ang)
         const long long c = k * g.sz + i;
         if (a.ex_time[c] != it) continue;
         double sxz = 0.0, szz = 0.0;
-        for (int dk = -2; dk <= 2; dk++)
-            for (int di = -2; di <= 2; di++) {
+        for (int dk = -hw; dk <= hw; dk++) {
+            if (k + dk < 0 || k + dk >= g.nz) continue;
+            for (int di = -hw; di <= hw; di++) {
+                if (i + di < 0 || i + di >= g.nx) continue;
                 const long long q = c + dk * g.sz + di;
                 const float t = tp[q];
                 const float px = -t * vxp[q], pz = -t * vzp[q];
                 sxz += (double)px * (double)pz;
                 szz += (double)pz * (double)pz;
             }
-        if (szz != 0.0) ang[c] = (float)(atan(sxz / szz) * (180.0 / 3.14159265358979323846));
+        }
+        if (szz != 0.0) {
+            // float(atan(sxz / szz)) * 180 / pai1 in float, pai1 = 3.1415926f
+            // (elastic_2D_kernel_3.cu:4, :204)
+            float d = (float)atan(sxz / szz);
+            d = d * 180.0f;
+            ang[c] = d / 3.1415926f;
+        }
     }
 }
 
@@ -251,9 +261,9 @@ cudaError_t launch_set_int(int* p, int v, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_angle(const Geom& g, const KArgs& a, float* ang, cudaStream_t s)
+cudaError_t launch_angle(const Geom& g, const KArgs& a, float* ang, int hw, cudaStream_t s)
 {
-    k_angle<<<grid_for((long long)g.nx * g.nz), 256, 0, s>>>(g, a, ang);
+    k_angle<<<grid_for((long long)g.nx * g.nz), 256, 0, s>>>(g, a, ang, hw);
     return cudaGetLastError();
 }
 

@@ -647,7 +647,8 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
     auto one_step = [&]() -> cudaError_t {
         cudaError_t e = launch_stress(R, c->g, a, sm, cpml, psplit, c->stream);
         if (e == cudaSuccess) e = launch_velocity(R, c->g, a, vm, cpml, epi, record, c->stream);
-        if (e == cudaSuccess && ang) e = launch_angle(c->g, a, ang, c->stream);
+        if (e == cudaSuccess && ang)
+            e = launch_angle(c->g, a, ang, mode == MODE_SOURCE ? 2 : 4, c->stream);
         if (e == cudaSuccess) e = launch_advance(c->it_d, dir, c->stream);
         return e;
     };

@@ -172,7 +172,9 @@ cudaError_t launch_advance(int* it_ptr, int delta, cudaStream_t s);
 cudaError_t launch_set_int(int* p, int v, cudaStream_t s);
 cudaError_t launch_sqrt_gather(const Geom& g, const float* amp2, float* out, cudaStream_t s);
 cudaError_t launch_axpy(long long n, const float* x, float* y, cudaStream_t s);   // y += x
-cudaError_t launch_angle(const Geom& g, const KArgs& a, float* ang, cudaStream_t s);   // 2D
+// 2D propagation angle at the cells whose excitation step it is; window (2 hw + 1)^2:
+// hw = 2 in the source pass, 4 in the receiver pass
+cudaError_t launch_angle(const Geom& g, const KArgs& a, float* ang, int hw, cudaStream_t s);
 cudaError_t launch_divcurl(int R, const Geom& g, const KArgs& a, const float* vp, const float* vs,
                            float* p, float* sx, float* sy, float* sz, cudaStream_t s);
 

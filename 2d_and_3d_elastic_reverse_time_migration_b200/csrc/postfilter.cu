@@ -116,28 +116,33 @@ __global__ void k_taper(float* img, long long n, int nx, int left, int right, in
         img[c] *= taper_at((int)(c % nx), nx, left, right, power);
 }
 
-// Angle-dependent amplitude compensation of one cell (open angle d = src - rcv, degrees)
+// Angle-dependent amplitude compensation of one cell (open angle d = src - rcv, degrees),
+// rounded as the reference's kernels round it: the angle in radians is formed in double
+// with the float constant pai1 = 3.1415926f, the cosine or sine is stored as a float,
+// and the division is done in double (elastic_2D_kernel_3.cu:622-761).
 __host__ __device__ inline float compensate(float img, float src, float rcv, int kind)
 {
-    const double rad = 3.14159265358979323846 / 180.0;
+    const double pai1 = (double)3.1415926f;
     const float d = src - rcv;
     switch (kind) {
     case ERTM_COMP_PP: {
-        const float den = (fabsf(d) >= 87.5f && fabsf(d) <= 92.5f) ? 0.1f : (float)cos(d * rad);
-        return img / (den + 0.0001f);
+        const float den = (fabsf(d) >= 87.5f && fabsf(d) <= 92.5f) ? 0.1f
+                                                                   : (float)cos((double)d * pai1 / 180.0);
+        return (float)((double)img / ((double)den + 0.0001));
     }
     case ERTM_COMP_PS: {
-        const float den = fabsf(d) <= 2.5f ? 0.1f : (float)sin(fabs(d * rad));
-        return img / (den + 0.0001f);
+        const float den = fabsf(d) <= 2.5f ? 0.1f : (float)sin(fabs((double)d * pai1 / 180.0));
+        return (float)((double)img / ((double)den + 0.0001));
     }
     case ERTM_COMP_PP_SIGN: {
-        const float den = (float)cos(d * rad);
-        const float v = den <= 0.f ? -img : img;
-        return -v / (fabsf(den) + 0.03f);
+        const float sgn = (float)cos((double)d * pai1 / 180.0);
+        const float v = sgn <= 0.f ? -img : img;
+        return (float)(-(double)v / ((double)fabsf(sgn) + 0.03));
     }
     default: {   // ERTM_COMP_PS_SIGN
-        const float den = (float)fabs(sin(d * rad)) + 0.1f;
-        return -img / den;
+        const float sgn = (float)fabs(sin((double)d * pai1 / 180.0));
+        const float den = (float)((double)fabsf(sgn) + 0.1);
+        return (float)(-(double)img / (double)den);
     }
     }
 }

@@ -37,6 +37,12 @@ sys.path.insert(0, REPO)
 
 METRIC = "Gcell-updates/s (3D elastic RTM shot: source + receiver pass)"
 UNIT = "Gcell/s"
+# compulsory DRAM traffic of the elastic step: 9 fields read and written, 3 model arrays
+COMPULSORY_B = 84
+# DRAM bytes per cell of each source-pass step kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum, one ncu capture per kernel on the 240 x 240 x 190 grid with a
+# 20-cell C-PML: the same slab fractions as the 3D workload)
+TRAFFIC_B_PER_CELL = {"stress": 95.3, "velocity": 105.3}
 
 
 def parse():
@@ -50,6 +56,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-steps", type=int, default=60)
     ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
+    ap.add_argument("--pml", type=int, default=40, help="C-PML width (profiling cases only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
     ap.add_argument("--workload", default="shot",
@@ -67,11 +74,11 @@ def parse():
     return ap.parse_args()
 
 
-def workload(small: bool, grid: str = ""):
+def workload(small: bool, grid: str = "", pml: int = 40):
     synth = importlib.import_module(PKG + ".synthetic")
     if grid:
         nx, ny, nz = (int(v) for v in grid.split(","))
-        return synth.layered_3d(n_interior=(nz, ny, nx), nt=400, smooth_sigma=0)
+        return synth.layered_3d(n_interior=(nz, ny, nx), pml=pml, nt=400, smooth_sigma=0)
     if small:
         return synth.layered_3d(n_interior=(60, 80, 80), pml=20, nt=400, smooth_sigma=4.0)
     return synth.layered_3d()
@@ -120,9 +127,12 @@ class ClockSampler:
 
 class CpuOracle:
     """FP32 OpenMP oracle (a port of the reference's update loops, same scheme) holding
-    the full-grid state; `run(n)` times n source-pass steps with excitation capture."""
+    the full-grid state.  `run(n)` times n source-pass steps with excitation capture;
+    `run_receiver(n)` times n receiver-pass steps (data injection at the surface
+    receivers, P/S split, imaging at the excitation time)."""
 
     def __init__(self, wl):
+        import numpy as np
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import oracle as orc
         self.orc, self.L = orc, orc.lib(32)
@@ -134,9 +144,12 @@ class CpuOracle:
                                           orc._fp(wl.srho))
         if not self.st:
             raise RuntimeError("oracle state allocation failed")
-        self.shot = orc.make_shot(*wl.src, orc.ricker(wl.freq, wl.dt_ms / 1000.0))
+        self.shot = orc.make_shot(*wl.src, orc.ricker(wl.freq, wl.dt_ms / 1000.0), **wl.rec)
         self.ex = orc.ExcitationArrays(wl.shape)
         self.es = self.ex.struct()
+        self.nrec = wl.rec["nrx"] * wl.rec["nry"]
+        self.data = np.zeros((3, 4, self.nrec), np.float32)     # 4 injected samples, cycled
+        self.img = [np.zeros(wl.shape, np.float32) for _ in range(3)]
         self.it = 0
         self.run(1)  # first touch of every page, untimed by callers
 
@@ -152,11 +165,20 @@ class CpuOracle:
             self.it += 1
         return time.perf_counter() - t0
 
+    def run_receiver(self, n: int) -> float:
+        f = self.orc._fp
+        t0 = time.perf_counter()
+        for q in range(n):
+            self.L.orc_state_step(self.st, C.byref(self.shot), self.orc.RECEIVER, q % 4, 4,
+                                  f(self.data), C.byref(self.es), *[f(a) for a in self.img])
+        return time.perf_counter() - t0
+
     def rate_for(self, seconds: float):
+        """Rate over rounds of 2 source-pass and 3 receiver-pass steps (the shot's ratio)."""
         n, el = 0, 0.0
-        while el < seconds or n < 2:
-            el += self.run(1)
-            n += 1
+        while el < seconds or n < 5:
+            el += self.run(2) + self.run_receiver(3)
+            n += 5
         return self.cells * n / el / 1e9, n
 
     def close(self):
@@ -165,28 +187,48 @@ class CpuOracle:
             self.st = None
 
 
+def shot_config(wl, world: int, nrec: int) -> dict:
+    """The `config` of the RTM-shot workload, shared by both bench arms."""
+    nz, ny, nx = wl.shape
+    return {"workload": wl.name, "cells": nx * ny * nz, "nt": wl.nt, "src_steps": 2 * wl.nt // 3,
+            "order": 8, "boundary": f"cpml{wl.pml}", "dt_ms": wl.dt_ms, "receivers": nrec,
+            "parallelism": f"shots x{world}",
+            "l2": "inputs larger than L2 (13 wavefields + model, ~8 GB)"}
+
+
 def run_reference(args):
+    """The reference arm: the FP32 OpenMP oracle, a port of the reference's update loops
+    (the reference has no CPU implementation and its 3D kernels are absent from its
+    tree), on the same RTM-shot workload as this library's arm: the 8th-order scheme
+    with the 40-cell C-PML of the 3D workload, source-pass and receiver-pass steps in
+    the shot's 2 : 3 ratio (2666 : 4000).  One step is a bounded sample of 2 source and
+    3 receiver time steps of the full grid; rank 0 alone runs it."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     synth = importlib.import_module(PKG + ".synthetic")
     wl = (synth.layered_3d(n_interior=(60, 80, 80), pml=20, nt=400, smooth_sigma=0)
           if args.small else synth.layered_3d(smooth_sigma=0))
     cpu = CpuOracle(wl)
-    per_step = 2
+    ns, nr = 2, 3
     for _ in range(args.warmup):
-        cpu.run(per_step)
-    el = sum(cpu.run(per_step) for _ in range(args.steps))
-    v = cpu.cells * per_step * args.steps / el / 1e9
+        cpu.run(ns)
+        cpu.run_receiver(nr)
+    el = 0.0
+    for _ in range(args.steps):
+        el += cpu.run(ns) + cpu.run_receiver(nr)
+    v = cpu.cells * (ns + nr) * args.steps / el / 1e9
     nz, ny, nx = wl.shape
-    sample = (f"{per_step} source-pass time steps (with excitation capture) of the full "
-              f"{nx}x{ny}x{nz} grid per step; FP32 OpenMP port of the update loops")
+    sample = (f"{ns} source-pass and {nr} receiver-pass time steps of the full {nx}x{ny}x{nz} "
+              f"grid per step (the shot's 2:3 ratio); FP32 OpenMP port of the update loops, "
+              f"{cpu.threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(el / args.steps * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded layered model with an ellipsoid)",
-        "config": {"workload": wl.name, "cells": cpu.cells, "order": 8, "boundary": "cpml40"},
+        "data": "synthetic (seeded layered model with an ellipsoid; observed data modelled "
+                "in the true model)",
+        "config": shot_config(wl, args.gpus, cpu.nrec),
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cpu.threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -484,7 +526,7 @@ def main():
 
     ertm = importlib.import_module(PKG)
     synth = importlib.import_module(PKG + ".synthetic")
-    wl = workload(args.small, args.grid)
+    wl = workload(args.small, args.grid, args.pml)
     nz, ny, nx = wl.shape
     cells = nx * ny * nz
     if args.kernels_only:
@@ -556,12 +598,14 @@ def main():
     imgs_h = [torch.empty(wl.shape, dtype=torch.float32, pin_memory=True) for _ in range(3)]
     torch.cuda.synchronize(dev)
     ctx.rtm_shot(shot, data_h, *imgs_h)   # warm the host path
+    reps = max(1, min(args.steps, 2))
     barrier()
     e0.record(stream)
-    ctx.rtm_shot(shot, data_h, *imgs_h)
+    for _ in range(reps):
+        ctx.rtm_shot(shot, data_h, *imgs_h)
     e1.record(stream)
     barrier()
-    ms_e2e = e0.elapsed_time(e1)
+    ms_e2e = e0.elapsed_time(e1) / reps
     t = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -577,20 +621,23 @@ def main():
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    # algorithmic bytes per cell of each source-pass kernel (FP32):
+    # The step's compulsory traffic: 84 B per cell-step (9 fields read and written,
+    # 3 model arrays; FP32).  achieved = 84 B x cells x (src_steps + nt) / timed shot.
+    achieved = COMPULSORY_B * updates / (ms_step / 1e3) / 1e9
+    # Algorithmic bytes per cell of each source-pass kernel (FP32):
     #   stress:   read v(3) sigma(6) tp(1) M, mu(2); write sigma(6) tp(1)          = 76 B
     #   velocity: read sigma(6) tp(1) v(3) vP(3) b(1) |e|^2(1); write v(3) vP(3) = 84 B
     bytes_k = {"stress": 76 * cells, "velocity": 84 * cells}
     t_k = {"stress": ms_stress / ks, "velocity": ms_vel / ks}
-    dom = max(t_k, key=t_k.get)
-    achieved = bytes_k[dom] / (t_k[dom] / 1e3) / 1e9
-    # DRAM bytes per launch from one ncu capture (dram__bytes_read.sum +
-    # dram__bytes_write.sum, 1-pass metrics) of `bench.py --kernels-only
-    # --kernel-steps 4` at the default workload; profiles/traffic_rtm_480x480x380.md
-    traffic = {"stress": 5364710144 + 2976416000, "velocity": 6583469824 + 2632403968}
-    traffic_ok = (not args.grid and not args.small)
+    per_kernel = {k: {"ms": round(t_k[k], 4), "algorithmic_bytes": bytes_k[k],
+                      "gbs": round(bytes_k[k] / (t_k[k] / 1e3) / 1e9, 1),
+                      "frac": round(bytes_k[k] / (t_k[k] / 1e3) / 1e9 / peak, 4)} for k in t_k}
+    # DRAM bytes per launch: the per-cell traffic of one ncu capture of each kernel on
+    # the half-size grid with a proportionally half-width C-PML (same slab fractions),
+    # scaled by the cell count (traffic grows with the cells at fixed slab fractions)
+    traffic_step = sum(TRAFFIC_B_PER_CELL.values()) * cells
+    traffic_ok = (not args.grid and not args.small and args.pml == 40)
     step_ms = (ms_stress + ms_vel) / ks
-    step_gbs = (bytes_k["stress"] + bytes_k["velocity"]) / (step_ms / 1e3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -598,8 +645,9 @@ def main():
             co = CpuOracle(wl)
             rate, n = co.rate_for(args.cpu_seconds)
             cpu = {"value": round(rate, 4), "unit": UNIT, "cores": co.threads, "kind": "port",
-                   "sample": f"{n} source-pass time steps of the full {nx}x{ny}x{nz} grid, "
-                             f"FP32 OpenMP oracle (same scheme), after one untimed step"}
+                   "sample": f"{n} time steps (source and receiver pass, 2:3) of the full "
+                             f"{nx}x{ny}x{nz} grid, FP32 OpenMP oracle (same scheme), after one "
+                             f"untimed step"}
             co.close()
         except Exception as e:  # a missing oracle build must not hide the GPU number
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port",
@@ -612,20 +660,21 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded layered model with an ellipsoid; observed data modelled "
                     "in the true model)",
-            "config": {"workload": wl.name, "cells": cells, "nt": wl.nt, "src_steps": src_steps,
-                       "order": 8, "boundary": "cpml40", "dt_ms": wl.dt_ms,
-                       "receivers": shot.nrec, "parallelism": f"shots x{world}",
-                       "l2": "inputs larger than L2 (13 wavefields + model, ~8 GB)"},
+            "config": shot_config(wl, world, shot.nrec),
             "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": f"k_{dom} (source pass)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "3D elastic step (k_stress + k_velocity), whole RTM shot",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "traffic": traffic[dom] if traffic_ok else None,
-                         "peak_source": peak_src,
-                         "bytes_per_cell": bytes_k[dom] // cells,
-                         "kernel_ms": {k: round(v, 4) for k, v in t_k.items()},
-                         "step_gbs": round(step_gbs, 1), "step_frac": round(step_gbs / peak, 4)},
+                         "traffic": int(traffic_step) if traffic_ok else None,
+                         "traffic_unit": "bytes per step (both kernels), scaled from a "
+                                         "half-size ncu capture",
+                         "peak_source": peak_src, "bytes_per_cell_step": COMPULSORY_B,
+                         "kernels": per_kernel,
+                         "rtm_algorithmic_bytes_per_cell_step": 160,
+                         "rtm_algorithmic_frac": round(160 * cells / (step_ms / 1e3) / 1e9 / peak, 4),
+                         "traffic_bytes_per_cell": TRAFFIC_B_PER_CELL},
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -328,8 +328,8 @@ int ertm_aperture_taper(float *img, int nx, int ny, int nz, int x0, int x1, int 
  * cell the P-wave propagation angle of the source wavefield at the cell's
  * excitation time, and the receiver pass that of the receiver wavefield at the
  * same time: Poynting vector p = -tp (vxp, vzp), angle = atan(sum px pz / sum pz^2)
- * over the 5 x 5 cells around the cell, in degrees from the z axis; a cell whose
- * window sum of pz^2 is zero keeps 0.  Replaces caculate_ex_angle_pp_only_RTM /
+ * over the 5 x 5 (source pass) or 9 x 9 (receiver pass) cells around the cell, in
+ * degrees from the z axis; a cell whose window sum of pz^2 is zero keeps 0.  Replaces caculate_ex_angle_pp_only_RTM /
  * caculate_ex_angle_rp_only_RTM on sum_poynting's vectors
  * (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284, elastic_2D_kernel_2.cu:8-30).
  * One extra kernel per step while on; ERTM_ENOTSUP on 3D grids.  ertm_get_angles

@@ -439,20 +439,29 @@ static long rec_cell(const orc_state *S, const orc_shot *s, int r, int *ok)
 static int image_pp_ps(real ex, real ey, real ez, real px, real py, real pz, real sx, real sy,
                        real sz, real *pp, real *ps);
 
+/* Angle of the window sums, rounded as the reference does: float(atan(sxz / szz))
+ * * 180 / pai1 in float arithmetic, pai1 = 3.1415926f (elastic_2D_kernel_3.cu:4, :204). */
+static float angle_of_sums(double sxz, double szz)
+{
+    float a = (float)atan(sxz / szz);
+    a = a * 180.0f;
+    return a / 3.1415926f;
+}
+
 /* P-wave propagation angle at cell (i, k) of a 2D state (and, when asked, the
- * window's P energy), restating
- * caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM
- * (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284) on the Poynting vector of
- * sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp): over the 5 x 5
- * cells around (i, k) (cells outside the grid count as zero), sxz = sum px pz and
- * szz = sum pz^2, angle = atan(sxz / szz) in degrees from the z axis.  Returns 0
- * and leaves *out alone where szz == 0, as the reference does. */
-static int window_angle(const orc_state *S, int i, int k, float *out, float *energy)
+ * window's P energy), restating caculate_ex_angle_pp_only_RTM (source wavefield,
+ * 5 x 5 window, hw = 2) and caculate_ex_angle_rp_only_RTM (receiver wavefield,
+ * 9 x 9 window, hw = 4) (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284) on the
+ * Poynting vector of sum_poynting (elastic_2D_kernel_2.cu:28-30), p = -tp (vxp, vzp):
+ * over the (2 hw + 1)^2 cells around (i, k) (cells outside the grid count as zero),
+ * sxz = sum px pz and szz = sum pz^2, angle = atan(sxz / szz) in degrees from the
+ * z axis.  Returns 0 and leaves *out alone where szz == 0, as the reference does. */
+static int window_angle(const orc_state *S, int i, int k, int hw, float *out, float *energy)
 {
     const orc_grid *g = &S->g;
     double sxz = 0.0, szz = 0.0, sxx = 0.0;
-    for (int dk = -2; dk <= 2; dk++)
-        for (int di = -2; di <= 2; di++) {
+    for (int dk = -hw; dk <= hw; dk++)
+        for (int di = -hw; di <= hw; di++) {
             int ii = i + di, kk = k + dk;
             if (ii < 0 || ii >= g->nx || kk < 0 || kk >= g->nz) continue;
             long c = AT(S, ii, 0, kk);
@@ -464,12 +473,12 @@ static int window_angle(const orc_state *S, int i, int k, float *out, float *ene
         }
     if (energy) *energy = (float)(sxx + szz);
     if (szz == 0.0) return 0;
-    *out = (float)(atan(sxz / szz) * 180.0 / SU_PI);
+    *out = angle_of_sums(sxz, szz);
     return 1;
 }
 
-static void capture_angles(const orc_state *S, const orc_excitation *ex, int it, float *angle,
-                           float *energy)
+static void capture_angles(const orc_state *S, const orc_excitation *ex, int it, int hw,
+                           float *angle, float *energy)
 {
     const orc_grid *g = &S->g;
     if (!S->two_d || !angle) return;
@@ -477,7 +486,7 @@ static void capture_angles(const orc_state *S, const orc_excitation *ex, int it,
     for (int k = 0; k < g->nz; k++)
         for (int i = 0; i < g->nx; i++) {
             long m = (long)k * g->nx + i;
-            if (ex->time[m] == it) window_angle(S, i, k, &angle[m], energy ? &energy[m] : NULL);
+            if (ex->time[m] == it) window_angle(S, i, k, hw, &angle[m], energy ? &energy[m] : NULL);
         }
 }
 
@@ -549,7 +558,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                         ex->second2[m] = (float)a2;
                     }
                 }
-        capture_angles(S, ex, it, ex->src_angle, ex->src_energy);
+        capture_angles(S, ex, it, 2, ex->src_angle, ex->src_energy);
     }
     if (mode == ORC_MODE_RECEIVER && ex) {
         /* imaging_inner_product_ex / imaging_correlation_ex, restating
@@ -573,7 +582,7 @@ static void state_step(orc_state *S, const orc_shot *s, int mode, int it, int ns
                     real et = ex->etp[m];
                     if (ptp && et != 0) ptp[m] = (float)(S->f[F_TP][c] / et);
                 }
-        capture_angles(S, ex, it, ex->rcv_angle, ex->rcv_energy);
+        capture_angles(S, ex, it, 4, ex->rcv_angle, ex->rcv_energy);
     }
 }
 
@@ -1194,5 +1203,34 @@ int orc_image_given(long n, const float *ex, const float *ez, const float *rpx, 
         pp[c] = (float)a;
         ps[c] = (float)b;
     }
+    return 0;
+}
+
+/* Propagation angle on given 2D arrays (nz x nx, x fastest): the window angle of
+ * window_angle over p = -tp (vxp, vzp), written at the cells whose excitation time
+ * equals `it` (elsewhere `out` is left alone); hw = 2 (source, 5 x 5) or 4
+ * (receiver, 9 x 9).  Pins the angle restatement to the reference's own
+ * caculate_ex_angle_pp_only_RTM / _rp_only_RTM run on the same arrays. */
+int orc_angle_given(int nx, int nz, int hw, int it, const float *tp, const float *vxp,
+                    const float *vzp, const int *ex_time, float *out)
+{
+    if (nx <= 0 || nz <= 0 || hw < 0 || !tp || !vxp || !vzp || !ex_time || !out) return -1;
+    for (int k = 0; k < nz; k++)
+        for (int i = 0; i < nx; i++) {
+            long m = (long)k * nx + i;
+            if (ex_time[m] != it) continue;
+            double sxz = 0.0, szz = 0.0;
+            for (int dk = -hw; dk <= hw; dk++)
+                for (int di = -hw; di <= hw; di++) {
+                    int ii = i + di, kk = k + dk;
+                    if (ii < 0 || ii >= nx || kk < 0 || kk >= nz) continue;
+                    long q = (long)kk * nx + ii;
+                    /* sum_poynting forms p in float (elastic_2D_kernel_2.cu:28-30) */
+                    const float px = -tp[q] * vxp[q], pz = -tp[q] * vzp[q];
+                    sxz += (double)px * (double)pz;
+                    szz += (double)pz * (double)pz;
+                }
+            if (szz != 0.0) out[m] = angle_of_sums(sxz, szz);
+        }
     return 0;
 }

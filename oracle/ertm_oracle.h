@@ -168,6 +168,10 @@ void orc_state_step(void *st, const orc_shot *s, int mode, int it, int nsteps, f
 void orc_state_fields(const void *st, float *out);
 void orc_state_destroy(void *st);
 
+/* Window propagation angle on given 2D arrays (see ertm_oracle.c). */
+int orc_angle_given(int nx, int nz, int hw, int it, const float *tp, const float *vxp,
+                    const float *vzp, const int *ex_time, float *out);
+
 /* Threads used by the OpenMP loops (1 if built without OpenMP). */
 int orc_threads(void);
 /* sizeof(REAL) of the loaded library (8 or 4). */

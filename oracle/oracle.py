@@ -100,6 +100,8 @@ def lib(bits: int = 64) -> C.CDLL:
         L.orc_visco_model.restype = C.c_int
         L.orc_visco_fit.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, P(C.c_double),
                                     P(C.c_double), P(C.c_double)]
+        L.orc_angle_given.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, f, f, f, P(C.c_int), f]
+        L.orc_angle_given.restype = C.c_int
         L.orc_threads.restype = C.c_int
         L.orc_real_size.restype = C.c_int
         _libs[bits] = L
@@ -238,6 +240,21 @@ def run_pass(g: Grid, vp, vs, rho, shot: Shot, mode: int, nsteps: int, data=None
     out.update(data=data, ex=ex, pp=pp, ps=ps, tp=tp)
     if want_fields:
         out["fields"] = {n: fields[i] for i, n in enumerate(FIELD_NAMES)}
+    return out
+
+
+def angle_given(tp, vxp, vzp, ex_time, it: int, hw: int, init: float = 0.0):
+    """Window propagation angle on given 2D (nz, nx) arrays at the cells whose
+    excitation step is `it` (hw 2: the source window, 4: the receiver window);
+    other cells keep `init`."""
+    nz, nx = tp.shape
+    out = np.full((nz, nx), init, np.float32)
+    a = [np.ascontiguousarray(v, np.float32) for v in (tp, vxp, vzp)]
+    t = np.ascontiguousarray(ex_time, np.int32)
+    rc = lib().orc_angle_given(nx, nz, hw, it, *[_fp(v) for v in a],
+                               t.ctypes.data_as(C.POINTER(C.c_int)), _fp(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_angle_given failed: {rc}")
     return out
 
 

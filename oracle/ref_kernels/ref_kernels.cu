@@ -196,3 +196,94 @@ extern "C" int ref_time_step(int nx, int nz, int nsteps, int warmup, float dt_ms
     for (int q = 0; q < 3; q++) ms[q] = tot[q];
     return (int)cudaGetLastError();
 }
+
+// sum_poynting (elastic_2D_kernel_2.cu:8-30) then caculate_ex_angle_pp_only_RTM
+// (hw_mode 0, 5 x 5 window) or caculate_ex_angle_rp_only_RTM (hw_mode 1, 9 x 9)
+// (elastic_2D_kernel_3.cu:132-284) at step `it`.  Inputs radius-padded, ix-major;
+// ex_time as the reference's float array.  `angle` (padded) keeps its input values
+// where the kernel writes nothing.  nx % 32 == 0, nz % 16 == 0.
+extern "C" int ref_angle(int nx, int nz, int hw_mode, int it, const float* tp, const float* vxp,
+                         const float* vzp, const float* ex_time, float* angle)
+{
+    if (nx % 32 || nz % 16) return -1;
+    const size_t n = (size_t)(nx + 2 * radius) * (nz + 2 * radius);
+    Dev D;
+    float *dtp = D.put(tp, n), *dvxp = D.put(vxp, n), *dvzp = D.put(vzp, n);
+    float *zero = D.put(nullptr, n);
+    float *px = D.put(nullptr, n), *pz = D.put(nullptr, n), *sx = D.put(nullptr, n), *sz = D.put(nullptr, n);
+    float *det = D.put(ex_time, n), *dang = D.put(angle, n);
+    const dim3 grid(nx / 32, nz / 16), block(32, 16);
+    sum_poynting<<<grid, block>>>(px, pz, sx, sz, dvxp, dvzp, zero, zero, zero, zero, zero, dtp, nx, nz);
+    if (hw_mode == 0)
+        caculate_ex_angle_pp_only_RTM<<<grid, block>>>(dang, px, pz, det, it, nx, nz);
+    else
+        caculate_ex_angle_rp_only_RTM<<<grid, block>>>(dang, px, pz, det, it, nx, nz);
+    return get(angle, dang, n);
+}
+
+// Angle-dependent compensation of an image, plain ix-major nx x nz arrays, every
+// cell at its excitation step (ex_time = it = 0):
+//   kind 0 imaging_pp_compensate_dependent_angle_2D, kind 1 imaging_ps_... (:622-676);
+//   kind 2 caculate_ex_open_pp_ps + cuda_ex_com_pp_ps_sign(mark 0) +
+//          imaging_pp_compensate_dependent_angle_2D_new;
+//   kind 3 the same with mark 1 and imaging_ps_compensate_dependent_angle_2D_new (:678-761).
+// out: the compensated image; for kinds 0 and 1 also rcv_out = the kernel's
+// rewrite of the receiver angle (the open angle).
+extern "C" int ref_compensate(int nx, int nz, int kind, const float* src, const float* rcv,
+                              const float* img, float* out, float* rcv_out)
+{
+    const size_t n = (size_t)nx * nz;
+    Dev D;
+    float *ds = D.put(src, n), *dr = D.put(rcv, n), *di = D.put(img, n), *dout = D.put(nullptr, n);
+    float *det = D.put(nullptr, n), *open = D.put(nullptr, n), *sgn = D.put(nullptr, n);
+    const dim3 grid((nx + 31) / 32, (nz + 15) / 16), block(32, 16);
+    if (kind == 0)
+        imaging_pp_compensate_dependent_angle_2D<<<grid, block>>>(ds, dr, dout, di, det, nx, nz, nz, 0, 0, 0);
+    else if (kind == 1)
+        imaging_ps_compensate_dependent_angle_2D<<<grid, block>>>(ds, dr, dout, di, det, nx, nz, nz, 0, 0, 0);
+    else {
+        caculate_ex_open_pp_ps<<<grid, block>>>(open, ds, dr, nx, nz, nx, nz, 0, 0, 0, det);
+        cuda_ex_com_pp_ps_sign<<<grid, block>>>(sgn, open, nx, nz, nx, nz, kind == 2 ? 0 : 1);
+        if (kind == 2)
+            imaging_pp_compensate_dependent_angle_2D_new<<<grid, block>>>(open, sgn, dout, di, det, nx, nz,
+                                                                           nz, 0, 0);
+        else
+            imaging_ps_compensate_dependent_angle_2D_new<<<grid, block>>>(open, sgn, dout, di, det, nx, nz,
+                                                                           nz, 0, 0);
+    }
+    int e = get(out, dout, n);
+    if (rcv_out) e |= get(rcv_out, dr, n);
+    return e;
+}
+
+// cuda_bell_smoothz_new (mode 0), cuda_bell_smoothx_new (mode 1) or
+// cuda_bell_smooth_2d (mode 2) (viscoelastic_equation.cu:2528-2604); ix-major nx x nz.
+extern "C" int ref_bell(int nx, int nz, int rbell, int mode, const float* g, float* out)
+{
+    const size_t n = (size_t)nx * nz;
+    Dev D;
+    float *dg = D.put(g, n), *dout = D.put(nullptr, n);
+    const dim3 grid((nx + 31) / 32, (nz + 15) / 16), block(32, 16);
+    if (mode == 0) cuda_bell_smoothz_new<<<grid, block>>>(dg, dout, rbell, nx, nz);
+    else if (mode == 1) cuda_bell_smoothx_new<<<grid, block>>>(dg, dout, rbell, nx, nz);
+    else cuda_bell_smooth_2d<<<grid, block>>>(dg, dout, rbell, nx, nz);
+    return get(out, dout, n);
+}
+
+// cuda_attenuation_truncation (zero_mode 0, :2881-2926) or
+// cauda_zero_and_attenuation_truncation (zero_mode 1, :2928-2988) in place on an
+// ix-major nx x nz array.
+extern "C" int ref_truncation(int nx, int nz, int zero_mode, int offset_left, int offset_right,
+                              int receiver_offset, int offset_attenuation, float* g)
+{
+    const size_t n = (size_t)nx * nz;
+    Dev D;
+    float* dg = D.put(g, n);
+    const dim3 grid((nx + 31) / 32, (nz + 15) / 16), block(32, 16);
+    if (zero_mode == 0)
+        cuda_attenuation_truncation<<<grid, block>>>(dg, nx, nz, offset_left, offset_right, receiver_offset);
+    else
+        cauda_zero_and_attenuation_truncation<<<grid, block>>>(dg, nx, nz, offset_left, offset_right,
+                                                               receiver_offset, offset_attenuation);
+    return get(g, dg, n);
+}

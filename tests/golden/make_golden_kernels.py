@@ -2,11 +2,16 @@
 
 Loads oracle/_ref/libref2d.so — built here from the reference tree by
 oracle/ref_kernels/Makefile (`__graft_entry__.build()` does it when the tree is
-present) — runs four reference kernels on seeded inputs and writes
-tests/golden/ref_kernels_2d.npz (inputs and outputs in the x-fastest [nz][nx]
-layout used by the oracle):
-  fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization (elastic: tao=strain=1)
-  decom_new, imaging_inner_product_ex_2D, cuda_cal_dem_parameter_viscoelastic_media_new
+present) — runs reference kernels on seeded inputs and writes, with inputs and
+outputs in the x-fastest [nz][nx] layout used by the oracle:
+  tests/golden/ref_kernels_2d.npz:
+    fwd_txxzzxzpp_viscoelastic_and_memory_3parameterization (elastic: tao=strain=1)
+    decom_new, imaging_inner_product_ex_2D, cuda_cal_dem_parameter_viscoelastic_media_new
+  tests/golden/ref_kernels_2d_post.npz (the post-imaging products):
+    sum_poynting + caculate_ex_angle_pp_only_RTM / caculate_ex_angle_rp_only_RTM,
+    imaging_pp/ps_compensate_dependent_angle_2D and their _new (sign) variants,
+    cuda_bell_smoothz_new / cuda_bell_smoothx_new / cuda_bell_smooth_2d,
+    cuda_attenuation_truncation, cauda_zero_and_attenuation_truncation
 
     python tests/golden/make_golden_kernels.py
 """
@@ -96,5 +101,78 @@ def main():
     print("wrote ref_kernels_2d.npz")
 
 
+def ix_major(a):
+    """[nz][nx] -> the reference's plain ix-major layout"""
+    return np.ascontiguousarray(a.T)
+
+
+def from_ix(a, nx, nz):
+    return np.ascontiguousarray(a.reshape(nx, nz).T)
+
+
+def main_post():
+    L = C.CDLL(LIB)
+    rng = np.random.default_rng(20261204)
+    out = {}
+    # propagation angles: P stress and P velocity fields, excitation step 0..3 per cell
+    nx, nz, it = 32, 32, 1
+    tp = rng.standard_normal((nz, nx)).astype(np.float32)
+    vxp = rng.standard_normal((nz, nx)).astype(np.float32)
+    vzp = rng.standard_normal((nz, nx)).astype(np.float32)
+    tp[:12, :12] = 0.0                   # windows with no P energy keep their input value
+    et = rng.integers(0, 4, (nz, nx)).astype(np.int32)
+    out.update(ang_tp=tp, ang_vxp=vxp, ang_vzp=vzp, ang_time=et,
+               ang_meta=np.array([nx, nz, it], np.int64))
+    for mode, name in ((0, "ang_pp"), (1, "ang_rp")):
+        a = np.full(((nx + 2 * RAD) * (nz + 2 * RAD)), -999.0, np.float32)
+        rc = L.ref_angle(nx, nz, mode, it, fp(to_ref(tp)), fp(to_ref(vxp)), fp(to_ref(vzp)),
+                         fp(to_ref(et.astype(np.float32))), fp(a))
+        assert rc == 0, rc
+        out[name] = from_ref(a)
+    # angle-dependent compensation, the four variants
+    nx, nz = 40, 30
+    img = rng.standard_normal((nz, nx)).astype(np.float32)
+    src = rng.uniform(-80, 80, (nz, nx)).astype(np.float32)
+    rcv = rng.uniform(-80, 80, (nz, nx)).astype(np.float32)
+    src[0, :10], rcv[0, :10] = 90.0, 0.0           # the clamped band near 90 degrees
+    src[1, :10], rcv[1, :10] = 1.0, 0.0            # small open angles (PS clamp)
+    src[2, :10], rcv[2, :10] = 30.0, 120.0         # cos < 0 (the sign variant)
+    out.update(comp_img=img, comp_src=src, comp_rcv=rcv)
+    for kind in range(4):
+        o = np.zeros(nx * nz, np.float32)
+        r2 = np.zeros(nx * nz, np.float32)
+        rc = L.ref_compensate(nx, nz, kind, fp(ix_major(src)), fp(ix_major(rcv)), fp(ix_major(img)),
+                              fp(o), fp(r2))
+        assert rc == 0, rc
+        out[f"comp_out{kind}"] = from_ix(o, nx, nz)
+        if kind < 2:
+            out[f"comp_open{kind}"] = from_ix(r2, nx, nz)
+    # truncated Gaussian smoothing
+    nx, nz = 48, 40
+    g = rng.standard_normal((nz, nx)).astype(np.float32)
+    out["bell_in"] = g
+    for mode, rb, name in ((0, 5, "bell_z5"), (1, 5, "bell_x5"), (2, 3, "bell_2d3")):
+        o = np.zeros(nx * nz, np.float32)
+        rc = L.ref_bell(nx, nz, rb, mode, fp(ix_major(g)), fp(o))
+        assert rc == 0, rc
+        out[name] = from_ix(o, nx, nz)
+    # edge tapers and aperture mutes of a gradient
+    nx, nz = 96, 20
+    g = rng.standard_normal((nz, nx)).astype(np.float32)
+    out["trunc_in"] = g
+    cases = {"trunc_a": (0, 30, 24, 10, 0), "trunc_b": (1, 40, 50, 20, 4), "trunc_c": (1, 30, 5, 8, 4)}
+    for name, (zm, ol, orr, ro, oa) in cases.items():
+        a = ix_major(g).copy()
+        rc = L.ref_truncation(nx, nz, zm, ol, orr, ro, oa, fp(a))
+        assert rc == 0, rc
+        out[name] = from_ix(a, nx, nz)
+        out[name + "_args"] = np.array([zm, ol, orr, ro, oa], np.int64)
+    np.savez_compressed(os.path.join(HERE, "ref_kernels_2d_post.npz"), **out)
+    print("wrote ref_kernels_2d_post.npz")
+
+
 if __name__ == "__main__":
-    main()
+    import sys as _sys
+    if "--post" not in _sys.argv:
+        main()
+    main_post()

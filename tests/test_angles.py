@@ -2,10 +2,11 @@
 angle-domain common-image gathers (2D_elastic_RTM/elastic_2D_kernel_3.cu:132-284,
 489-511, 622-761; Poynting vectors of elastic_2D_kernel_2.cu:8-30).
 
-The oracle's angle capture is pinned twice on the CPU: against the direction of
-the direct P wave of a point source in a homogeneous medium (a known answer), and
-against a numpy restatement of the 5 x 5 window applied to the oracle's own
-wavefield at the step where a cell's excitation time is set.  The GPU path is
+The oracle's angle capture is pinned on the CPU against the direction of the
+direct P wave of a point source in a homogeneous medium (a known answer), against
+a numpy restatement of the 5 x 5 source window applied to the oracle's own
+wavefield at the step where a cell's excitation time is set, and (in
+test_oracle_ref_post.py) against the reference's own angle kernels.  The GPU path is
 then compared with the oracle on the parity case of the imaging tests."""
 import numpy as np
 import pytest
@@ -41,17 +42,21 @@ def test_oracle_source_angle_is_the_direct_wave_direction(orc):
     assert err.max() < 4.0 and np.percentile(err, 90) < 2.0, (err.max(), np.percentile(err, 90))
 
 
-def _window_angle(f, i, k):
+def _window_angle(f, i, k, hw=2):
+    """The reference's window angle (5 x 5 source window, hw = 2), rounded as it rounds:
+    float(atan(sxz / szz)) * 180 / 3.1415926f in float."""
     nz, nx = f["tp"].shape[0], f["tp"].shape[2]
     sxz = szz = 0.0
-    for kk in range(k - 2, k + 3):
-        for ii in range(i - 2, i + 3):
+    for kk in range(k - hw, k + hw + 1):
+        for ii in range(i - hw, i + hw + 1):
             if 0 <= ii < nx and 0 <= kk < nz:
                 tp = float(f["tp"][kk, 0, ii])
                 px, pz = -tp * float(f["vxp"][kk, 0, ii]), -tp * float(f["vzp"][kk, 0, ii])
                 sxz += px * pz
                 szz += pz * pz
-    return None if szz == 0 else np.degrees(np.arctan(sxz / szz))
+    if szz == 0:
+        return None
+    return float(np.float32(np.arctan(sxz / szz)) * np.float32(180.0) / np.float32(3.1415926))
 
 
 @pytest.mark.parametrize("nsteps", [90, 130])
@@ -207,8 +212,8 @@ def test_angle_products_on_the_device_match_the_host(ertm):
 
 def test_oracle_receiver_angle_is_the_window_angle_at_the_excitation_step(orc):
     """The receiver pass stepped one step at a time: at each step, the cells whose
-    excitation time it is get the window angle of the receiver wavefield of that
-    step, and the window energy the oracle reports."""
+    excitation time it is get the 9 x 9 window angle of the receiver wavefield of
+    that step (caculate_ex_angle_rp_only_RTM, elastic_2D_kernel_3.cu:209-284)."""
     import ctypes as C
     n, nt, nsrc = 60, 160, 110
     g, (vp, vs, rho), shot = _homogeneous(orc, n, (30, 20))
@@ -231,7 +236,7 @@ def test_oracle_receiver_angle_is_the_window_angle_at_the_excitation_step(orc):
             L.orc_state_fields(st, orc._fp(F))
             f = {"tp": F[9], "vxp": F[10], "vzp": F[12]}
             for k, i in cells[:: max(1, len(cells) // 5)]:
-                a = _window_angle(f, i, k)
+                a = _window_angle(f, i, k, hw=4)      # the receiver kernel's 9 x 9 window
                 if a is None:
                     continue
                 assert abs(ex.rcv_angle[k, 0, i] - a) < 1e-4, (it, k, i)

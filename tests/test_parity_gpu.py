@@ -114,7 +114,8 @@ def test_divcurl(ertm, orc, case):
 
 
 def test_wavefields_after_1000_steps(ertm, orc):
-    """Larger 3D grid so the wavefield is still inside after 1000 steps."""
+    """Larger 3D grid so the wavefield is still inside after 1000 steps; a flat
+    relative L2 bound of 1e-5 on all nine wavefields."""
     shape, pml = (72, 76, 80), (10,) * 6
     vp, vs, rho = model(shape, seed=11, vmin=1800.0, vmax=2400.0)
     nz, ny, nx = shape
@@ -133,10 +134,11 @@ def test_wavefields_after_1000_steps(ertm, orc):
     ctx.propagate(ertm.TRUE_MODEL, ertm.Shot(*src, wavelet=w), 1000)
     report = {}
     for name in FIELDS3:
-        e_gpu, e_32 = rel(ctx.get_wavefield(name), ref[name]), rel(r32[name], ref[name])
-        report[name] = (e_gpu, e_32)
-        assert e_gpu <= max(1e-5, 3 * e_32), (name, e_gpu, e_32)
+        report[name] = (rel(ctx.get_wavefield(name), ref[name]), rel(r32[name], ref[name]))
     print("1000-step relative L2 (gpu, fp32 oracle):", report)
+    # the bound of the specification: relative L2 <= 1e-5 on every wavefield after 1000 steps
+    bad = {k: v for k, v in report.items() if not v[0] <= 1e-5}
+    assert not bad, bad
 
 
 def test_call_order_and_argument_errors(ertm, orc):
