@@ -104,6 +104,8 @@ SIGNATURES = {
     "ertm_set_wait_fault": (C.c_int, [_P, C.c_int, C.c_uint32]),
     "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
+    "ertm_born_forward_shots": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, _P, _P, _P, _P]),
+    "ertm_born_adjoint_shots": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, _P, _P, _P, _P]),
     "ertm_write_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
     "ertm_read_volume_xyz": (C.c_int, [C.c_char_p, _P] + [C.c_int] * 9),
     "ertm_laplace_filter": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
@@ -271,7 +273,8 @@ def _pass_steps(cfg, name: str) -> int:
     src = cfg.src_steps or (2 * cfg.nt) // 3
     return {"forward_together_using_real_model": cfg.nt, "forward_together_using_smoothed_model": src,
             "backward_together_using_smoothed_model": cfg.nt, "rtm_shot": src + cfg.nt,
-            "born_forward": 2 * cfg.nt, "born_adjoint": 3 * cfg.nt}.get(name, 0)
+            "born_forward": 2 * cfg.nt, "born_adjoint": 3 * cfg.nt,
+            "born_forward_shots": 2 * cfg.nt, "born_adjoint_shots": 3 * cfg.nt}.get(name, 0)
 
 
 def _logged(fn):
@@ -291,6 +294,8 @@ def _logged(fn):
         out = fn(self, *a, **k)
         dt = time.perf_counter() - t0
         steps = _pass_steps(self.cfg, fn.__name__)
+        if fn.__name__.endswith("_shots"):
+            steps *= len(a[0])          # every shot of the call
         rec = {"event": "pass", "call": fn.__name__, "cells": self.ncell, "cell_steps": self.ncell * steps,
                "seconds": round(dt, 6), "gcell_s": round(self.ncell * steps / dt / 1e9, 4) if dt > 0 else None}
         with open(self._log, "a") as f:
@@ -486,6 +491,44 @@ class Context:
         s = shot.struct()
         self._ck(self._L.ertm_born_adjoint(self._h, C.byref(s), _ptr(r, 3 * self.cfg.nt * shot.nrec),
                                            *[_ptr(o, n, True) for o in outs]))
+        return tuple(outs)
+
+    def _shot_array(self, shots):
+        arr = (_Shot * len(shots))()
+        keep = []
+        for i, sh in enumerate(shots):
+            st = sh.struct()
+            keep.append(st)
+            arr[i] = st
+        return arr, keep
+
+    @_logged
+    def born_forward_shots(self, shots, r_vp, r_vs, r_rho, out=None):
+        """Linearised data of every shot, (nshots, 3, nt, nrec): the shots share each step's
+        kernel launches (ertm_born_forward_shots)."""
+        n, ns = self.ncell, len(shots)
+        nrec = shots[0].nrec
+        if out is None:
+            out = np.zeros((ns, 3, self.cfg.nt, nrec), np.float32)
+        args = [a if _is_torch(a) else np.ascontiguousarray(a, np.float32) for a in (r_vp, r_vs, r_rho)]
+        arr, keep = self._shot_array(shots)
+        self._ck(self._L.ertm_born_forward_shots(self._h, arr, ns, *[_ptr(a, n) for a in args],
+                                                 _ptr(out, ns * 3 * self.cfg.nt * nrec, True)))
+        del keep
+        return out
+
+    @_logged
+    def born_adjoint_shots(self, shots, residual, g_vp=None, g_vs=None, g_rho=None):
+        """Gradient summed over the shots for residuals (nshots, 3, nt, nrec)
+        (ertm_born_adjoint_shots): (g_vp, g_vs, g_rho)."""
+        n, ns = self.ncell, len(shots)
+        outs = [self._vol(o) for o in (g_vp, g_vs, g_rho)]
+        r = residual if _is_torch(residual) else np.ascontiguousarray(residual, np.float32)
+        arr, keep = self._shot_array(shots)
+        self._ck(self._L.ertm_born_adjoint_shots(self._h, arr, ns,
+                                                 _ptr(r, ns * 3 * self.cfg.nt * shots[0].nrec),
+                                                 *[_ptr(o, n, True) for o in outs]))
+        del keep
         return tuple(outs)
 
     @property

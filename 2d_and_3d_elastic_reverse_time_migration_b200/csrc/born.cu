@@ -73,14 +73,16 @@ __device__ __forceinline__ float dmz(const float* __restrict__ f, long long c, c
     return s;
 }
 
-// products of neighbours for the transposed stencils
-struct Prod2 {   // f(c) = p(c) * q(c) * w(c)
+// products of neighbours for the transposed stencils: f(c) = p(c - zo) q(c - zo) w(c),
+// p and q shared by the shots of a launch, w the shot's own volume (offset zo)
+struct Prod2 {
     const float* p;
     const float* q;
     const float* w;
+    long long zo;
     __device__ __forceinline__ float operator()(long long c) const
     {
-        return __ldg(p + c) * __ldg(q + c) * w[c];
+        return __ldg(p + (c - zo)) * __ldg(q + (c - zo)) * w[c];
     }
 };
 template <int R, typename F>
@@ -118,23 +120,32 @@ __device__ __forceinline__ float tdmz(F f, long long c, const BornArgs& a)
     return s;
 }
 
-__device__ __forceinline__ bool cell_of(const BornArgs& a, int& i, int& k, long long& c)
+// cell (i, k) of the launch's shot blockIdx.z: c indexes the shared volumes,
+// c + zo (zo = shot * ss) the shot's own volumes
+__device__ __forceinline__ bool cell_of(const BornArgs& a, int& i, int& k, long long& c, long long& zo)
 {
     i = blockIdx.x * blockDim.x + threadIdx.x;
     k = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= a.nx || k >= a.nz) return false;
     c = (long long)(k + a.R) * a.px + i + BXH;
+    zo = (long long)blockIdx.z * a.ss;
     return true;
 }
 
+// the shot's parameters: sx, sz, rx0, nrx, drx, rz
+__device__ __forceinline__ int shot_par(const BornArgs& a, int q) { return __ldg(a.shot_tab + blockIdx.z * 8 + q); }
+
 __device__ __forceinline__ int recv_of(const BornArgs& a, int i, int k)
 {
-    if (k != a.rz) return -1;
-    int d = i - a.rx0;
-    if (d < 0 || d % a.drx) return -1;
-    d /= a.drx;
-    return d < a.nrx ? d : -1;
+    if (k != shot_par(a, 5)) return -1;
+    int d = i - shot_par(a, 2);
+    const int drx = shot_par(a, 4);
+    if (d < 0 || d % drx) return -1;
+    d /= drx;
+    return d < shot_par(a, 3) ? d : -1;
 }
+
+__device__ __forceinline__ float* shot_traces(const BornArgs& a) { return a.traces + blockIdx.z * a.tstride; }
 
 __device__ __forceinline__ void iso(float m, float u, float exx, float ezz, float exz, float* o)
 {
@@ -149,15 +160,18 @@ template <int R, bool BORN, int NM>
 __global__ void k_born_stress(BornArgs a, int it)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
+    const long long cz = c + zo;
     const float dt = a.dt;
     const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
-    const float e0xx = dpx<R>(a.v0x, c, a), e0zz = dmz<R>(a.v0z, c, a);
-    const float e0xz = dpz<R>(a.v0x, c, a) + dmx<R>(a.v0z, c, a);
-    float o[3] = {a.s0xx[c], a.s0zz[c], a.s0xz[c]};
-    if (it >= 0 && it < a.nw && i == a.ssx && k == a.ssz) {   // explosive source into the background
-        const float w = __ldg(a.wavelet + it);
+    const float *v0x = a.v0x + zo, *v0z = a.v0z + zo;
+    const float e0xx = dpx<R>(v0x, c, a), e0zz = dmz<R>(v0z, c, a);
+    const float e0xz = dpz<R>(v0x, c, a) + dmx<R>(v0z, c, a);
+    float o[3] = {a.s0xx[cz], a.s0zz[cz], a.s0xz[cz]};
+    if (it >= 0 && it < a.nw && i == shot_par(a, 0) && k == shot_par(a, 1)) {
+        // explosive source into the background
+        const float w = __ldg(a.wavelet + (long long)blockIdx.z * a.wstride + it);
         o[0] += w;
         o[1] += w;
     }
@@ -171,15 +185,16 @@ __global__ void k_born_stress(BornArgs a, int it)
 #pragma unroll
         for (int l = 0; l < NM; l++) {
             float* r = a.r0[q * 3 + l];
-            const float v = a.ra[l] * r[c] + a.rb[l] * F0[q];
-            r[c] = v;
+            const float v = a.ra[l] * r[cz] + a.rb[l] * F0[q];
+            r[cz] = v;
             sum += v;
         }
-        s0[q][c] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
+        s0[q][cz] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
     }
     if (BORN) {
-        const float exx = dpx<R>(a.vx, c, a), ezz = dmz<R>(a.vz, c, a);
-        const float exz = dpz<R>(a.vx, c, a) + dmx<R>(a.vz, c, a);
+        const float *vx = a.vx + zo, *vz = a.vz + zo;
+        const float exx = dpx<R>(vx, c, a), ezz = dmz<R>(vz, c, a);
+        const float exz = dpz<R>(vx, c, a) + dmx<R>(vz, c, a);
         const float dpi = a.dM[c], dmu = a.dU[c];
         float E[3], dE[3], F[3], dF[3];
         iso(pi * a.kp, mu * a.ks, exx, ezz, exz, E);
@@ -196,11 +211,11 @@ __global__ void k_born_stress(BornArgs a, int it)
 #pragma unroll
             for (int l = 0; l < NM; l++) {
                 float* r = a.r[q * 3 + l];
-                const float v = a.ra[l] * r[c] + a.rb[l] * (F[q] + dF[q]);
-                r[c] = v;
+                const float v = a.ra[l] * r[cz] + a.rb[l] * (F[q] + dF[q]);
+                r[cz] = v;
                 sum += v;
             }
-            sc[q][c] = g1 * (g2 * sc[q][c] + dt * (E[q] + dE[q] + sum));
+            sc[q][cz] = g1 * (g2 * sc[q][cz] + dt * (E[q] + dE[q] + sum));
         }
     }
 }
@@ -209,33 +224,34 @@ template <int R, bool BORN, bool KEEP>
 __global__ void k_born_velocity(BornArgs a, int it)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
+    const long long cz = c + zo;
     const float dt = a.dt;
     const float g1 = a.g1[c], g2 = a.g2[c], b = a.B[c];
-    const float a0x = b * (dmx<R>(a.s0xx, c, a) + dmz<R>(a.s0xz, c, a));
-    const float a0z = b * (dpx<R>(a.s0xz, c, a) + dpz<R>(a.s0zz, c, a));
-    const float ov0x = a.v0x[c], ov0z = a.v0z[c];
+    const float a0x = b * (dmx<R>(a.s0xx + zo, c, a) + dmz<R>(a.s0xz + zo, c, a));
+    const float a0z = b * (dpx<R>(a.s0xz + zo, c, a) + dpz<R>(a.s0zz + zo, c, a));
+    const float ov0x = a.v0x[cz], ov0z = a.v0z[cz];
     if (KEEP) {   // background history for the adjoint: v0 at the start of the step, a0
-        a.kv0x[c] = ov0x;
-        a.kv0z[c] = ov0z;
-        a.ka0x[c] = a0x;
-        a.ka0z[c] = a0z;
+        a.kv0x[cz] = ov0x;
+        a.kv0z[cz] = ov0z;
+        a.ka0x[cz] = a0x;
+        a.ka0z[cz] = a0z;
     }
-    a.v0x[c] = g1 * (g2 * ov0x + dt * a0x);
-    a.v0z[c] = g1 * (g2 * ov0z + dt * a0z);
+    a.v0x[cz] = g1 * (g2 * ov0x + dt * a0x);
+    a.v0z[cz] = g1 * (g2 * ov0z + dt * a0z);
     if (BORN) {
-        const float ax = b * (dmx<R>(a.sxx, c, a) + dmz<R>(a.sxz, c, a));
-        const float az = b * (dpx<R>(a.sxz, c, a) + dpz<R>(a.szz, c, a));
+        const float ax = b * (dmx<R>(a.sxx + zo, c, a) + dmz<R>(a.sxz + zo, c, a));
+        const float az = b * (dpx<R>(a.sxz + zo, c, a) + dpz<R>(a.szz + zo, c, a));
         const float r = a.rr[c];
-        const float nvx = g1 * (g2 * a.vx[c] + dt * (ax - r * a0x));
-        const float nvz = g1 * (g2 * a.vz[c] + dt * (az - r * a0z));
-        a.vx[c] = nvx;
-        a.vz[c] = nvz;
+        const float nvx = g1 * (g2 * a.vx[cz] + dt * (ax - r * a0x));
+        const float nvz = g1 * (g2 * a.vz[cz] + dt * (az - r * a0z));
+        a.vx[cz] = nvx;
+        a.vz[cz] = nvz;
         const int rec = a.traces ? recv_of(a, i, k) : -1;
         if (rec >= 0) {
             const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
-            float* d = a.traces + (long long)it * nrec + rec;
+            float* d = shot_traces(a) + (long long)it * nrec + rec;
             d[0] = nvx;
             d[cs] = 0.f;
             d[2 * cs] = nvz;
@@ -244,15 +260,19 @@ __global__ void k_born_velocity(BornArgs a, int it)
 }
 
 // ---- adjoint ---------------------------------------------------------------
+// residual sample `it` of every shot's receivers into its velocity adjoint
+// (grid: receivers x, shots y)
 __global__ void k_adj_inject(BornArgs a, int it)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nrx) return;
-    const int i = a.rx0 + r * a.drx;
-    if (i < 0 || i >= a.nx || a.rz < 0 || a.rz >= a.nz) return;
-    const long long c = (long long)(a.rz + a.R) * a.px + i + BXH;
+    const int sh = blockIdx.y;
+    const int* t = a.shot_tab + sh * 8;
+    if (r >= t[3]) return;
+    const int i = t[2] + r * t[4], rz = t[5];
+    if (i < 0 || i >= a.nx || rz < 0 || rz >= a.nz) return;
+    const long long c = (long long)(rz + a.R) * a.px + i + BXH + (long long)sh * a.ss;
     const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
-    const float* d = a.traces + (long long)it * nrec + r;
+    const float* d = a.traces + sh * a.tstride + (long long)it * nrec + r;
     a.ax[c] += d[0];
     a.az[c] += d[2 * cs];
 }
@@ -263,16 +283,18 @@ template <int R>
 __global__ void k_adj_vel(BornArgs a)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
+    const long long cz = c + zo;
     const float dt = a.dt;
     const float g1 = a.g1[c];
     // rho gradient: -dt g1 (vx^ a0x + vz^ a0z)
-    a.gR[c] += -dt * (g1 * a.ax[c] * __ldg(a.ha0x + c) + g1 * a.az[c] * __ldg(a.ha0z + c));
-    const Prod2 tx{a.B, a.g1, a.ax}, tz{a.B, a.g1, a.az};
-    a.hxx[c] = a.hxx[c] - dt * tdpx<R>(tx, c, a);
-    a.hxz[c] = a.hxz[c] - dt * (tdpz<R>(tx, c, a) + tdmx<R>(tz, c, a));
-    a.hzz[c] = a.hzz[c] - dt * tdmz<R>(tz, c, a);
+    a.gR[cz] += -dt * (g1 * a.ax[cz] * __ldg(a.ha0x + cz) + g1 * a.az[cz] * __ldg(a.ha0z + cz));
+    // the shot's adjoint velocity through per-cell products B g1 a^ (shared B, g1)
+    const Prod2 tx{a.B, a.g1, a.ax, zo}, tz{a.B, a.g1, a.az, zo};
+    a.hxx[cz] = a.hxx[cz] - dt * tdpx<R>(tx, cz, a);
+    a.hxz[cz] = a.hxz[cz] - dt * (tdpz<R>(tx, cz, a) + tdmx<R>(tz, cz, a));
+    a.hzz[cz] = a.hzz[cz] - dt * tdmz<R>(tz, cz, a);
 }
 
 // stress and memory-variable update^T of one cell: Q = g1 h is the adjoint of
@@ -284,36 +306,37 @@ template <int R, int NM>
 __global__ void k_adj_mem(BornArgs a)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
+    const long long cz = c + zo;
     const float dt = a.dt;
     const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
-    const float Q[3] = {g1 * a.hxx[c], g1 * a.hzz[c], g1 * a.hxz[c]};
+    const float Q[3] = {g1 * a.hxx[cz], g1 * a.hzz[cz], g1 * a.hxz[cz]};
     float P[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < 3; q++)
 #pragma unroll
         for (int l = 0; l < NM; l++) {
             float* lr = a.lr[q * 3 + l];
-            const float lam = lr[c] + dt * Q[q];
+            const float lam = lr[cz] + dt * Q[q];
             P[q] += a.rb[l] * lam;
-            lr[c] = a.ra[l] * lam;
+            lr[cz] = a.ra[l] * lam;
         }
-    const float e0xx = dpx<R>(a.hv0x, c, a), e0zz = dmz<R>(a.hv0z, c, a);
-    const float e0xz = dpz<R>(a.hv0x, c, a) + dmx<R>(a.hv0z, c, a);
+    const float e0xx = dpx<R>(a.hv0x + zo, c, a), e0zz = dmz<R>(a.hv0z + zo, c, a);
+    const float e0xz = dpz<R>(a.hv0x + zo, c, a) + dmx<R>(a.hv0z + zo, c, a);
     const float tq0 = dt * Q[0], tq1 = dt * Q[1], tq2 = dt * Q[2];
-    a.gM[c] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
-    a.gU[c] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
-               a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
+    a.gM[cz] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
+    a.gU[cz] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
+                a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
     float E[3], F[3] = {0.f, 0.f, 0.f};
     iso(pi * a.kp, mu * a.ks, tq0, tq1, tq2, E);
     if (NM) iso(pi * a.tp, mu * a.ts, P[0], P[1], P[2], F);
-    a.Sxx[c] = E[0] + F[0];
-    a.Szz[c] = E[1] + F[1];
-    a.Sxz[c] = E[2] + F[2];
-    a.hxx[c] = g2 * Q[0];
-    a.hzz[c] = g2 * Q[1];
-    a.hxz[c] = g2 * Q[2];
+    a.Sxx[cz] = E[0] + F[0];
+    a.Szz[cz] = E[1] + F[1];
+    a.Sxz[cz] = E[2] + F[2];
+    a.hxx[cz] = g2 * Q[0];
+    a.hzz[cz] = g2 * Q[1];
+    a.hxz[cz] = g2 * Q[2];
 }
 
 struct Load {
@@ -327,36 +350,46 @@ template <int R>
 __global__ void k_adj_str(BornArgs a, int it_next)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
+    const long long cz = c + zo;
     const float g12 = a.g2[c] * a.g1[c];
     const Load sxx{a.Sxx}, szz{a.Szz}, sxz{a.Sxz};
-    float nx = g12 * a.ax[c] - (tdmx<R>(sxx, c, a) + tdmz<R>(sxz, c, a));
-    float nz = g12 * a.az[c] - (tdpz<R>(szz, c, a) + tdpx<R>(sxz, c, a));
+    float nx = g12 * a.ax[cz] - (tdmx<R>(sxx, cz, a) + tdmz<R>(sxz, cz, a));
+    float nz = g12 * a.az[cz] - (tdpz<R>(szz, cz, a) + tdpx<R>(sxz, cz, a));
     if (it_next >= 0) {
         const int rec = recv_of(a, i, k);
         if (rec >= 0) {
             const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
-            const float* d = a.traces + (long long)it_next * nrec + rec;
+            const float* d = shot_traces(a) + (long long)it_next * nrec + rec;
             nx += d[0];
             nz += d[2 * cs];
         }
     }
-    a.ax[c] = nx;
-    a.az[c] = nz;
+    a.ax[cz] = nx;
+    a.az[cz] = nz;
 }
 
-// gradients w.r.t. (r_vp, r_vs, r_rho) on the contiguous nz x nx grid
-__global__ void k_born_final(BornArgs a, float* gvp, float* gvs, float* grho)
+// gradients w.r.t. (r_vp, r_vs, r_rho) on the contiguous nz x nx grid, summed over
+// the launch's shots (in shot order) and added to the outputs when `accumulate`
+__global__ void k_born_final(BornArgs a, float* gvp, float* gvs, float* grho, int accumulate)
 {
     int i, k;
-    long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long c, zo;
+    if (!cell_of(a, i, k, c, zo)) return;
     const long long m = (long long)k * a.nx + i;
-    const float gp = a.gM[c], gu = a.gU[c];
-    gvp[m] = 2.f * a.M[c] * gp;
-    gvs[m] = 2.f * a.U[c] * gu;
-    grho[m] = a.M[c] * gp + a.U[c] * gu + a.gR[c];
+    float gp = 0.f, gu = 0.f, gr = 0.f;
+    for (int sh = 0; sh < a.nshot; sh++) {
+        const long long q = c + sh * a.ss;
+        gp += a.gM[q];
+        gu += a.gU[q];
+        gr += a.gR[q];
+    }
+    const float ovp = accumulate ? gvp[m] : 0.f, ovs = accumulate ? gvs[m] : 0.f;
+    const float orho = accumulate ? grho[m] : 0.f;
+    gvp[m] = ovp + 2.f * a.M[c] * gp;
+    gvs[m] = ovs + 2.f * a.U[c] * gu;
+    grho[m] = orho + (a.M[c] * gp + a.U[c] * gu + gr);
 }
 
 // model products (copied from the context's padded model, plane j = 0) and damping
@@ -367,7 +400,8 @@ __global__ void k_born_model(BornArgs a, const float* Mc, const float* Uc, const
 {
     int i, k;
     long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long zo;
+    if (!cell_of(a, i, k, c, zo)) return;
     const long long m = (long long)k * csz + i;
     M[c] = Mc[m];
     U[c] = Uc[m];
@@ -384,14 +418,15 @@ __global__ void k_born_pert(BornArgs a, const float* rvp, const float* rvs, cons
 {
     int i, k;
     long long c;
-    if (!cell_of(a, i, k, c)) return;
+    long long zo;
+    if (!cell_of(a, i, k, c, zo)) return;
     const long long m = (long long)k * a.nx + i;
     dM[c] = a.M[c] * (rrho[m] + 2.f * rvp[m]);
     dU[c] = a.U[c] * (rrho[m] + 2.f * rvs[m]);
     rr[c] = rrho[m];
 }
 
-dim3 born_grid(const BornArgs& a) { return dim3((a.nx + 31) / 32, (a.nz + 7) / 8); }
+dim3 born_grid(const BornArgs& a, int shots = 1) { return dim3((a.nx + 31) / 32, (a.nz + 7) / 8, shots); }
 
 }  // namespace
 
@@ -415,7 +450,7 @@ namespace {
 template <int R, int NM>
 void step_r(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
 {
-    const dim3 g = born_grid(a), b(32, 8);
+    const dim3 g = born_grid(a, a.nshot), b(32, 8);
     if (born) k_born_stress<R, true, NM><<<g, b, 0, s>>>(a, it);
     else k_born_stress<R, false, NM><<<g, b, 0, s>>>(a, it);
     if (born) k_born_velocity<R, true, false><<<g, b, 0, s>>>(a, it);
@@ -425,7 +460,7 @@ void step_r(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
 template <int R, int NM>
 void adj_r(const BornArgs& a, int it, cudaStream_t s)
 {
-    const dim3 g = born_grid(a), b(32, 8);
+    const dim3 g = born_grid(a, a.nshot), b(32, 8);
     k_adj_vel<R><<<g, b, 0, s>>>(a);
     k_adj_mem<R, NM><<<g, b, 0, s>>>(a);
     k_adj_str<R><<<g, b, 0, s>>>(a, it - 1);
@@ -469,13 +504,14 @@ cudaError_t born_launch_adjoint_step(const BornArgs& a, int it, cudaStream_t s)
 cudaError_t born_launch_inject(const BornArgs& a, int it, cudaStream_t s)
 {
     if (a.nrx <= 0) return cudaSuccess;
-    k_adj_inject<<<(a.nrx + 127) / 128, 128, 0, s>>>(a, it);
+    k_adj_inject<<<dim3((a.nrx + 127) / 128, a.nshot), 128, 0, s>>>(a, it);
     return cudaGetLastError();
 }
 
-cudaError_t born_launch_final(const BornArgs& a, float* gvp, float* gvs, float* grho, cudaStream_t s)
+cudaError_t born_launch_final(const BornArgs& a, float* gvp, float* gvs, float* grho, bool accumulate,
+                              cudaStream_t s)
 {
-    k_born_final<<<born_grid(a), dim3(32, 8), 0, s>>>(a, gvp, gvs, grho);
+    k_born_final<<<born_grid(a), dim3(32, 8), 0, s>>>(a, gvp, gvs, grho, accumulate ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -28,11 +28,21 @@ struct BornArgs {
     float *Sxx, *Szz, *Sxz;                // strain adjoint of the reverse step (scratch)
     const float *hv0x, *hv0z, *ha0x, *ha0z;// background history read by the adjoint step
     float *kv0x, *kv0z, *ka0x, *ka0z;      // history slot written by a recording step
-    int ssx, ssz, nw;
-    const float* wavelet;
-    int rx0, nrx, drx, rz;
-    float* traces;                         // [3][nt][nrx]: recorded (forward) or residual (adjoint)
+    int nw;
+    const float* wavelet;                  // shot s's wavelet at wavelet + s * wstride
+    int wstride;
+    int nrx;                               // receivers per shot
+    float* traces;                         // per shot [3][nt][nrx]: recorded (forward) or residual (adjoint)
     int nt;
+    // Shots of one launch (blockIdx.z = shot): every per-shot volume above (states,
+    // memory variables, adjoint, strain scratch, gradient accumulators, history) is
+    // [shot][n] with the shot stride `ss` floats; shot s's source cell, receiver line
+    // and traces come from shot_tab[s * 8 + 0..5] = (sx, sz, rx0, nrx, drx, rz) and
+    // traces + s * tstride.  The model and perturbation products are shared.
+    int nshot;
+    long long ss;
+    const int* shot_tab;
+    long long tstride;
 };
 
 cudaError_t born_launch_model(const BornArgs& a, const float* Mc, const float* Uc, const float* Bc,
@@ -43,6 +53,9 @@ cudaError_t born_launch_pert(const BornArgs& a, const float* rvp, const float* r
 cudaError_t born_launch_step(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s);
 cudaError_t born_launch_adjoint_step(const BornArgs& a, int it, cudaStream_t s);
 cudaError_t born_launch_inject(const BornArgs& a, int it, cudaStream_t s);
-cudaError_t born_launch_final(const BornArgs& a, float* gvp, float* gvs, float* grho, cudaStream_t s);
+// gradients summed over the launch's shots, written to (or, with accumulate, added to)
+// the nz x nx outputs
+cudaError_t born_launch_final(const BornArgs& a, float* gvp, float* gvs, float* grho, bool accumulate,
+                              cudaStream_t s);
 
 }  // namespace ertm

@@ -105,16 +105,25 @@ struct ertm_ctx {
     std::string err;
     long long launches = 0;
 
-    // Born / adjoint state (2D, compact layout; allocated on first use)
+    // Born / adjoint state (2D, compact layout; allocated on first use).  Shared
+    // volumes (model and perturbation products) once; per-shot volumes for a group
+    // of `G` shots run by one launch per step, each type laid out [shot][n].
     struct BornState {
         bool ready = false;
         long long px = 0, n = 0;          // pitch and floats per compact volume
-        float* block = nullptr;           // one allocation holding every compact volume
-        float* vol[64] = {nullptr};       // the BV_* volumes (BV_N of them)
-        float* ckpt = nullptr;            // checkpoints: nck x 5 volumes
-        int nck = 0;
-        float* hist = nullptr;            // history: K x 4 volumes
-        int K = 0;
+        float* shared = nullptr;          // the SV_* volumes
+        float* sv[16] = {nullptr};
+        float* block = nullptr;           // the PV_* volumes of G shots
+        float* pv[64] = {nullptr};        // type q, shot 0 (shot s at + s * n)
+        int G = 0;
+        float* ckpt = nullptr;            // checkpoints: nck x 14 types x G shots
+        long long ckpt_floats = 0;
+        float* hist = nullptr;            // history: K x 4 types x G shots
+        long long hist_floats = 0;
+        int* tab = nullptr;               // shot table, G x 8 ints (device)
+        int tab_cap = 0;
+        float* wav = nullptr;             // wavelets, G x nw (device)
+        long long wav_cap = 0;
     } born;
 };
 
@@ -849,9 +858,12 @@ int ertm_destroy(ertm_ctx* c)
     cudaFree(c->it_d);
     cudaFree(c->vmax_d);
     cudaFree(c->err_d);
+    cudaFree(c->born.shared);
     cudaFree(c->born.block);
     cudaFree(c->born.ckpt);
     cudaFree(c->born.hist);
+    cudaFree(c->born.tab);
+    cudaFree(c->born.wav);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return ERTM_OK;
@@ -1260,14 +1272,16 @@ int ertm_set_wait_fault(ertm_ctx* c, int plane, uint32_t polls)
 // ---------------------------------------------------------------------------
 namespace {
 
-// compact volumes: model products; background state (5 fields + 9 memory
-// variables, contiguous so that a checkpoint is one copy); scattered state;
-// perturbation products; adjoint state, gradients, adjoint memory variables and
-// the strain-adjoint scratch
-enum { BV_M, BV_U, BV_L, BV_B, BV_G1, BV_G2, BV_BG, BV_R0 = BV_BG + 5, BV_SC = BV_R0 + 9,
-       BV_R = BV_SC + 5, BV_DM = BV_R + 9, BV_DU, BV_RR, BV_ADJ, BV_GRAD = BV_ADJ + 5,
-       BV_LR = BV_GRAD + 4, BV_S = BV_LR + 9, BV_N = BV_S + 3 };
-static_assert(BV_N <= 64, "BornState::vol holds 64 volumes");
+// Shared compact volumes: model products, damping factors, perturbation products.
+enum { SV_M, SV_U, SV_L, SV_B, SV_G1, SV_G2, SV_DM, SV_DU, SV_RR, SV_N };
+// Per-shot compact volume types, each [shot][n] over a group of shots: background
+// state (5 fields + 9 memory variables, contiguous so that a checkpoint of every shot
+// is one copy), scattered state and memory variables, adjoint state, gradient
+// accumulators (pi, unused, mu, rho), adjoint memory variables, strain-adjoint scratch.
+enum { PV_BG = 0, PV_R0 = PV_BG + 5, PV_SC = PV_R0 + 9, PV_R = PV_SC + 5, PV_ADJ = PV_R + 9,
+       PV_GRAD = PV_ADJ + 5, PV_LR = PV_GRAD + 4, PV_S = PV_LR + 9, PV_N = PV_S + 3 };
+static_assert(PV_N <= 64 && SV_N <= 16, "BornState volume tables");
+constexpr int kBornMaxShots = 256;   // shots per launch (grid z)
 
 // GSLS fit (tau method, first order): relaxation frequencies
 // f_l = f0 10^(2 (l + 1/2) / nm - 1), tau_sigma = 1 / (2 pi f_l);
@@ -1289,39 +1303,43 @@ void visco_fit(int nm, double qp, double qs, double f0, double* tau_sigma, doubl
     *ts = (1.0 / qs) * s1 / s2;
 }
 
-int born_check(ertm_ctx* c, const ertm_shot* s)
+int born_check(ertm_ctx* c, const ertm_shot* shots, int nshots)
 {
     if (!c->g.two_d) return fail(c, ERTM_ENOTSUP, "Born operators support 2D grids only");
     if (c->cfg.boundary == ERTM_BOUNDARY_CPML)
         return fail(c, ERTM_ENOTSUP, "Born operators support sponge boundaries only");
     if (!c->model_set[1]) return fail(c, ERTM_ESTATE, "migration model not set");
-    int rc = validate_shot(c, s, true);
-    if (rc) return rc;
+    if (!shots || nshots < 1) return fail(c, ERTM_EINVAL, "no shots");
+    for (int i = 0; i < nshots; i++) {
+        int rc = validate_shot(c, &shots[i], true);
+        if (rc) return rc;
+        if (shots[i].nrx != shots[0].nrx || shots[i].nw != shots[0].nw)
+            return fail(c, ERTM_EINVAL, "shots of one call need the same receiver count and wavelet length");
+    }
     return ERTM_OK;
 }
 
-// arguments over the compact layout; model products copied from the migration model
+// shared volumes and the argument block (shot-independent part); model products
+// copied from the migration model
 int born_prepare(ertm_ctx* c, BornArgs& a)
 {
     auto& B = c->born;
     const Geom& g = c->g;
     int rc;
     if (!B.ready) {
-        if (B.block) {   // the active grid changed (ertm_set_grid): size everything afresh
-            CK(c, cudaStreamSynchronize(c->stream));
-            cudaFree(B.block);
-            cudaFree(B.ckpt);
-            cudaFree(B.hist);
-            B.block = B.ckpt = B.hist = nullptr;
-            B.nck = B.K = 0;
-        }
+        CK(c, cudaStreamSynchronize(c->stream));
+        cudaFree(B.shared);
+        cudaFree(B.block);
+        cudaFree(B.ckpt);
+        cudaFree(B.hist);
+        B.shared = B.block = B.ckpt = B.hist = nullptr;
+        B.G = 0;
+        B.ckpt_floats = B.hist_floats = 0;
         B.px = round_up(2LL * BXH + round_up(g.nx, 32), 32);
         B.n = B.px * (g.nz + 2LL * c->R);
-        // one block so that consecutive volumes (the background fields and memory
-        // variables of a checkpoint) are contiguous
-        CK(c, cudaMalloc(&B.block, sizeof(float) * B.n * BV_N));
-        CK(c, cudaMemsetAsync(B.block, 0, sizeof(float) * B.n * BV_N, c->stream));
-        for (int q = 0; q < BV_N; q++) B.vol[q] = B.block + (size_t)q * B.n;
+        CK(c, cudaMalloc(&B.shared, sizeof(float) * B.n * SV_N));
+        CK(c, cudaMemsetAsync(B.shared, 0, sizeof(float) * B.n * SV_N, c->stream));
+        for (int q = 0; q < SV_N; q++) B.sv[q] = B.shared + (size_t)q * B.n;
         B.ready = true;
     }
     if ((rc = upload_profiles(c, 0.f))) return rc;
@@ -1335,25 +1353,9 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
         a.cz[q] = (float)(c->coef[q] / c->cfg.dz);
     }
     a.dt = c->cfg.dt_ms / 1000.f;
-    a.M = B.vol[BV_M]; a.U = B.vol[BV_U]; a.L = B.vol[BV_L]; a.B = B.vol[BV_B];
-    a.g1 = B.vol[BV_G1]; a.g2 = B.vol[BV_G2];
-    float** bg[5] = {&a.v0x, &a.v0z, &a.s0xx, &a.s0zz, &a.s0xz};
-    float** sc[5] = {&a.vx, &a.vz, &a.sxx, &a.szz, &a.sxz};
-    float** ad[5] = {&a.ax, &a.az, &a.hxx, &a.hzz, &a.hxz};
-    for (int q = 0; q < 5; q++) {
-        *bg[q] = B.vol[BV_BG + q];
-        *sc[q] = B.vol[BV_SC + q];
-        *ad[q] = B.vol[BV_ADJ + q];
-    }
-    a.dM = B.vol[BV_DM]; a.dU = B.vol[BV_DU]; a.rr = B.vol[BV_RR];
-    a.gM = B.vol[BV_GRAD]; a.gL = B.vol[BV_GRAD + 1]; a.gU = B.vol[BV_GRAD + 2];
-    a.gR = B.vol[BV_GRAD + 3];
-    for (int q = 0; q < 9; q++) {
-        a.r0[q] = B.vol[BV_R0 + q];
-        a.r[q] = B.vol[BV_R + q];
-        a.lr[q] = B.vol[BV_LR + q];
-    }
-    a.Sxx = B.vol[BV_S]; a.Szz = B.vol[BV_S + 1]; a.Sxz = B.vol[BV_S + 2];
+    a.M = B.sv[SV_M]; a.U = B.sv[SV_U]; a.L = B.sv[SV_L]; a.B = B.sv[SV_B];
+    a.g1 = B.sv[SV_G1]; a.g2 = B.sv[SV_G2];
+    a.dM = B.sv[SV_DM]; a.dU = B.sv[SV_DU]; a.rr = B.sv[SV_RR];
     a.nm = c->cfg.visco_nmech;
     a.kp = a.ks = 1.f;
     a.tp = a.ts = 0.f;
@@ -1372,29 +1374,98 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
         }
     }
     a.nt = c->cfg.nt;
+    a.nshot = 1;
+    a.ss = B.n;
     CK(c, born_launch_model(a, c->m[1][0], c->m[1][1], c->m[1][2], g.sz, c->att[0], c->att[2],
-                            B.vol[BV_M], B.vol[BV_U], B.vol[BV_L], B.vol[BV_B], B.vol[BV_G1],
-                            B.vol[BV_G2], c->stream));
+                            B.sv[SV_M], B.sv[SV_U], B.sv[SV_L], B.sv[SV_B], B.sv[SV_G1], B.sv[SV_G2],
+                            c->stream));
     c->launches++;
     return ERTM_OK;
 }
 
-void born_shot(BornArgs& a, const ertm_shot* s, const float* wav)
+// per-shot volumes for a group of G shots (grown on demand; the type stride is G n)
+int born_group_volumes(ertm_ctx* c, int G)
 {
-    a.ssx = s->sx;
-    a.ssz = s->sz;
-    a.nw = s->nw;
-    a.wavelet = wav;
-    a.rx0 = s->rx0;
-    a.nrx = s->nrx;
-    a.drx = s->drx;
-    a.rz = s->rz;
+    auto& B = c->born;
+    if (B.G < G) {
+        CK(c, cudaStreamSynchronize(c->stream));
+        cudaFree(B.block);
+        B.block = nullptr;
+        B.G = 0;
+        CK(c, cudaMalloc(&B.block, sizeof(float) * B.n * PV_N * G));
+        B.G = G;
+    }
+    return ERTM_OK;
 }
 
-int born_zero(ertm_ctx* c, int first, int count)
+// lay the per-shot volumes of a group of G shots out densely (type q at q G n, shot
+// s at + s n) and point the per-shot arguments at them
+void born_group_args(ertm_ctx* c, BornArgs& a, int G)
 {
-    for (int q = first; q < first + count; q++)
-        CK(c, cudaMemsetAsync(c->born.vol[q], 0, sizeof(float) * c->born.n, c->stream));
+    auto& B = c->born;
+    for (int q = 0; q < PV_N; q++) B.pv[q] = B.block + (size_t)q * G * B.n;
+    a.nshot = G;
+    a.ss = B.n;
+    float** bg[5] = {&a.v0x, &a.v0z, &a.s0xx, &a.s0zz, &a.s0xz};
+    float** sc[5] = {&a.vx, &a.vz, &a.sxx, &a.szz, &a.sxz};
+    float** ad[5] = {&a.ax, &a.az, &a.hxx, &a.hzz, &a.hxz};
+    for (int q = 0; q < 5; q++) {
+        *bg[q] = B.pv[PV_BG + q];
+        *sc[q] = B.pv[PV_SC + q];
+        *ad[q] = B.pv[PV_ADJ + q];
+    }
+    a.gM = B.pv[PV_GRAD]; a.gL = B.pv[PV_GRAD + 1]; a.gU = B.pv[PV_GRAD + 2];
+    a.gR = B.pv[PV_GRAD + 3];
+    for (int q = 0; q < 9; q++) {
+        a.r0[q] = B.pv[PV_R0 + q];
+        a.r[q] = B.pv[PV_R + q];
+        a.lr[q] = B.pv[PV_LR + q];
+    }
+    a.Sxx = B.pv[PV_S]; a.Szz = B.pv[PV_S + 1]; a.Sxz = B.pv[PV_S + 2];
+}
+
+// shot table and wavelets of shots[0..G) on the device
+int born_group_shots(ertm_ctx* c, BornArgs& a, const ertm_shot* shots, int G)
+{
+    auto& B = c->born;
+    const int nw = shots[0].nw;
+    if (B.tab_cap < G) {
+        cudaFree(B.tab);
+        B.tab = nullptr;
+        B.tab_cap = 0;
+        CK(c, cudaMalloc(&B.tab, sizeof(int) * 8 * G));
+        B.tab_cap = G;
+    }
+    const long long wn = (long long)G * (nw > 0 ? nw : 1);
+    if (B.wav_cap < wn) {
+        cudaFree(B.wav);
+        B.wav = nullptr;
+        B.wav_cap = 0;
+        CK(c, cudaMalloc(&B.wav, sizeof(float) * wn));
+        B.wav_cap = wn;
+    }
+    std::vector<int> tab(8 * (size_t)G, 0);
+    for (int s = 0; s < G; s++) {
+        const ertm_shot& sh = shots[s];
+        int* t = &tab[8 * (size_t)s];
+        t[0] = sh.sx; t[1] = sh.sz; t[2] = sh.rx0; t[3] = sh.nrx; t[4] = sh.drx; t[5] = sh.rz;
+        if (nw > 0)
+            CK(c, cudaMemcpyAsync(B.wav + (size_t)s * nw, sh.wavelet, sizeof(float) * nw, cudaMemcpyDefault,
+                                  c->stream));
+    }
+    CK(c, cudaMemcpyAsync(B.tab, tab.data(), sizeof(int) * 8 * G, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));   // the host table is a temporary
+    a.shot_tab = B.tab;
+    a.nw = nw;
+    a.wavelet = B.wav;
+    a.wstride = nw > 0 ? nw : 1;
+    a.nrx = shots[0].nrx;
+    return ERTM_OK;
+}
+
+int born_zero_types(ertm_ctx* c, int first, int count, int G)
+{
+    CK(c, cudaMemsetAsync(c->born.pv[first], 0, sizeof(float) * c->born.n * G * count, c->stream));
     return ERTM_OK;
 }
 
@@ -1416,114 +1487,114 @@ int born_stage_in(ertm_ctx* c, const float* const* src, int count, const float**
     return ERTM_OK;
 }
 
+// Shots per launch: at most `want`, bounded so that the group's volumes (and, for the
+// adjoint, its checkpoints and history) take at most about 60 % of the free memory.
+int born_group_size(ertm_ctx* c, int want, long long floats_per_shot)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    // memory the context already holds for a group counts as available
+    const long long held = (long long)c->born.G * c->born.n * PV_N + c->born.ckpt_floats + c->born.hist_floats;
+    const double avail = 0.6 * (double)free_b + 4.0 * (double)held;
+    long long g = (long long)(avail / (4.0 * (double)floats_per_shot));
+    if (g > want) g = want;
+    if (g > kBornMaxShots) g = kBornMaxShots;
+    return g < 1 ? 1 : (int)g;
+}
+
 }  // namespace
 
 extern "C" {
 
-int ertm_born_forward(ertm_ctx* c, const ertm_shot* s, const float* r_vp, const float* r_vs,
-                      const float* r_rho, float* data_out)
+int ertm_born_forward_shots(ertm_ctx* c, const ertm_shot* shots, int nshots, const float* r_vp,
+                            const float* r_vs, const float* r_rho, float* data_out)
 {
     if (!c) return ERTM_EINVAL;
     Range range("ertm born forward");
     if (!r_vp || !r_vs || !r_rho || !data_out) return fail(c, ERTM_EINVAL, "NULL argument");
     CK(c, cudaSetDevice(c->device));
-    int rc = born_check(c, s);
+    int rc = born_check(c, shots, nshots);
     if (rc) return rc;
     BornArgs a;
     if ((rc = born_prepare(c, a))) return rc;
-    if ((rc = upload_wavelet(c, s))) return rc;
-    born_shot(a, s, c->wavelet);
     const float* src[3] = {r_vp, r_vs, r_rho};
     const float* dev[3];
     if ((rc = born_stage_in(c, src, 3, dev))) return rc;
-    CK(c, born_launch_pert(a, dev[0], dev[1], dev[2], c->born.vol[BV_DM], c->born.vol[BV_DU],
-                           c->born.vol[BV_RR], c->stream));
-    if ((rc = born_zero(c, BV_BG, BV_DM - BV_BG))) return rc;   // background and scattered states
-    const size_t nd = 3 * (size_t)c->cfg.nt * s->nrx;
+    auto& B = c->born;
+    CK(c, born_launch_pert(a, dev[0], dev[1], dev[2], B.sv[SV_DM], B.sv[SV_DU], B.sv[SV_RR], c->stream));
+    c->launches++;
+    const int nt = c->cfg.nt;
+    const long long nd = 3LL * nt * shots[0].nrx;   // floats of one shot's traces
     const bool dev_out = is_device_ptr(data_out);
-    if (!dev_out && (rc = ensure_traces(c, nd))) return rc;
-    a.traces = dev_out ? data_out : c->traces;
-    CK(c, cudaMemsetAsync(a.traces, 0, sizeof(float) * nd, c->stream));
-    for (int it = 0; it < c->cfg.nt; it++) CK(c, born_launch_step(a, it, true, false, c->stream));
-    c->launches += 1 + 2LL * c->cfg.nt;
-    if (!dev_out)
-        CK(c, cudaMemcpyAsync(data_out, a.traces, sizeof(float) * nd, cudaMemcpyDeviceToHost, c->stream));
+    const int G = born_group_size(c, nshots, B.n * (long long)PV_N + (dev_out ? 0 : nd));
+    if ((rc = born_group_volumes(c, G))) return rc;
+    if (!dev_out && (rc = ensure_traces(c, (size_t)nd * G))) return rc;
+    for (int s0 = 0; s0 < nshots; s0 += G) {
+        const int g = std::min(G, nshots - s0);
+        born_group_args(c, a, g);
+        if ((rc = born_group_shots(c, a, shots + s0, g))) return rc;
+        a.tstride = nd;
+        a.traces = dev_out ? data_out + (size_t)s0 * nd : c->traces;
+        // background and scattered states of the group (types BG .. R, contiguous)
+        if ((rc = born_zero_types(c, PV_BG, PV_ADJ - PV_BG, g))) return rc;
+        CK(c, cudaMemsetAsync(a.traces, 0, sizeof(float) * nd * g, c->stream));
+        for (int it = 0; it < nt; it++) CK(c, born_launch_step(a, it, true, false, c->stream));
+        c->launches += 2LL * nt;
+        if (!dev_out)
+            CK(c, cudaMemcpyAsync(data_out + (size_t)s0 * nd, a.traces, sizeof(float) * nd * g,
+                                  cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(c, cudaStreamSynchronize(c->stream));
     return ERTM_OK;
 }
 
-int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, float* g_vp,
-                      float* g_vs, float* g_rho)
+int ertm_born_forward(ertm_ctx* c, const ertm_shot* s, const float* r_vp, const float* r_vs,
+                      const float* r_rho, float* data_out)
+{
+    return ertm_born_forward_shots(c, s, 1, r_vp, r_vs, r_rho, data_out);
+}
+
+int ertm_born_adjoint_shots(ertm_ctx* c, const ertm_shot* shots, int nshots, const float* residual,
+                            float* g_vp, float* g_vs, float* g_rho)
 {
     if (!c) return ERTM_EINVAL;
     Range range("ertm born adjoint");
     if (!residual || !g_vp || !g_vs || !g_rho) return fail(c, ERTM_EINVAL, "NULL argument");
     CK(c, cudaSetDevice(c->device));
-    int rc = born_check(c, s);
+    int rc = born_check(c, shots, nshots);
     if (rc) return rc;
     BornArgs a;
     if ((rc = born_prepare(c, a))) return rc;
-    if ((rc = upload_wavelet(c, s))) return rc;
-    born_shot(a, s, c->wavelet);
     auto& B = c->born;
     const int nt = c->cfg.nt;
     const int K = std::min(nt, c->cfg.checkpoint_every > 0 ? c->cfg.checkpoint_every : 200);
     const int nck = (nt + K - 1) / K;
-    const int nbg = 5 + (a.nm ? 9 : 0);   // background volumes in a checkpoint
-    if (B.nck < nck) {
+    const int nbg = 5 + (a.nm ? 9 : 0);   // background volume types in a checkpoint
+    const long long nd = 3LL * nt * shots[0].nrx;
+    const bool dev_res = is_device_ptr(residual);
+    const long long per_shot = B.n * ((long long)PV_N + 14LL * nck + 4LL * K) + (dev_res ? 0 : nd);
+    const int G = born_group_size(c, nshots, per_shot);
+    if ((rc = born_group_volumes(c, G))) return rc;
+    const long long ck_need = 14LL * nck * G * B.n, hist_need = 4LL * K * G * B.n;
+    if (B.ckpt_floats < ck_need) {
         cudaFree(B.ckpt);
         B.ckpt = nullptr;
-        CK(c, cudaMalloc(&B.ckpt, sizeof(float) * 14 * B.n * nck));
-        B.nck = nck;
+        B.ckpt_floats = 0;
+        CK(c, cudaMalloc(&B.ckpt, sizeof(float) * ck_need));
+        B.ckpt_floats = ck_need;
     }
-    if (B.K < K) {
+    if (B.hist_floats < hist_need) {
         cudaFree(B.hist);
         B.hist = nullptr;
-        CK(c, cudaMalloc(&B.hist, sizeof(float) * 4 * B.n * K));
-        B.K = K;
+        B.hist_floats = 0;
+        CK(c, cudaMalloc(&B.hist, sizeof(float) * hist_need));
+        B.hist_floats = hist_need;
     }
-    // residual on the device
-    const size_t nd = 3 * (size_t)nt * s->nrx;
-    if (is_device_ptr(residual)) a.traces = const_cast<float*>(residual);
-    else {
-        if ((rc = ensure_traces(c, nd))) return rc;
-        CK(c, cudaMemcpyAsync(c->traces, residual, sizeof(float) * nd, cudaMemcpyHostToDevice, c->stream));
-        a.traces = c->traces;
-    }
-    // 1. background forward, checkpointing its state every K steps
-    if ((rc = born_zero(c, BV_BG, 14))) return rc;
-    for (int it = 0; it < nt; it++) {
-        if (it % K == 0)
-            CK(c, cudaMemcpyAsync(B.ckpt + (size_t)(it / K) * nbg * B.n, B.vol[BV_BG],
-                                  sizeof(float) * nbg * B.n, cudaMemcpyDeviceToDevice, c->stream));
-        CK(c, born_launch_step(a, it, false, false, c->stream));
-    }
-    // 2. reverse sweep, one checkpoint segment at a time
-    if ((rc = born_zero(c, BV_ADJ, BV_N - BV_ADJ))) return rc;   // adjoint, gradients, scratch
-    CK(c, born_launch_inject(a, nt - 1, c->stream));
-    for (int sg = nck - 1; sg >= 0; sg--) {
-        const int t0 = sg * K, t1 = std::min(nt, t0 + K);
-        CK(c, cudaMemcpyAsync(B.vol[BV_BG], B.ckpt + (size_t)sg * nbg * B.n, sizeof(float) * nbg * B.n,
-                              cudaMemcpyDeviceToDevice, c->stream));
-        for (int it = t0; it < t1; it++) {
-            float* h = B.hist + (size_t)(it - t0) * 4 * B.n;
-            a.kv0x = h;
-            a.kv0z = h + B.n;
-            a.ka0x = h + 2 * B.n;
-            a.ka0z = h + 3 * B.n;
-            CK(c, born_launch_step(a, it, false, true, c->stream));
-        }
-        for (int it = t1 - 1; it >= t0; it--) {
-            const float* h = B.hist + (size_t)(it - t0) * 4 * B.n;
-            a.hv0x = h;
-            a.hv0z = h + B.n;
-            a.ha0x = h + 2 * B.n;
-            a.ha0z = h + 3 * B.n;
-            CK(c, born_launch_adjoint_step(a, it, c->stream));
-        }
-    }
-    c->launches += 2LL * nt * 2 + 3LL * nt + 2;
-    // 3. gradients w.r.t. the relative perturbations
+    if (!dev_res && (rc = ensure_traces(c, (size_t)nd * G))) return rc;
+    // gradient targets: the caller's device arrays, or the stage for host arrays
     float* outs[3] = {g_vp, g_vs, g_rho};
     const long long n = (long long)c->g.nx * c->g.nz;
     bool dev[3];
@@ -1531,12 +1602,72 @@ int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, fl
     if (!(dev[0] && dev[1] && dev[2]) && (rc = ensure_stage(c))) return rc;
     float* tgt[3];
     for (int q = 0; q < 3; q++) tgt[q] = dev[q] ? outs[q] : c->stage + q * n;
-    CK(c, born_launch_final(a, tgt[0], tgt[1], tgt[2], c->stream));
+    for (int s0 = 0; s0 < nshots; s0 += G) {
+        const int g = std::min(G, nshots - s0);
+        born_group_args(c, a, g);
+        if ((rc = born_group_shots(c, a, shots + s0, g))) return rc;
+        a.tstride = nd;
+        if (dev_res) a.traces = const_cast<float*>(residual) + (size_t)s0 * nd;
+        else {
+            CK(c, cudaMemcpyAsync(c->traces, residual + (size_t)s0 * nd, sizeof(float) * nd * g,
+                                  cudaMemcpyHostToDevice, c->stream));
+            a.traces = c->traces;
+        }
+        const size_t ck_seg = (size_t)nbg * g * B.n;   // floats of one checkpoint of the group
+        // 1. background forward, checkpointing every shot's state every K steps
+        if ((rc = born_zero_types(c, PV_BG, 14, g))) return rc;
+        // the group's background types (BG, R0) are contiguous: one copy per checkpoint
+        auto save = [&](int seg) {
+            return cudaMemcpyAsync(B.ckpt + seg * ck_seg, B.pv[PV_BG], sizeof(float) * ck_seg,
+                                   cudaMemcpyDeviceToDevice, c->stream);
+        };
+        auto load = [&](int seg) {
+            return cudaMemcpyAsync(B.pv[PV_BG], B.ckpt + seg * ck_seg, sizeof(float) * ck_seg,
+                                   cudaMemcpyDeviceToDevice, c->stream);
+        };
+        for (int it = 0; it < nt; it++) {
+            if (it % K == 0) CK(c, save(it / K));
+            CK(c, born_launch_step(a, it, false, false, c->stream));
+        }
+        // 2. reverse sweep, one checkpoint segment at a time
+        if ((rc = born_zero_types(c, PV_ADJ, PV_N - PV_ADJ, g))) return rc;   // adjoint, gradients, scratch
+        CK(c, born_launch_inject(a, nt - 1, c->stream));
+        for (int sg = nck - 1; sg >= 0; sg--) {
+            const int t0 = sg * K, t1 = std::min(nt, t0 + K);
+            CK(c, load(sg));
+            for (int it = t0; it < t1; it++) {
+                float* h = B.hist + (size_t)(it - t0) * 4 * g * B.n;
+                a.kv0x = h;
+                a.kv0z = h + g * B.n;
+                a.ka0x = h + 2 * g * B.n;
+                a.ka0z = h + 3 * g * B.n;
+                CK(c, born_launch_step(a, it, false, true, c->stream));
+            }
+            for (int it = t1 - 1; it >= t0; it--) {
+                const float* h = B.hist + (size_t)(it - t0) * 4 * g * B.n;
+                a.hv0x = h;
+                a.hv0z = h + g * B.n;
+                a.ha0x = h + 2 * g * B.n;
+                a.ha0z = h + 3 * g * B.n;
+                CK(c, born_launch_adjoint_step(a, it, c->stream));
+            }
+        }
+        c->launches += 2LL * nt * 2 + 3LL * nt + 1;
+        // 3. gradients w.r.t. the relative perturbations, summed over the group's shots
+        CK(c, born_launch_final(a, tgt[0], tgt[1], tgt[2], s0 > 0, c->stream));
+        c->launches++;
+    }
     for (int q = 0; q < 3; q++)
         if (!dev[q])
             CK(c, cudaMemcpyAsync(outs[q], tgt[q], sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     return ERTM_OK;
+}
+
+int ertm_born_adjoint(ertm_ctx* c, const ertm_shot* s, const float* residual, float* g_vp,
+                      float* g_vs, float* g_rho)
+{
+    return ertm_born_adjoint_shots(c, s, 1, residual, g_vp, g_vs, g_rho);
 }
 
 }  // extern "C"

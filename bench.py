@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
     ap.add_argument("--workload", default="shot",
-                    choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op", "refstep"],
+                    choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op", "lsrtm-cg", "refstep"],
                     help="windows: batched aperture windows; unet: one U-Net training step at "
                          "256x512, batch 16; lsrtm: learned vs plain CG (each its own line); "
                          "lsrtm-op: Born forward + adjoint per shot on the 880x480 GSLS-3 LSRTM grid; "
@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--shots", type=int, default=64, help="windows workload: shots")
     ap.add_argument("--lanes", type=int, default=4, help="windows workload: shots in flight")
+    ap.add_argument("--cg-iters", type=int, default=20, help="lsrtm-cg workload: CG iterations")
     return ap.parse_args()
 
 
@@ -364,18 +365,16 @@ def run_lsrtm(args):
         "cases": [_fmt_case(r) for r in rows]}), flush=True)
 
 
-def run_lsrtm_op(args):
-    """LSRTM operators at the LSRTM workload's size: 880 x 480 cells (800 x 400 interior +
-    40-cell sponge) at 5 m, GSLS with 3 mechanisms (Qp 100, Qs 50, f0 15 Hz), dt 0.5 ms,
-    4000 steps, 800 receivers, checkpoints every 200 steps.  Times the Born forward and
-    its adjoint (one CG iteration's work per shot) over `--shots` shots of the 40-shot
-    layout and projects one 40-shot iteration and the 20-iteration run."""
+def _lsrtm_setup(nshots: int):
+    """The LSRTM workload: 880 x 480 cells (800 x 400 interior + 40-cell sponge) at 5 m,
+    seeded layered-and-faulted model, GSLS with 3 mechanisms (Qp 100, Qs 50, f0 15 Hz),
+    dt 0.5 ms, 4000 steps, 800 receivers at 10 m depth, 40 shot positions, checkpoints
+    every 200 steps; migration model smoothed with sigma 10 cells; the true relative
+    perturbations are the model against its smoothed version."""
     import numpy as np
-    import torch
+    ertm = importlib.import_module(PKG)
     L = importlib.import_module(PKG + ".learned")
     syn = importlib.import_module(PKG + ".synthetic")
-    ertm = importlib.import_module(PKG)
-    nshots = max(1, min(args.shots, 40))
     g = L.Geometry(nzi=400, nxi=800, h=5.0, pml=40, nt=4000, dt_ms=0.5, nshots=40, f0=15.0,
                    sigma=10.0, visco=(3, 100.0, 50.0, 15.0))
     vp, vs, rho = syn.faulted_2d(20261203, g.nzi, g.nxi, g.h)
@@ -392,38 +391,126 @@ def run_lsrtm_op(args):
     w = syn.ricker(g.f0, g.dt_ms / 1000.0)
     xs = np.linspace(g.pml + 4, nx - g.pml - 5, 40).round().astype(int)
     rz = g.pml + 2
+    pick = xs[np.linspace(0, 39, max(1, min(nshots, 40))).round().astype(int)]
     shots = [ertm.Shot(int(x), 0, rz, wavelet=w, rx0=g.pml, nrx=nx - 2 * g.pml, drx=1, rz=rz)
-             for x in xs[np.linspace(0, 39, nshots).round().astype(int)]]
-    # warm-up: one forward and one adjoint on the first shot (allocations, graphs)
-    d0 = ctx.born_forward(shots[0], *true)
-    ctx.born_adjoint(shots[0], d0)
-    torch.cuda.synchronize()
-    tf = ta = 0.0
-    data = []
-    for s in shots:
-        t0 = time.perf_counter()
-        d = ctx.born_forward(s, *true)
-        tf += time.perf_counter() - t0
-        data.append(d)
-    for s, d in zip(shots, data):
-        t0 = time.perf_counter()
-        ctx.born_adjoint(s, d)
-        ta += time.perf_counter() - t0
-    cell_steps = float(nx * nz) * g.nt
-    per_shot = (tf + ta) / nshots
+             for x in pick]
+    return ertm, ctx, cfg, shots, true, (nz, nx), g
+
+
+LSRTM_WORKLOAD = ("LSRTM 880x480 (800x400 + 40-cell sponge), dx 5 m, GSLS-3 Qp 100 Qs 50 f0 15 Hz, "
+                  "dt 0.5 ms, nt 4000, 800 receivers, checkpoints every 200 steps")
+
+
+def run_lsrtm_op(args):
+    """LSRTM operators at the LSRTM workload's size: the Born forward and its adjoint
+    over `--shots` of the 40 shot positions, all shots in one batched call each (every
+    step's kernels cover every shot), device arrays in and out, CUDA events on the
+    context stream; projects one 40-shot CG iteration and the 20-iteration run."""
+    import torch
+    nshots = max(1, min(args.shots, 40))
+    ertm, ctx, cfg, shots, true, (nz, nx), g = _lsrtm_setup(nshots)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream(dev)
+    ctx.set_stream(st.cuda_stream)
+    m = [torch.from_numpy(a).to(dev) for a in true]
+    data = torch.zeros((len(shots), 3, g.nt, shots[0].nrec), device=dev)
+    grads = [torch.zeros((nz, 1, nx), device=dev) for _ in range(3)]
+    ctx.born_forward_shots(shots[:1], *m, out=data[:1])          # warm-up: allocations
+    ctx.born_adjoint_shots(shots[:1], data[:1], *grads)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize(dev)
+    e[0].record(st)
+    ctx.born_forward_shots(shots, *m, out=data)
+    e[1].record(st)
+    ctx.born_adjoint_shots(shots, data, *grads)
+    e[2].record(st)
+    torch.cuda.synchronize(dev)
+    tf, ta = e[0].elapsed_time(e[1]) / 1e3, e[1].elapsed_time(e[2]) / 1e3
+    cells = float(nx * nz)
+    fwd_steps = 2.0 * cells * g.nt * len(shots)          # background + scattered
+    adj_steps = 3.0 * cells * g.nt * len(shots)          # background, rebuild, adjoint
+    per_shot = (tf + ta) / len(shots)
     print(json.dumps({
-        "metric": "LSRTM operator throughput (Born forward + adjoint, GSLS-3)",
-        "value": round(2 * cell_steps * nshots / (tf + ta) / 1e9, 3), "unit": "Gcell-steps/s",
+        "metric": "LSRTM operator throughput (Born forward + adjoint, GSLS-3, batched shots)",
+        "value": round((fwd_steps + adj_steps) / (tf + ta) / 1e9, 3), "unit": "Gcell-steps/s",
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "LSRTM 880x480 (800x400 + 40-cell sponge), dx 5 m, GSLS-3 Qp 100 Qs 50 "
-                               "f0 15 Hz, dt 0.5 ms, nt 4000, 800 receivers, checkpoints every 200 steps",
-                   "shots_timed": nshots},
-        "forward_s_per_shot": round(tf / nshots, 3), "adjoint_s_per_shot": round(ta / nshots, 3),
-        "forward_gcell_steps_s": round(cell_steps * nshots / tf / 1e9, 3),
-        "adjoint_gcell_steps_s": round(cell_steps * nshots / ta / 1e9, 3),
-        "projected_cg_iteration_40_shots_s": round(40 * per_shot, 1),
+        "config": {"workload": LSRTM_WORKLOAD, "shots_timed": len(shots)},
+        "forward_s": round(tf, 3), "adjoint_s": round(ta, 3),
+        "forward_gcell_steps_s": round(fwd_steps / tf / 1e9, 3),
+        "adjoint_gcell_steps_s": round(adj_steps / ta / 1e9, 3),
+        "projected_cg_iteration_40_shots_s": round(40 * per_shot, 2),
         "projected_20_iterations_s": round(20 * 40 * per_shot, 1),
-        "timing": "host wall clock around each synchronous call, host arrays in and out"}), flush=True)
+        "timing": "CUDA events on the context stream around one batched call each, device arrays"}),
+        flush=True)
+    ctx.close()
+
+
+def run_lsrtm_cg(args):
+    """The LSRTM workload end to end: 20 CGLS iterations over the 40 shots, every CG
+    vector on the device, data modelled with the Born operator from the true
+    perturbations.  Reports the misfit curve and the wall time per iteration, the
+    reflectivity error, and two checks at this size on one shot: the dot-product test
+    of the operator pair and the centred finite difference of the misfit
+    0.5 |F m - d|^2 along a random direction against the adjoint gradient."""
+    import numpy as np
+    import torch
+    lsrtm = importlib.import_module(PKG + ".lsrtm")
+    ertm, ctx, cfg, shots, true, (nz, nx), g = _lsrtm_setup(args.shots)
+    dev = torch.device("cuda", 0)
+    m_true = [torch.from_numpy(a).to(dev) for a in true]
+    t0 = time.perf_counter()
+    data_all = lsrtm.born_all(ctx, shots, m_true)
+    torch.cuda.synchronize(dev)
+    t_data = time.perf_counter() - t0
+    data = [data_all[i] for i in range(len(shots))]
+    times = []
+    last = [time.perf_counter()]
+
+    def cb(it, mis):
+        now = time.perf_counter()
+        times.append(now - last[0])
+        last[0] = now
+
+    t0 = time.perf_counter()
+    last[0] = t0
+    res = lsrtm.cgls(ctx, shots, data, niter=args.cg_iters, callback=cb)
+    torch.cuda.synchronize(dev)
+    t_cg = time.perf_counter() - t0
+    err = [float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(res.m, m_true)]
+    # checks on the first shot at full size
+    rng = np.random.default_rng(7)
+    one = shots[:1]
+    mh = [torch.from_numpy((0.05 * rng.standard_normal((nz, 1, nx))).astype(np.float32)).to(dev)
+          for _ in range(3)]
+    d = lsrtm.born_all(ctx, one, mh)
+    dh = torch.from_numpy(rng.standard_normal(tuple(d.shape)).astype(np.float32)).to(dev)
+    dh[:, 1] = 0
+    gh = lsrtm.adjoint_all(ctx, one, dh)
+    lhs = float((d.double() * dh.double()).sum())
+    rhs = sum(float((a.double() * b.double()).sum()) for a, b in zip(mh, gh))
+    # misfit phi(m) = 0.5 |F m - d1|^2 around m0 = 0.5 true along direction p
+    d1 = data_all[:1]
+    m0 = [0.5 * a for a in m_true]
+    r0 = lsrtm.born_all(ctx, one, m0) - d1
+    grad = lsrtm.adjoint_all(ctx, one, r0)
+    p = mh
+    h = 1.0
+    phi = lambda mm: 0.5 * float(((lsrtm.born_all(ctx, one, mm) - d1).double() ** 2).sum())
+    fd = (phi([a + h * b for a, b in zip(m0, p)]) - phi([a - h * b for a, b in zip(m0, p)])) / (2 * h)
+    an = sum(float((a.double() * b.double()).sum()) for a, b in zip(grad, p))
+    print(json.dumps({
+        "metric": "LSRTM 20-iteration CGLS wall time (40 shots, GSLS-3)", "value": round(t_cg, 2),
+        "unit": "s", "higher_is_better": False, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": LSRTM_WORKLOAD, "shots": len(shots), "cg_iterations": args.cg_iters,
+                   "vectors": "device (torch CUDA tensors)"},
+        "data_modelling_s": round(t_data, 2),
+        "seconds_per_iteration": [round(x, 2) for x in times],
+        "misfit": [round(x, 6) for x in res.misfit], "accepted": res.accepted,
+        "reflectivity_rel_error": {"vp": round(err[0], 4), "vs": round(err[1], 4), "rho": round(err[2], 4)},
+        "dot_test": {"lhs": lhs, "rhs": rhs, "rel": abs(lhs - rhs) / abs(lhs)},
+        "fd_gradient": {"fd": fd, "adjoint": an, "rel": abs(fd - an) / abs(an), "h": h,
+                        "note": "one shot; phi = 0.5 |F m - d|^2 is quadratic in m, so the centred "
+                                "difference is exact up to rounding"}}), flush=True)
     ctx.close()
 
 
@@ -512,6 +599,8 @@ def main():
         return run_lsrtm_op(args)
     if args.workload == "refstep":
         return run_refstep(args)
+    if args.workload == "lsrtm-cg":
+        return run_lsrtm_cg(args)
     import numpy as np
     import torch
     import torch.distributed as dist

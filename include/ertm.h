@@ -215,6 +215,18 @@ int ertm_born_forward(ertm_ctx *ctx, const ertm_shot *shot, const float *r_vp,
                       const float *r_vs, const float *r_rho, float *data_out);
 int ertm_born_adjoint(ertm_ctx *ctx, const ertm_shot *shot, const float *residual,
                       float *g_vp, float *g_vs, float *g_rho);
+/* The same operators over `nshots` shots at once: the shots of a group share every
+ * step kernel launch (one grid layer per shot), the group as large as about 60 % of
+ * the free device memory allows (at most 256 shots).  The reference's LSRTM driver,
+ * absent from its tree, would loop over shots calling its per-shot kernels
+ * (viscoelastic_equation.cu:328-477, :1827-2294, :2398-2505).  All shots need the
+ * same receiver count and wavelet length.  data_out / residual hold
+ * [nshots][3][nt][nrec]; the adjoint returns the gradient summed over the shots
+ * (in shot order).  Host or device pointers. */
+int ertm_born_forward_shots(ertm_ctx *ctx, const ertm_shot *shots, int nshots, const float *r_vp,
+                            const float *r_vs, const float *r_rho, float *data_out);
+int ertm_born_adjoint_shots(ertm_ctx *ctx, const ertm_shot *shots, int nshots,
+                            const float *residual, float *g_vp, float *g_vs, float *g_rho);
 
 /* ---- inspection (the reference's output_3d_wavefiled_* / EA outputs,
  *      3D_output_file.cu:2-250) ------------------------------------------ */
