@@ -31,6 +31,7 @@ TRUE_MODEL, MIGRATION_MODEL = 0, 1
 BOUNDARY_CPML, BOUNDARY_SPONGE_COS, BOUNDARY_SPONGE_CUBIC = 0, 1, 2
 COEF_TAYLOR, COEF_REFERENCE12, COEF_USER = 0, 1, 2
 INJECT_ADD, INJECT_REPLACE = 1, 2
+STEP_PAIRS, STEP_SINGLE = 0, 1
 FIELDS = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz", "tp", "vxp", "vyp", "vzp")
 ERRORS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENOTSUP",
           -6: "EDEVICE"}
@@ -102,6 +103,7 @@ SIGNATURES = {
     "ertm_time_kernels": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(C.c_float)]),
     "ertm_kernel_launches": (C.c_int64, [_P]),
     "ertm_set_wait_fault": (C.c_int, [_P, C.c_int, C.c_uint32]),
+    "ertm_set_step_variant": (C.c_int, [_P, C.c_int]),
     "ertm_born_forward": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_adjoint": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_born_forward_shots": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, _P, _P, _P, _P]),
@@ -534,6 +536,10 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self._L.ertm_kernel_launches(self._h))
+
+    def set_step_variant(self, variant: int):
+        """3D step kernels: STEP_PAIRS (two cells per thread, default) or STEP_SINGLE."""
+        self._ck(self._L.ertm_set_step_variant(self._h, int(variant)))
 
     def set_wait_fault(self, plane: int = -1, polls: int = 0):
         """Test hook of the device-error path: the first CTA of each step kernel skips

@@ -623,10 +623,14 @@ def main():
                                        dt_ms=wl.dt_ms, nt=wl.nt, order=8, pml=(wl.pml,) * 6,
                                        device=local))
         ctx.set_model(ertm.MIGRATION_MODEL, wl.svp, wl.svs, wl.srho)
-        ms = ctx.time_kernels(_shot(ertm, wl, synth, 0), args.kernel_steps)
-        print(json.dumps({"workload": wl.name, "cells": cells, "steps": args.kernel_steps,
-                          "ms_per_launch": [m / args.kernel_steps for m in ms],
-                          "gcells": [cells / (m / args.kernel_steps) / 1e6 for m in ms]}))
+        out = {"workload": wl.name, "cells": cells, "steps": args.kernel_steps}
+        for name, variant in (("pairs", ertm.STEP_PAIRS), ("single_cell", ertm.STEP_SINGLE)):
+            ctx.set_step_variant(variant)
+            ctx.time_kernels(_shot(ertm, wl, synth, 0), 2)          # warm-up launches
+            ms = ctx.time_kernels(_shot(ertm, wl, synth, 0), args.kernel_steps)
+            out[name] = {"ms_per_launch": [m / args.kernel_steps for m in ms],
+                         "gcells": [cells / (m / args.kernel_steps) / 1e6 for m in ms]}
+        print(json.dumps(out))
         ctx.close()
         return
     cfg = ertm.Config(nx=nx, ny=ny, nz=nz, dx=wl.dx, dy=wl.dy, dz=wl.dz, dt_ms=wl.dt_ms,
