@@ -31,7 +31,7 @@ TRUE_MODEL, MIGRATION_MODEL = 0, 1
 BOUNDARY_CPML, BOUNDARY_SPONGE_COS, BOUNDARY_SPONGE_CUBIC = 0, 1, 2
 COEF_TAYLOR, COEF_REFERENCE12, COEF_USER = 0, 1, 2
 INJECT_ADD, INJECT_REPLACE = 1, 2
-STEP_PAIRS, STEP_SINGLE = 0, 1
+STEP_SINGLE, STEP_PAIRS = 0, 1
 FIELDS = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz", "tp", "vxp", "vyp", "vzp")
 ERRORS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENOTSUP",
           -6: "EDEVICE"}
@@ -538,7 +538,7 @@ class Context:
         return int(self._L.ertm_kernel_launches(self._h))
 
     def set_step_variant(self, variant: int):
-        """3D step kernels: STEP_PAIRS (two cells per thread, default) or STEP_SINGLE."""
+        """3D step kernels: STEP_SINGLE (one cell per thread, default) or STEP_PAIRS."""
         self._ck(self._L.ertm_set_step_variant(self._h, int(variant)))
 
     def set_wait_fault(self, plane: int = -1, polls: int = 0):

@@ -101,8 +101,8 @@ struct ertm_ctx {
     // test hook of the device-error path (ertm_set_wait_fault)
     int skip_plane1 = 0;
     unsigned wait_polls = 0;
-    // 3D step-kernel variant (ertm_set_step_variant): 0 cell pairs, 1 one cell per thread
-    int single_cell = 0;
+    // 3D step-kernel variant (ertm_set_step_variant): 0 one cell per thread, 1 cell pairs
+    int pairs = 0;
 
     std::string err;
     long long launches = 0;
@@ -487,7 +487,7 @@ void fill_args(ertm_ctx* c, int which, const ertm_shot* s, KArgs& a)
     a.err = c->err_d;
     a.skip_plane1 = c->skip_plane1;
     a.wait_polls = c->wait_polls;
-    a.single_cell = c->single_cell;
+    a.pairs = c->pairs;
 }
 
 int check_device_error(ertm_ctx* c)
@@ -1264,7 +1264,7 @@ int ertm_set_step_variant(ertm_ctx* c, int variant)
     if (!c) return ERTM_EINVAL;
     if (variant != ERTM_STEP_PAIRS && variant != ERTM_STEP_SINGLE)
         return fail(c, ERTM_EINVAL, "step variant %d", variant);
-    c->single_cell = variant == ERTM_STEP_SINGLE;
+    c->pairs = variant == ERTM_STEP_PAIRS;
     return ERTM_OK;
 }
 

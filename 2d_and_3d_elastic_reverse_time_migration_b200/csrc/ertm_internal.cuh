@@ -88,8 +88,8 @@ struct KArgs {
     // (wait_polls polls; 0 = kWaitPolls) runs out
     int skip_plane1;
     unsigned wait_polls;
-    // 3D step-kernel variant: 0 = cell pairs (default), 1 = one cell per thread
-    int single_cell;
+    // 3D step-kernel variant: 0 = one cell per thread (default), 1 = cell pairs
+    int pairs;
 };
 
 // Device error codes written to KArgs::err

@@ -4,8 +4,7 @@
 // chunks as k_stress / k_velocity (step_kernels.cuh), but each consumer thread
 // updates two x-adjacent cells: a warp covers two rows of the 32 x 8 tile
 // (16 lanes x 2 cells each), so a CTA has TYB/2 consumer warps plus the producer
-// warp.  What the pairing buys is fewer instructions per cell, the resource the
-// single-cell kernels run short of next to HBM bandwidth:
+// warp.  The pairing cuts instructions per cell:
 //   * every shared-memory read of the staged planes is a 64-bit load: the x
 //     stencils read their 2R+2-wide window once for both cells, the y stencils
 //     and the per-cell values one float2 per row;
@@ -14,12 +13,18 @@
 //     the loaded window;
 //   * z queues hold float2, loop control, waits, releases and stores (64-bit)
 //     are shared by two cells.
-// Per cell the arithmetic is that of the single-cell kernels in the same order:
-// a difference a - b is fma(-1, b, a) (one rounding, as a subtraction), each tap
-// is fma(c_n, difference, sum), so results agree bit for bit.  The memory
+// Per cell the stencil arithmetic is that of the single-cell kernels in the same
+// order: a difference a - b is fma(-1, b, a) (one rounding, as a subtraction),
+// each tap is fma(c_n, difference, sum); the compiler may fuse the update's
+// products differently, so results agree to float rounding.  The memory
 // variables of the C-PML, the source, receivers and the excitation / imaging
 // epilogue are handled cell by cell.  2D grids keep the single-cell kernels (one
-// tile row only).
+// tile row only).  Measured on B200 at 480 x 480 x 380 (R = 4, C-PML, source
+// pass) the pairs are slower than the single-cell kernels (stress 1.517 against
+// 1.447 ms, velocity 1.658 against 1.615 ms): those already move their DRAM
+// traffic at ~89 % of the copy bandwidth, and half as many warps per SM hide
+// less latency.  They stay an option (ertm_set_step_variant); the single-cell
+// kernels are the default.
 #pragma once
 
 #include "step_kernels.cuh"
@@ -783,13 +788,13 @@ static cudaError_t launch_velocity_pair(dim3 grid, const VelMaps& m, const KArgs
         grid, block, VelShape<R, true, C, EPI_NONE>::BYTES, m, a, st);
 }
 
-// 3D grids: the pair kernels (the single-cell kernels when KArgs::single_cell is set);
+// 3D grids: the pair kernels when KArgs::pairs is set, else the single-cell kernels;
 // 2D grids: the single-cell kernels (one tile row)
 template <int R>
 cudaError_t launch_stress_any(const Geom& g, const KArgs& a, const StressMaps& m, bool cpml, bool ps,
                               cudaStream_t st)
 {
-    if (g.two_d || a.single_cell) return launch_stress_t<R>(g, a, m, cpml, ps, st);
+    if (g.two_d || !a.pairs) return launch_stress_t<R>(g, a, m, cpml, ps, st);
     const dim3 grid = step_grid(g, a, TY3);
     if (cpml) return ps ? launch_stress_pair<R, true, true>(grid, m, a, st)
                         : launch_stress_pair<R, true, false>(grid, m, a, st);
@@ -801,7 +806,7 @@ template <int R>
 cudaError_t launch_velocity_any(const Geom& g, const KArgs& a, const VelMaps& m, bool cpml, int epi,
                                 bool rec, cudaStream_t st)
 {
-    if (g.two_d || a.single_cell) return launch_velocity_t<R>(g, a, m, cpml, epi, rec, st);
+    if (g.two_d || !a.pairs) return launch_velocity_t<R>(g, a, m, cpml, epi, rec, st);
     const dim3 grid = step_grid(g, a, TY3);
     return cpml ? launch_velocity_pair<R, true>(grid, m, a, epi, rec, st)
                 : launch_velocity_pair<R, false>(grid, m, a, epi, rec, st);

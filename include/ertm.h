@@ -256,12 +256,13 @@ int ertm_time_kernels(ertm_ctx *ctx, const ertm_shot *shot, int nsteps, float *m
 /* Number of kernels this context has launched (for launch accounting). */
 int64_t ertm_kernel_launches(const ertm_ctx *ctx);
 
-/* Variant of the 3D step kernels (both compute the same numbers): two x-adjacent
- * cells per thread with packed FP32 pairs (the default), or one cell per thread.
- * No counterpart in the reference; for measurement and equivalence tests.  2D
- * grids always use one cell per thread. */
-#define ERTM_STEP_PAIRS   0
-#define ERTM_STEP_SINGLE  1
+/* Variant of the 3D step kernels (both compute the same numbers to float
+ * rounding): one cell per thread (the default, the faster on B200) or two
+ * x-adjacent cells per thread with packed FP32 pairs.  No counterpart in the
+ * reference; for measurement and equivalence tests.  2D grids always use one
+ * cell per thread. */
+#define ERTM_STEP_SINGLE  0
+#define ERTM_STEP_PAIRS   1
 int ertm_set_step_variant(ertm_ctx *ctx, int variant);
 
 /* Test hook of the device-error path.  No counterpart in the reference (it
