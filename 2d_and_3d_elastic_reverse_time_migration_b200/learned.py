@@ -64,7 +64,7 @@ def make_case(seed: int, g: Geometry, device: int = 0, checkpoint_every: int = 1
     xs = np.linspace(g.pml + 4, nx - g.pml - 5, g.nshots).round().astype(int)
     rz = g.pml + 2
     shots = [Shot(int(x), 0, rz, wavelet=w, rx0=g.pml, nrx=nx - 2 * g.pml, drx=1, rz=rz) for x in xs]
-    data = [ctx.born_forward(s, *true) for s in shots]
+    data = list(ctx.born_forward_shots(shots, *true))   # every shot in one batched call
     return Case(ctx, shots, data, true, vp.shape)
 
 

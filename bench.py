@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--train-models", type=int, default=48)
     ap.add_argument("--test-models", type=int, default=6)
     ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--lsrtm-geometry", default="small", choices=["small", "patch"],
+                    help="lsrtm workload: small = 128x64 cells, 6 shots, 500 steps, 64x128 patches; "
+                         "patch = 512x256 cells at 5 m, 8 shots, 2000 steps, one 256x512 patch per model")
+    ap.add_argument("--train-batch", type=int, default=16)
     ap.add_argument("--shots", type=int, default=64, help="windows workload: shots")
     ap.add_argument("--lanes", type=int, default=4, help="windows workload: shots in flight")
     ap.add_argument("--cg-iters", type=int, default=20, help="lsrtm-cg workload: CG iterations")
@@ -326,16 +330,29 @@ def run_lsrtm(args):
     nn = importlib.import_module(PKG + ".nn")
     L = importlib.import_module(PKG + ".learned")
     dev = torch.device("cuda", 0)
-    geo = L.Geometry()
+    if args.lsrtm_geometry == "patch":
+        # the LSRTM workload's 5 m cells and generator, cut to one 256 x 512 training
+        # patch per model (512 x 256 interior + 40-cell sponge), 8 shots, 2000 steps
+        geo = L.Geometry(nzi=256, nxi=512, h=5.0, pml=40, nt=2000, dt_ms=0.5, nshots=8, f0=15.0,
+                         sigma=10.0)
+        patch = (256, 512)
+    else:
+        geo = L.Geometry()
+        patch = (64, 128)
     t0 = time.perf_counter()
     pairs = []
     for k in range(args.train_models):
         case = L.make_case(1000 + k, geo)
         pairs.append(L.training_pair(case, cg_iters=10))
         case.ctx.close()
+        if k in (0, 3) or (k + 1) % 16 == 0:
+            print(json.dumps({"event": "training_pairs", "done": k + 1,
+                              "seconds": round(time.perf_counter() - t0, 1)}), flush=True)
     t_data = time.perf_counter() - t0
     net = nn.UNet(dev, seed=0)
-    log = L.train(net, pairs, steps=args.train_steps, batch=16, patch=(64, 128), lr=1e-3)
+    log = L.train(net, pairs, steps=args.train_steps, batch=args.train_batch, patch=patch, lr=1e-3)
+    print(json.dumps({"event": "trained", "seconds": round(log.seconds, 1),
+                      "loss_first_last": [log.loss[0][1], log.loss[-1][1]]}), flush=True)
     target, niter = 1e-2, 20
     rows = []
     for k in range(args.test_models):
@@ -348,7 +365,8 @@ def run_lsrtm(args):
     print(json.dumps({
         "metric": "LSRTM: learned vs plain CG (iterations and wall time to plain CG's 20-iteration misfit, and to 1e-2)",
         "unit": "iterations / s", "config": {"grid": f"{geo.nxi}x{geo.nzi} + sponge {geo.pml}",
-                                           "shots": geo.nshots, "nt": geo.nt,
+                                           "dx": geo.h, "shots": geo.nshots, "nt": geo.nt,
+                                           "patch": list(patch), "batch": args.train_batch,
                                            "train_models": args.train_models,
                                            "test_models": args.test_models,
                                            "train_steps": args.train_steps, "cg_iters_target": 10},
