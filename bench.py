@@ -42,7 +42,7 @@ COMPULSORY_B = 84
 # DRAM bytes per cell of each source-pass step kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum, one ncu capture per kernel on the 240 x 240 x 190 grid with a
 # 20-cell C-PML: the same slab fractions as the 3D workload)
-TRAFFIC_B_PER_CELL = {"stress": 95.3, "velocity": 105.3}
+TRAFFIC_B_PER_CELL = {"stress": 96.2, "velocity": 107.9}
 
 
 def parse():
