@@ -55,3 +55,44 @@ def test_windows_equal_per_window_contexts(ertm, orc, two_d):
             assert scale > 0
             err = np.abs(out[k][ok] - r[ok]).max() / scale
             assert err < 1e-5, (lanes, k, err)
+
+
+def test_windows_match_the_oracle(ertm, orc):
+    """The batched path against the FP64 oracle: two non-overlapping 2D windows, the
+    oracle's modelling, source and receiver passes on each window's cropped and
+    padded model, its images placed into the stack; compared on the cells whose
+    excitation is tie-free (as the parity tests do), relative L2 1e-4."""
+    shape = (40, 1, 160)
+    nz, ny, nx = shape
+    true = shared_model(shape, seed=5)
+    wins = [ertm.Window(6, 0, 60, 1, 220), ertm.Window(90, 0, 56, 1, 200)]
+    w = orc.ricker(25.0, DT_MS / 1000.0)
+    shots, data = [], []
+    ref = [np.zeros(shape) for _ in range(3)]
+    clear = np.zeros(shape, bool)
+    for win in wins:
+        m = [crop_pad(a, win.x0, 0, win.wx, 1, PML, True) for a in true]
+        wnz, _, wnx = m[0].shape
+        s = dict(sx=win.x0 + win.wx // 2, sy=0, sz=2, rx0=win.x0, nrx=(win.wx + 1) // 2, drx=2,
+                 ry0=0, nry=1, dry=2, rz=2)
+        g = orc.make_grid(wnx, 1, wnz, 10.0, 10.0, 10.0, DT_MS, R=4, boundary=orc.CPML,
+                          pml=(PML, PML, 0, 0, PML, PML), pml_vmax=float(m[0].max()))
+        osh = orc.make_shot(s["sx"] - win.x0 + PML, 0, s["sz"] + PML, w, rx0=s["rx0"] - win.x0 + PML,
+                            nrx=s["nrx"], drx=2, rz=s["rz"] + PML)
+        d = orc.run_pass(g, *m, osh, orc.MODEL, win.nt)["data"]
+        nsrc = 2 * win.nt // 3
+        ex = orc.run_pass(g, *m, osh, orc.SOURCE, nsrc)["ex"]
+        r = orc.run_pass(g, *m, osh, orc.RECEIVER, win.nt, data=d, ex=ex)
+        ok = (ex.amp2 - ex.second2 > 2e-4 * ex.amp2) & (ex.amp2 > 1e-4 * np.percentile(ex.amp2, 99))
+        for k, name in enumerate(("pp", "ps")):
+            ref[k][:, :, win.x0:win.x0 + win.wx] = r[name][PML:PML + nz, :, PML:PML + win.wx]
+        clear[:, :, win.x0:win.x0 + win.wx] = ok[PML:PML + nz, :, PML:PML + win.wx]
+        shots.append(ertm.Shot(s["sx"], 0, s["sz"], wavelet=w, rx0=s["rx0"], nrx=s["nrx"], drx=2, rz=s["rz"]))
+        data.append(d)
+    base = config(ertm, nx, ny, nz, 1, True)
+    out = ertm.rtm_windows(base, *true, wins, shots, data, lanes=2)
+    assert clear.sum() > 1000
+    for k in range(2):
+        got, want = out[k][clear], ref[k][clear]
+        err = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+        assert err <= 1e-4, (k, err)
