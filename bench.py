@@ -433,8 +433,9 @@ def run_lsrtm_op(args):
     m = [torch.from_numpy(a).to(dev) for a in true]
     data = torch.zeros((len(shots), 3, g.nt, shots[0].nrec), device=dev)
     grads = [torch.zeros((nz, 1, nx), device=dev) for _ in range(3)]
-    ctx.born_forward_shots(shots[:1], *m, out=data[:1])          # warm-up: allocations
-    ctx.born_adjoint_shots(shots[:1], data[:1], *grads)
+    if args.warmup > 0:   # warm-up: allocations (--warmup 0 for profiling captures)
+        ctx.born_forward_shots(shots[:1], *m, out=data[:1])
+        ctx.born_adjoint_shots(shots[:1], data[:1], *grads)
     e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     torch.cuda.synchronize(dev)
     e[0].record(st)

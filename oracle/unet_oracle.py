@@ -21,6 +21,12 @@ intermediate gradients, the loss gradient) is rounded to BF16 at the same point
 (round to nearest even); sums and products stay float64.  With `bf16=False` it
 is the exact float64 network (for finite-difference checks of this file).
 Arrays are NHWC float64.
+
+`loss_grad` runs the whole network from the input; `replay` recomputes every
+layer from the values the kernels stored for its operands (buffer names of
+nn.py), so that a BF16 rounding which lands on the other side of a tie in one
+layer does not carry into the next and each layer can be checked to one BF16
+unit.
 """
 from __future__ import annotations
 
@@ -132,7 +138,9 @@ class Net:
 
     # ---- forward / loss / backward -------------------------------------------
     def loss_grad(self, x, target):
-        """x, target: (n, h, w, 3).  Returns (output (n, h, w, 3), loss, grads name -> (dw, db))."""
+        """x, target: (n, h, w, 3).  Returns (output (n, h, w, 3), loss, grads name -> (dw, db)).
+        The stored activations and gradients are kept in `self.stored` as (B, G)
+        under the buffer names of nn.py (the input of `replay`)."""
         r = self.r
         n, h, w, _ = x.shape
         relu = lambda a: np.maximum(a, 0.0)
@@ -169,13 +177,16 @@ class Net:
 
         G = {}
         grads = {}
+        SG = {"out": gout}
         grads["out"] = self._conv_dw(A["d0b"], gout)
         g = r(self._conv_dx(gout, wo, LEVELS[0]) * (A["d0b"] > 0))
+        SG["d0b"] = g
         for l in (0, 1, 2):
             c = LEVELS[l]
             wb, _ = self._W(f"d{l}b")
             grads[f"d{l}b"] = self._conv_dw(A[f"d{l}a"], g)
             g = r(self._conv_dx(g, wb, c) * (A[f"d{l}a"] > 0))
+            SG[f"d{l}a"] = g
             wa, _ = self._W(f"d{l}a")
             grads[f"d{l}a"] = self._conv_dw(A[f"cat{l}"], g)
             gcat = r(self._conv_dx(g, wa, 2 * c) * (A[f"cat{l}"] > 0))
@@ -185,6 +196,7 @@ class Net:
             wu, _ = self._W(f"u{l}")
             grads[f"u{l}"] = self._up_dw(src, gup, c)
             g = r(self._up_dx(gup, wu, c, src.shape[3]) * (src > 0))
+            SG["e3b" if l == 2 else f"d{l + 1}b"] = g
         # g is now the gradient at e3b
         for l in (3, 2, 1, 0):
             c = LEVELS[l]
@@ -193,11 +205,91 @@ class Net:
             else:
                 # the skip gradient (from cat) plus the pooled path, summed in BF16 storage
                 geb = r(G[f"cat{l}"][..., c:] + self._pool_back(A[f"e{l}b"], gin))
+                SG[f"cat{l}"] = np.concatenate([G[f"cat{l}"][..., :c], geb], axis=3)
             wb, _ = self._W(f"e{l}b")
             grads[f"e{l}b"] = self._conv_dw(A[f"e{l}a"], geb)
             gea = r(self._conv_dx(geb, wb, c) * (A[f"e{l}a"] > 0))
+            SG[f"e{l}a"] = gea
             wa, _ = self._W(f"e{l}a")
             grads[f"e{l}a"] = self._conv_dw(A[f"in{l}"], gea)
             if l > 0:
                 gin = r(self._conv_dx(gea, wa, A[f"in{l}"].shape[3]))
+                SG[f"in{l}"] = gin
+        SB = {k: v for k, v in A.items() if not (k.startswith("e") and k.endswith("b") and k != "e3b")}
+        SB["out"] = y
+        self.stored = (SB, SG)
         return y[..., :OUT_C], loss, grads
+
+    # ---- layer-by-layer replay --------------------------------------------
+    def replay(self, B, G, target):
+        """B, G: the kernels' stored activation and gradient buffers (nn.py names; the
+        BF16 values as float64; B["out"] the FP32 output), target (n, h, w, 3).
+        Returns (acts, grads, wgrads): the value of every stored buffer recomputed
+        from the stored values it is made of (the encoder half of cat{l} under
+        "cat{l}_enc", the up-sampled half under "cat{l}_up"), and the weight and
+        bias gradients of every layer from the stored operands."""
+        r = self.r
+        relu = lambda a: np.maximum(a, 0.0)
+        A, Gr, W = {}, {}, {}
+        for l, c in enumerate(LEVELS):
+            wa, ba = self._W(f"e{l}a")
+            wb, bb = self._W(f"e{l}b")
+            A[f"e{l}a"] = r(relu(self._conv(B[f"in{l}"], wa, ba)))
+            eb = r(relu(self._conv(B[f"e{l}a"], wb, bb)))
+            if l < 3:
+                A[f"cat{l}_enc"] = eb
+                A[f"in{l + 1}"] = self._pool(B[f"cat{l}"][..., c:])
+            else:
+                A["e3b"] = eb
+        for l in (2, 1, 0):
+            c = LEVELS[l]
+            src = B["e3b"] if l == 2 else B[f"d{l + 1}b"]
+            wu, bu = self._W(f"u{l}")
+            A[f"cat{l}_up"] = r(relu(self._up(src, wu, bu, c)))
+            wa, ba = self._W(f"d{l}a")
+            A[f"d{l}a"] = r(relu(self._conv(B[f"cat{l}"], wa, ba)))
+            wb, bb = self._W(f"d{l}b")
+            A[f"d{l}b"] = r(relu(self._conv(B[f"d{l}a"], wb, bb)))
+        wo, bo = self._W("out")
+        A["out"] = self._conv(B["d0b"], wo, bo)
+
+        y = B["out"]
+        n, h, w, _ = y.shape
+        cnt = n * h * w * OUT_C
+        d = np.zeros_like(y)
+        d[..., :OUT_C] = y[..., :OUT_C] - target
+        Gr["out"] = r(2.0 / cnt * d)
+        W["out"] = self._conv_dw(B["d0b"], G["out"])
+        Gr["d0b"] = r(self._conv_dx(G["out"], wo, LEVELS[0]) * (B["d0b"] > 0))
+        skip = {}
+        for l in (0, 1, 2):
+            c = LEVELS[l]
+            wb, _ = self._W(f"d{l}b")
+            W[f"d{l}b"] = self._conv_dw(B[f"d{l}a"], G[f"d{l}b"])
+            Gr[f"d{l}a"] = r(self._conv_dx(G[f"d{l}b"], wb, c) * (B[f"d{l}a"] > 0))
+            wa, _ = self._W(f"d{l}a")
+            W[f"d{l}a"] = self._conv_dw(B[f"cat{l}"], G[f"d{l}a"])
+            gcat = r(self._conv_dx(G[f"d{l}a"], wa, 2 * c) * (B[f"cat{l}"] > 0))
+            Gr[f"cat{l}_up"] = gcat[..., :c]
+            skip[l] = gcat[..., c:]
+            sname = "e3b" if l == 2 else f"d{l + 1}b"
+            src = B[sname]
+            wu, _ = self._W(f"u{l}")
+            gup = G[f"cat{l}"][..., :c]
+            W[f"u{l}"] = self._up_dw(src, gup, c)
+            Gr[sname] = r(self._up_dx(gup, wu, c, src.shape[3]) * (src > 0))
+        for l in (3, 2, 1, 0):
+            c = LEVELS[l]
+            if l == 3:
+                geb = G["e3b"]
+            else:
+                Gr[f"cat{l}_enc"] = r(skip[l] + self._pool_back(B[f"cat{l}"][..., c:], G[f"in{l + 1}"]))
+                geb = G[f"cat{l}"][..., c:]
+            wb, _ = self._W(f"e{l}b")
+            W[f"e{l}b"] = self._conv_dw(B[f"e{l}a"], geb)
+            Gr[f"e{l}a"] = r(self._conv_dx(geb, wb, c) * (B[f"e{l}a"] > 0))
+            wa, _ = self._W(f"e{l}a")
+            W[f"e{l}a"] = self._conv_dw(B[f"in{l}"], G[f"e{l}a"])
+            if l > 0:
+                Gr[f"in{l}"] = r(self._conv_dx(G[f"e{l}a"], wa, B[f"in{l}"].shape[3]))
+        return A, Gr, W

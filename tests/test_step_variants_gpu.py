@@ -10,7 +10,10 @@ cell lies outside the grid), both stencil radii and both boundary kinds.
 Tolerances: relative L2 1e-5 on traces and wavefields (the bound both variants
 meet against the FP64 oracle; measured 1e-6 to 4e-6 between them after 220
 steps), the excitation time equal on at least 99.9 % of the excited cells, the
-images 1e-5 on those cells.
+PP and PS images 1e-5 on those cells, the TP image (r_tp / e_tp, ill-conditioned
+where the excitation P stress crosses zero: 9.7e-4 measured over all excited
+cells) 1e-4, the image bound of the parity tests, on those whose |e_tp| is above
+1e-3 of its 99th percentile.
 """
 import numpy as np
 import pytest
@@ -52,8 +55,10 @@ def test_pair_and_single_cell_kernels_agree(ertm, orc, case):
     same = a[3]["time"] == b[3]["time"]
     assert same[excited].mean() > 0.999, same[excited].mean()
     m = excited & same
-    for q in range(3):
-        assert rel(a[2][q][m], b[2][q][m]) <= 1e-5, ("image", q)
+    etp = np.abs(b[3]["etp"].astype(np.float64))
+    tp_ok = m & (etp > 1e-3 * np.percentile(etp[m], 99))
+    for q, mask, tol in ((0, m, 1e-5), (1, m, 1e-5), (2, tp_ok, 1e-4)):
+        assert rel(a[2][q][mask], b[2][q][mask]) <= tol, ("image", q, rel(a[2][q][mask], b[2][q][mask]))
 
 
 def test_step_variant_argument_checked(ertm):

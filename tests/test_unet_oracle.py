@@ -69,3 +69,42 @@ def test_bf16_rounding_matches_torch():
     v = np.random.default_rng(3).standard_normal(10000) * 10.0 ** np.random.default_rng(4).integers(-20, 20, 10000)
     ref = torch.from_numpy(v.astype(np.float32)).bfloat16().float().numpy().astype(np.float64)
     assert np.array_equal(U.to_bf16(v), ref)
+
+
+@pytest.mark.parametrize("bf16", [True, False])
+def test_replay_reproduces_the_whole_network(bf16):
+    """Fed the buffers the whole-network pass stored, the layer-by-layer replay
+    recomputes every one of them and every weight gradient exactly."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import unet_oracle as U
+    rng = np.random.default_rng(12)
+    P = _params(rng)
+    x = rng.standard_normal((2, 16, 24, 3))
+    t = rng.standard_normal((2, 16, 24, 3))
+    net = U.Net(P, bf16=bf16)
+    _, _, grads = net.loss_grad(x, t)
+    B, G = net.stored
+    A, Gr, W = net.replay(B, G, t)
+    for k, v in A.items():
+        if k.endswith("_enc"):
+            want = B[k[:-4]][..., U.LEVELS[int(k[3])]:]
+        elif k.endswith("_up"):
+            want = B[k[:-3]][..., :U.LEVELS[int(k[3])]]
+        else:
+            want = B[k]
+        assert np.array_equal(v, want), k
+    for k, v in Gr.items():
+        if k.endswith("_enc"):
+            want = G[k[:-4]][..., U.LEVELS[int(k[3])]:]
+        elif k.endswith("_up"):
+            want = G[k[:-3]][..., :U.LEVELS[int(k[3])]]
+        else:
+            want = G[k]
+        assert np.array_equal(v, want), k
+    assert set(W) == set(grads)
+    for k in W:
+        assert np.array_equal(W[k][0], grads[k][0]) and np.array_equal(W[k][1], grads[k][1]), k
+    names = {k.split("_")[0] for k in list(A) + list(Gr)}
+    assert {"e0a", "e3b", "cat0", "cat2", "in3", "d0b", "out"} <= names
