@@ -54,36 +54,55 @@ __device__ __forceinline__ float dmx(const float* __restrict__ f, long long c, c
     for (int n = 1; n <= R; n++) s = fmaf(a.cx[n], __ldg(f + c + n - 1) - __ldg(f + c - n), s);
     return s;
 }
+// Rows k-R .. k+R of one field at the thread's column, carried down the warp's z
+// chunk: each row is loaded once (one aligned 128-byte line per warp) and every
+// z stencil reads registers.  dpz / dmz are the forward / backward z differences
+// at row k with the same terms in the same order as the x differences above.
 template <int R>
-__device__ __forceinline__ float dpz(const float* __restrict__ f, long long c, const BornArgs& a)
-{
-    const long long p = a.px;
-    float s = 0.f;
+struct ZWin {
+    float w[2 * R + 1];
+    template <typename F>
+    __device__ __forceinline__ void init(F f, long long c, long long p)
+    {
 #pragma unroll
-    for (int n = 1; n <= R; n++) s = fmaf(a.cz[n], __ldg(f + c + n * p) - __ldg(f + c - (n - 1) * p), s);
-    return s;
-}
-template <int R>
-__device__ __forceinline__ float dmz(const float* __restrict__ f, long long c, const BornArgs& a)
-{
-    const long long p = a.px;
-    float s = 0.f;
+        for (int j = 0; j <= 2 * R; j++) w[j] = f(c + (long long)(j - R) * p);
+    }
+    // c: the next row's cell
+    template <typename F>
+    __device__ __forceinline__ void shift(F f, long long c, long long p)
+    {
 #pragma unroll
-    for (int n = 1; n <= R; n++) s = fmaf(a.cz[n], __ldg(f + c + (n - 1) * p) - __ldg(f + c - n * p), s);
-    return s;
-}
+        for (int j = 0; j < 2 * R; j++) w[j] = w[j + 1];
+        w[2 * R] = f(c + (long long)R * p);
+    }
+    __device__ __forceinline__ float dpz(const float* cz) const
+    {
+        float s = 0.f;
+#pragma unroll
+        for (int n = 1; n <= R; n++) s = fmaf(cz[n], w[R + n] - w[R - n + 1], s);
+        return s;
+    }
+    __device__ __forceinline__ float dmz(const float* cz) const
+    {
+        float s = 0.f;
+#pragma unroll
+        for (int n = 1; n <= R; n++) s = fmaf(cz[n], w[R + n - 1] - w[R - n], s);
+        return s;
+    }
+};
 
-// products of neighbours for the transposed stencils: f(c) = p(c - zo) q(c - zo) w(c),
-// p and q shared by the shots of a launch, w the shot's own volume (offset zo)
-struct Prod2 {
+// read-only field (not written by the kernel that reads it)
+struct Ld {
     const float* p;
-    const float* q;
+    __device__ __forceinline__ float operator()(long long c) const { return __ldg(p + c); }
+};
+// product of the shared B g1 (shot-independent, index c - zo) and the shot's own
+// field w: the velocity update's transposed operand
+struct Prod {
+    const float* bg;
     const float* w;
     long long zo;
-    __device__ __forceinline__ float operator()(long long c) const
-    {
-        return __ldg(p + (c - zo)) * __ldg(q + (c - zo)) * w[c];
-    }
+    __device__ __forceinline__ float operator()(long long c) const { return __ldg(bg + (c - zo)) * __ldg(w + c); }
 };
 template <int R, typename F>
 __device__ __forceinline__ float tdpx(F f, long long c, const BornArgs& a)
@@ -101,23 +120,29 @@ __device__ __forceinline__ float tdmx(F f, long long c, const BornArgs& a)
     for (int n = 1; n <= R; n++) s = fmaf(a.cx[n], f(c + n - 1) - f(c - n), s);
     return s;
 }
-template <int R, typename F>
-__device__ __forceinline__ float tdpz(F f, long long c, const BornArgs& a)
+
+// Work of one warp: a strip of 32 allocated columns (cells i = 32 w + lane - BXH, so
+// every row access is one aligned 128-byte line) and a chunk of a.kc rows, marched
+// top to bottom; blockIdx.z is the shot.  Lanes outside the grid (i < 0 or
+// i >= nx: zero halo columns) load and compute like the others and store nothing.
+constexpr int WPB = 4;       // warps per block: adjacent strips
+struct Strip {
+    int i, k0, k1;
+    bool act;                // the lane's cell is inside the grid
+    long long c;             // cell (i, k0) of the shared volumes
+    long long zo;            // shot offset of the per-shot volumes
+};
+__device__ __forceinline__ bool strip_of(const BornArgs& a, Strip& s)
 {
-    const long long p = a.px;
-    float s = 0.f;
-#pragma unroll
-    for (int n = 1; n <= R; n++) s = fmaf(a.cz[n], f(c + n * p) - f(c - (n - 1) * p), s);
-    return s;
-}
-template <int R, typename F>
-__device__ __forceinline__ float tdmz(F f, long long c, const BornArgs& a)
-{
-    const long long p = a.px;
-    float s = 0.f;
-#pragma unroll
-    for (int n = 1; n <= R; n++) s = fmaf(a.cz[n], f(c + (n - 1) * p) - f(c - n * p), s);
-    return s;
+    const int w = blockIdx.x * WPB + threadIdx.y;
+    s.k0 = blockIdx.y * a.kc;
+    if (32 * w - BXH >= a.nx || s.k0 >= a.nz) return false;
+    s.k1 = min(s.k0 + a.kc, a.nz);
+    s.i = 32 * w + (int)threadIdx.x - BXH;
+    s.act = s.i >= 0 && s.i < a.nx;
+    s.c = (long long)(s.k0 + a.R) * a.px + 32 * w + threadIdx.x;
+    s.zo = (long long)blockIdx.z * a.ss;
+    return true;
 }
 
 // cell (i, k) of the launch's shot blockIdx.z: c indexes the shared volumes,
@@ -157,104 +182,160 @@ __device__ __forceinline__ void iso(float m, float u, float exx, float ezz, floa
 
 // ---- forward ---------------------------------------------------------------
 template <int R, bool BORN, int NM>
-__global__ void k_born_stress(BornArgs a, int it)
+__global__ void __launch_bounds__(32 * WPB) k_born_stress(BornArgs a, int it)
 {
-    int i, k;
-    long long c, zo;
-    if (!cell_of(a, i, k, c, zo)) return;
-    const long long cz = c + zo;
+    Strip S;
+    if (!strip_of(a, S)) return;
+    const long long p = a.px, zo = S.zo;
     const float dt = a.dt;
-    const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
-    const float *v0x = a.v0x + zo, *v0z = a.v0z + zo;
-    const float e0xx = dpx<R>(v0x, c, a), e0zz = dmz<R>(v0z, c, a);
-    const float e0xz = dpz<R>(v0x, c, a) + dmx<R>(v0z, c, a);
-    float o[3] = {a.s0xx[cz], a.s0zz[cz], a.s0xz[cz]};
-    if (it >= 0 && it < a.nw && i == shot_par(a, 0) && k == shot_par(a, 1)) {
-        // explosive source into the background
-        const float w = __ldg(a.wavelet + (long long)blockIdx.z * a.wstride + it);
-        o[0] += w;
-        o[1] += w;
-    }
-    float E0[3], F0[3];
-    iso(pi * a.kp, mu * a.ks, e0xx, e0zz, e0xz, E0);
-    if (NM) iso(pi * a.tp, mu * a.ts, e0xx, e0zz, e0xz, F0);
-    float* s0[3] = {a.s0xx, a.s0zz, a.s0xz};
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-        float sum = 0.f;
-#pragma unroll
-        for (int l = 0; l < NM; l++) {
-            float* r = a.r0[q * 3 + l];
-            const float v = a.ra[l] * r[cz] + a.rb[l] * F0[q];
-            r[cz] = v;
-            sum += v;
-        }
-        s0[q][cz] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
-    }
+    const float* v0x = a.v0x + zo;
+    const float* v0z = a.v0z + zo;
+    const float* vx = a.vx + zo;
+    const float* vz = a.vz + zo;
+    // z windows: v0x and vx feed forward z differences, v0z and vz backward ones
+    ZWin<R> w0x, w0z, wx, wz;
+    w0x.init(Ld{v0x}, S.c, p);
+    w0z.init(Ld{v0z}, S.c, p);
     if (BORN) {
-        const float *vx = a.vx + zo, *vz = a.vz + zo;
-        const float exx = dpx<R>(vx, c, a), ezz = dmz<R>(vz, c, a);
-        const float exz = dpz<R>(vx, c, a) + dmx<R>(vz, c, a);
-        const float dpi = a.dM[c], dmu = a.dU[c];
-        float E[3], dE[3], F[3], dF[3];
-        iso(pi * a.kp, mu * a.ks, exx, ezz, exz, E);
-        // the reference's stress sources (dem_p), scaled by the GSLS strengths
-        iso(dpi * a.kp, dmu * a.ks, e0xx, e0zz, e0xz, dE);
-        if (NM) {
-            iso(pi * a.tp, mu * a.ts, exx, ezz, exz, F);
-            iso(dpi * a.tp, dmu * a.ts, e0xx, e0zz, e0xz, dF);
-        }
-        float* sc[3] = {a.sxx, a.szz, a.sxz};
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            float sum = 0.f;
-#pragma unroll
-            for (int l = 0; l < NM; l++) {
-                float* r = a.r[q * 3 + l];
-                const float v = a.ra[l] * r[cz] + a.rb[l] * (F[q] + dF[q]);
-                r[cz] = v;
-                sum += v;
+        wx.init(Ld{vx}, S.c, p);
+        wz.init(Ld{vz}, S.c, p);
+    }
+    const bool src_step = it >= 0 && it < a.nw;
+    const int sx = shot_par(a, 0), sz = shot_par(a, 1);
+    long long c = S.c;
+    for (int k = S.k0; k < S.k1; k++, c += p) {
+        const long long cz = c + zo;
+        const float e0xx = dpx<R>(v0x, c, a), e0zz = w0z.dmz(a.cz);
+        const float e0xz = w0x.dpz(a.cz) + dmx<R>(v0z, c, a);
+        if (S.act) {
+            const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
+            float o[3] = {a.s0xx[cz], a.s0zz[cz], a.s0xz[cz]};
+            if (src_step && S.i == sx && k == sz) {
+                // explosive source into the background
+                const float w = __ldg(a.wavelet + (long long)blockIdx.z * a.wstride + it);
+                o[0] += w;
+                o[1] += w;
             }
-            sc[q][cz] = g1 * (g2 * sc[q][cz] + dt * (E[q] + dE[q] + sum));
+            float E0[3], F0[3];
+            iso(pi * a.kp, mu * a.ks, e0xx, e0zz, e0xz, E0);
+            if (NM) iso(pi * a.tp, mu * a.ts, e0xx, e0zz, e0xz, F0);
+            float* s0[3] = {a.s0xx, a.s0zz, a.s0xz};
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                float sum = 0.f;
+#pragma unroll
+                for (int l = 0; l < NM; l++) {
+                    float* r = a.r0[q * 3 + l];
+                    const float v = a.ra[l] * r[cz] + a.rb[l] * F0[q];
+                    r[cz] = v;
+                    sum += v;
+                }
+                s0[q][cz] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
+            }
+            if (BORN) {
+                const float exx = dpx<R>(vx, c, a), ezz = wz.dmz(a.cz);
+                const float exz = wx.dpz(a.cz) + dmx<R>(vz, c, a);
+                const float dpi = a.dM[c], dmu = a.dU[c];
+                float E[3], dE[3], F[3], dF[3];
+                iso(pi * a.kp, mu * a.ks, exx, ezz, exz, E);
+                // the reference's stress sources (dem_p), scaled by the GSLS strengths
+                iso(dpi * a.kp, dmu * a.ks, e0xx, e0zz, e0xz, dE);
+                if (NM) {
+                    iso(pi * a.tp, mu * a.ts, exx, ezz, exz, F);
+                    iso(dpi * a.tp, dmu * a.ts, e0xx, e0zz, e0xz, dF);
+                }
+                float* sc[3] = {a.sxx, a.szz, a.sxz};
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    float sum = 0.f;
+#pragma unroll
+                    for (int l = 0; l < NM; l++) {
+                        float* r = a.r[q * 3 + l];
+                        const float v = a.ra[l] * r[cz] + a.rb[l] * (F[q] + dF[q]);
+                        r[cz] = v;
+                        sum += v;
+                    }
+                    sc[q][cz] = g1 * (g2 * sc[q][cz] + dt * (E[q] + dE[q] + sum));
+                }
+            }
+        }
+        if (k + 1 < S.k1) {
+            w0x.shift(Ld{v0x}, c + p, p);
+            w0z.shift(Ld{v0z}, c + p, p);
+            if (BORN) {
+                wx.shift(Ld{vx}, c + p, p);
+                wz.shift(Ld{vz}, c + p, p);
+            }
         }
     }
 }
 
 template <int R, bool BORN, bool KEEP>
-__global__ void k_born_velocity(BornArgs a, int it)
+__global__ void __launch_bounds__(32 * WPB) k_born_velocity(BornArgs a, int it)
 {
-    int i, k;
-    long long c, zo;
-    if (!cell_of(a, i, k, c, zo)) return;
-    const long long cz = c + zo;
+    Strip S;
+    if (!strip_of(a, S)) return;
+    const long long p = a.px, zo = S.zo;
     const float dt = a.dt;
-    const float g1 = a.g1[c], g2 = a.g2[c], b = a.B[c];
-    const float a0x = b * (dmx<R>(a.s0xx + zo, c, a) + dmz<R>(a.s0xz + zo, c, a));
-    const float a0z = b * (dpx<R>(a.s0xz + zo, c, a) + dpz<R>(a.s0zz + zo, c, a));
-    const float ov0x = a.v0x[cz], ov0z = a.v0z[cz];
-    if (KEEP) {   // background history for the adjoint: v0 at the start of the step, a0
-        a.kv0x[cz] = ov0x;
-        a.kv0z[cz] = ov0z;
-        a.ka0x[cz] = a0x;
-        a.ka0z[cz] = a0z;
-    }
-    a.v0x[cz] = g1 * (g2 * ov0x + dt * a0x);
-    a.v0z[cz] = g1 * (g2 * ov0z + dt * a0z);
+    const float* s0xx = a.s0xx + zo;
+    const float* s0xz = a.s0xz + zo;
+    const float* s0zz = a.s0zz + zo;
+    const float* sxx = a.sxx + zo;
+    const float* sxz = a.sxz + zo;
+    const float* szz = a.szz + zo;
+    ZWin<R> w0xz, w0zz, wxz, wzz;      // sigma_xz: backward z difference; sigma_zz: forward
+    w0xz.init(Ld{s0xz}, S.c, p);
+    w0zz.init(Ld{s0zz}, S.c, p);
     if (BORN) {
-        const float ax = b * (dmx<R>(a.sxx + zo, c, a) + dmz<R>(a.sxz + zo, c, a));
-        const float az = b * (dpx<R>(a.sxz + zo, c, a) + dpz<R>(a.szz + zo, c, a));
-        const float r = a.rr[c];
-        const float nvx = g1 * (g2 * a.vx[cz] + dt * (ax - r * a0x));
-        const float nvz = g1 * (g2 * a.vz[cz] + dt * (az - r * a0z));
-        a.vx[cz] = nvx;
-        a.vz[cz] = nvz;
-        const int rec = a.traces ? recv_of(a, i, k) : -1;
-        if (rec >= 0) {
-            const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
-            float* d = shot_traces(a) + (long long)it * nrec + rec;
-            d[0] = nvx;
-            d[cs] = 0.f;
-            d[2 * cs] = nvz;
+        wxz.init(Ld{sxz}, S.c, p);
+        wzz.init(Ld{szz}, S.c, p);
+    }
+    const int rz = a.traces ? shot_par(a, 5) : -1;
+    long long c = S.c;
+    for (int k = S.k0; k < S.k1; k++, c += p) {
+        const long long cz = c + zo;
+        const float b = a.B[c];
+        const float a0x = b * (dmx<R>(s0xx, c, a) + w0xz.dmz(a.cz));
+        const float a0z = b * (dpx<R>(s0xz, c, a) + w0zz.dpz(a.cz));
+        float ax = 0.f, az = 0.f;
+        if (BORN) {
+            ax = b * (dmx<R>(sxx, c, a) + wxz.dmz(a.cz));
+            az = b * (dpx<R>(sxz, c, a) + wzz.dpz(a.cz));
+        }
+        if (S.act) {
+            const float g1 = a.g1[c], g2 = a.g2[c];
+            const float ov0x = a.v0x[cz], ov0z = a.v0z[cz];
+            if (KEEP) {   // background history for the adjoint: v0 at the start of the step, a0
+                a.kv0x[cz] = ov0x;
+                a.kv0z[cz] = ov0z;
+                a.ka0x[cz] = a0x;
+                a.ka0z[cz] = a0z;
+            }
+            a.v0x[cz] = g1 * (g2 * ov0x + dt * a0x);
+            a.v0z[cz] = g1 * (g2 * ov0z + dt * a0z);
+            if (BORN) {
+                const float r = a.rr[c];
+                const float nvx = g1 * (g2 * a.vx[cz] + dt * (ax - r * a0x));
+                const float nvz = g1 * (g2 * a.vz[cz] + dt * (az - r * a0z));
+                a.vx[cz] = nvx;
+                a.vz[cz] = nvz;
+                const int rec = k == rz ? recv_of(a, S.i, k) : -1;
+                if (rec >= 0) {
+                    const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
+                    float* d = shot_traces(a) + (long long)it * nrec + rec;
+                    d[0] = nvx;
+                    d[cs] = 0.f;
+                    d[2 * cs] = nvz;
+                }
+            }
+        }
+        if (k + 1 < S.k1) {
+            w0xz.shift(Ld{s0xz}, c + p, p);
+            w0zz.shift(Ld{s0zz}, c + p, p);
+            if (BORN) {
+                wxz.shift(Ld{sxz}, c + p, p);
+                wzz.shift(Ld{szz}, c + p, p);
+            }
         }
     }
 }
@@ -278,23 +359,38 @@ __global__ void k_adj_inject(BornArgs a, int it)
 }
 
 // velocity update^T: h (the stress adjoint, already carried through g2 g1 by
-// k_adj_mem) gains the velocity update's stencil transposed; rho gradient from a0
+// k_adj_mem) gains the velocity update's stencil transposed, applied to the
+// products B g1 a^; rho gradient from a0
 template <int R>
-__global__ void k_adj_vel(BornArgs a)
+__global__ void __launch_bounds__(32 * WPB) k_adj_vel(BornArgs a)
 {
-    int i, k;
-    long long c, zo;
-    if (!cell_of(a, i, k, c, zo)) return;
-    const long long cz = c + zo;
+    Strip S;
+    if (!strip_of(a, S)) return;
+    const long long p = a.px, zo = S.zo;
     const float dt = a.dt;
-    const float g1 = a.g1[c];
-    // rho gradient: -dt g1 (vx^ a0x + vz^ a0z)
-    a.gR[cz] += -dt * (g1 * a.ax[cz] * __ldg(a.ha0x + cz) + g1 * a.az[cz] * __ldg(a.ha0z + cz));
-    // the shot's adjoint velocity through per-cell products B g1 a^ (shared B, g1)
-    const Prod2 tx{a.B, a.g1, a.ax, zo}, tz{a.B, a.g1, a.az, zo};
-    a.hxx[cz] = a.hxx[cz] - dt * tdpx<R>(tx, cz, a);
-    a.hxz[cz] = a.hxz[cz] - dt * (tdpz<R>(tx, cz, a) + tdmx<R>(tz, cz, a));
-    a.hzz[cz] = a.hzz[cz] - dt * tdmz<R>(tz, cz, a);
+    const Prod tx{a.Bg1, a.ax, zo}, tz{a.Bg1, a.az, zo};
+    ZWin<R> wx, wz;                    // products: forward z difference of x, backward of z
+    wx.init(tx, S.c + zo, p);
+    wz.init(tz, S.c + zo, p);
+    long long c = S.c;
+    for (int k = S.k0; k < S.k1; k++, c += p) {
+        const long long cz = c + zo;
+        const float dxx = tdpx<R>(tx, cz, a);
+        const float dxz = wx.dpz(a.cz) + tdmx<R>(tz, cz, a);
+        const float dzz = wz.dmz(a.cz);
+        if (S.act) {
+            const float g1 = a.g1[c];
+            // rho gradient: -dt g1 (vx^ a0x + vz^ a0z)
+            a.gR[cz] += -dt * (g1 * a.ax[cz] * __ldg(a.ha0x + cz) + g1 * a.az[cz] * __ldg(a.ha0z + cz));
+            a.hxx[cz] = a.hxx[cz] - dt * dxx;
+            a.hxz[cz] = a.hxz[cz] - dt * dxz;
+            a.hzz[cz] = a.hzz[cz] - dt * dzz;
+        }
+        if (k + 1 < S.k1) {
+            wx.shift(tx, cz + p, p);
+            wz.shift(tz, cz + p, p);
+        }
+    }
 }
 
 // stress and memory-variable update^T of one cell: Q = g1 h is the adjoint of
@@ -303,71 +399,93 @@ __global__ void k_adj_vel(BornArgs a)
 // mu ts; P) (both maps are symmetric), carries lr_l = ra_l Lambda_l and h = g2 Q,
 // and accumulates the pi and mu gradients from the background strain rates.
 template <int R, int NM>
-__global__ void k_adj_mem(BornArgs a)
+__global__ void __launch_bounds__(32 * WPB) k_adj_mem(BornArgs a)
 {
-    int i, k;
-    long long c, zo;
-    if (!cell_of(a, i, k, c, zo)) return;
-    const long long cz = c + zo;
+    Strip S;
+    if (!strip_of(a, S)) return;
+    const long long p = a.px, zo = S.zo;
     const float dt = a.dt;
-    const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
-    const float Q[3] = {g1 * a.hxx[cz], g1 * a.hzz[cz], g1 * a.hxz[cz]};
-    float P[3] = {0.f, 0.f, 0.f};
+    const float* hv0x = a.hv0x + zo;
+    const float* hv0z = a.hv0z + zo;
+    ZWin<R> wx, wz;
+    wx.init(Ld{hv0x}, S.c, p);
+    wz.init(Ld{hv0z}, S.c, p);
+    long long c = S.c;
+    for (int k = S.k0; k < S.k1; k++, c += p) {
+        const long long cz = c + zo;
+        const float e0xx = dpx<R>(hv0x, c, a), e0zz = wz.dmz(a.cz);
+        const float e0xz = wx.dpz(a.cz) + dmx<R>(hv0z, c, a);
+        if (S.act) {
+            const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
+            const float Q[3] = {g1 * a.hxx[cz], g1 * a.hzz[cz], g1 * a.hxz[cz]};
+            float P[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int q = 0; q < 3; q++)
+            for (int q = 0; q < 3; q++)
 #pragma unroll
-        for (int l = 0; l < NM; l++) {
-            float* lr = a.lr[q * 3 + l];
-            const float lam = lr[cz] + dt * Q[q];
-            P[q] += a.rb[l] * lam;
-            lr[cz] = a.ra[l] * lam;
+                for (int l = 0; l < NM; l++) {
+                    float* lr = a.lr[q * 3 + l];
+                    const float lam = lr[cz] + dt * Q[q];
+                    P[q] += a.rb[l] * lam;
+                    lr[cz] = a.ra[l] * lam;
+                }
+            const float tq0 = dt * Q[0], tq1 = dt * Q[1], tq2 = dt * Q[2];
+            a.gM[cz] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
+            a.gU[cz] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
+                        a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
+            float E[3], F[3] = {0.f, 0.f, 0.f};
+            iso(pi * a.kp, mu * a.ks, tq0, tq1, tq2, E);
+            if (NM) iso(pi * a.tp, mu * a.ts, P[0], P[1], P[2], F);
+            a.Sxx[cz] = E[0] + F[0];
+            a.Szz[cz] = E[1] + F[1];
+            a.Sxz[cz] = E[2] + F[2];
+            a.hxx[cz] = g2 * Q[0];
+            a.hzz[cz] = g2 * Q[1];
+            a.hxz[cz] = g2 * Q[2];
         }
-    const float e0xx = dpx<R>(a.hv0x + zo, c, a), e0zz = dmz<R>(a.hv0z + zo, c, a);
-    const float e0xz = dpz<R>(a.hv0x + zo, c, a) + dmx<R>(a.hv0z + zo, c, a);
-    const float tq0 = dt * Q[0], tq1 = dt * Q[1], tq2 = dt * Q[2];
-    a.gM[cz] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
-    a.gU[cz] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
-                a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
-    float E[3], F[3] = {0.f, 0.f, 0.f};
-    iso(pi * a.kp, mu * a.ks, tq0, tq1, tq2, E);
-    if (NM) iso(pi * a.tp, mu * a.ts, P[0], P[1], P[2], F);
-    a.Sxx[cz] = E[0] + F[0];
-    a.Szz[cz] = E[1] + F[1];
-    a.Sxz[cz] = E[2] + F[2];
-    a.hxx[cz] = g2 * Q[0];
-    a.hzz[cz] = g2 * Q[1];
-    a.hxz[cz] = g2 * Q[2];
+        if (k + 1 < S.k1) {
+            wx.shift(Ld{hv0x}, c + p, p);
+            wz.shift(Ld{hv0z}, c + p, p);
+        }
+    }
 }
-
-struct Load {
-    const float* p;
-    __device__ __forceinline__ float operator()(long long c) const { return p[c]; }
-};
 
 // velocity adjoint: a <- g2 g1 a (the velocity update^T) - D^T S (the stress
 // update's stencils transposed), plus the next (earlier) step's residual
 template <int R>
-__global__ void k_adj_str(BornArgs a, int it_next)
+__global__ void __launch_bounds__(32 * WPB) k_adj_str(BornArgs a, int it_next)
 {
-    int i, k;
-    long long c, zo;
-    if (!cell_of(a, i, k, c, zo)) return;
-    const long long cz = c + zo;
-    const float g12 = a.g2[c] * a.g1[c];
-    const Load sxx{a.Sxx}, szz{a.Szz}, sxz{a.Sxz};
-    float nx = g12 * a.ax[cz] - (tdmx<R>(sxx, cz, a) + tdmz<R>(sxz, cz, a));
-    float nz = g12 * a.az[cz] - (tdpz<R>(szz, cz, a) + tdpx<R>(sxz, cz, a));
-    if (it_next >= 0) {
-        const int rec = recv_of(a, i, k);
-        if (rec >= 0) {
-            const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
-            const float* d = shot_traces(a) + (long long)it_next * nrec + rec;
-            nx += d[0];
-            nz += d[2 * cs];
+    Strip S;
+    if (!strip_of(a, S)) return;
+    const long long p = a.px, zo = S.zo;
+    const Ld sxx{a.Sxx + zo}, szz{a.Szz + zo}, sxz{a.Sxz + zo};
+    ZWin<R> wxz, wzz;                  // S_xz: backward z difference; S_zz: forward
+    wxz.init(sxz, S.c, p);
+    wzz.init(szz, S.c, p);
+    const int rz = it_next >= 0 ? shot_par(a, 5) : -1;
+    long long c = S.c;
+    for (int k = S.k0; k < S.k1; k++, c += p) {
+        const long long cz = c + zo;
+        const float dx = tdmx<R>(sxx, c, a) + wxz.dmz(a.cz);
+        const float dz = wzz.dpz(a.cz) + tdpx<R>(sxz, c, a);
+        if (S.act) {
+            const float g12 = a.g2[c] * a.g1[c];
+            float nx = g12 * a.ax[cz] - dx;
+            float nz = g12 * a.az[cz] - dz;
+            const int rec = k == rz ? recv_of(a, S.i, k) : -1;
+            if (rec >= 0) {
+                const long long nrec = a.nrx, cs = (long long)a.nt * nrec;
+                const float* d = shot_traces(a) + (long long)it_next * nrec + rec;
+                nx += d[0];
+                nz += d[2 * cs];
+            }
+            a.ax[cz] = nx;
+            a.az[cz] = nz;
+        }
+        if (k + 1 < S.k1) {
+            wxz.shift(sxz, c + p, p);
+            wzz.shift(szz, c + p, p);
         }
     }
-    a.ax[cz] = nx;
-    a.az[cz] = nz;
 }
 
 // gradients w.r.t. (r_vp, r_vs, r_rho) on the contiguous nz x nx grid, summed over
@@ -392,11 +510,11 @@ __global__ void k_born_final(BornArgs a, float* gvp, float* gvs, float* grho, in
     grho[m] = orho + (a.M[c] * gp + a.U[c] * gu + gr);
 }
 
-// model products (copied from the context's padded model, plane j = 0) and damping
-// factors on the compact layout
+// model products (copied from the context's padded model, plane j = 0), damping
+// factors and B g1 on the compact layout
 __global__ void k_born_model(BornArgs a, const float* Mc, const float* Uc, const float* Bc,
                              long long csz, const float* att_x, const float* att_z, float* M,
-                             float* U, float* L, float* B, float* g1, float* g2)
+                             float* U, float* Bg1, float* B, float* g1, float* g2)
 {
     int i, k;
     long long c;
@@ -405,12 +523,12 @@ __global__ void k_born_model(BornArgs a, const float* Mc, const float* Uc, const
     const long long m = (long long)k * csz + i;
     M[c] = Mc[m];
     U[c] = Uc[m];
-    L[c] = M[c] - 2.f * U[c];
     B[c] = Bc[m];
     const float at = att_z[k] + att_x[i];
     const float h = at * a.dt * 0.5f;
     g1[c] = 1.f / (1.f + h);
     g2[c] = 1.f - h;
+    Bg1[c] = B[c] * g1[c];
 }
 
 __global__ void k_born_pert(BornArgs a, const float* rvp, const float* rvs, const float* rrho,
@@ -428,14 +546,38 @@ __global__ void k_born_pert(BornArgs a, const float* rvp, const float* rvs, cons
 
 dim3 born_grid(const BornArgs& a, int shots = 1) { return dim3((a.nx + 31) / 32, (a.nz + 7) / 8, shots); }
 
+// The marching kernels' arguments and grid: WPB strips per block, chunks of kc
+// rows, one grid layer per shot.  kc is the longest chunk (32, 16 or 8 rows) that
+// still gives about two waves of blocks on the device (a shorter chunk reloads
+// the 2R rows of its z windows more often).
+BornArgs march(const BornArgs& a, dim3& grid)
+{
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
+    BornArgs b = a;
+    const long long xb = ((a.nx + BXH + 31) / 32 + WPB - 1) / WPB;
+    b.kc = 8;
+    for (int kc = 32; kc > 8; kc /= 2)
+        if (xb * ((a.nz + kc - 1) / kc) * a.nshot >= 2LL * 7 * sms) {
+            b.kc = kc;
+            break;
+        }
+    grid = dim3((unsigned)xb, (a.nz + b.kc - 1) / b.kc, a.nshot);
+    return b;
+}
+
 }  // namespace
 
 cudaError_t born_launch_model(const BornArgs& a, const float* Mc, const float* Uc, const float* Bc,
                               long long csz, const float* att_x, const float* att_z, float* M,
-                              float* U, float* L, float* B, float* g1, float* g2, cudaStream_t s)
+                              float* U, float* Bg1, float* B, float* g1, float* g2, cudaStream_t s)
 {
-    k_born_model<<<born_grid(a), dim3(32, 8), 0, s>>>(a, Mc, Uc, Bc, csz, att_x, att_z, M, U, L, B, g1,
-                                                      g2);
+    k_born_model<<<born_grid(a), dim3(32, 8), 0, s>>>(a, Mc, Uc, Bc, csz, att_x, att_z, M, U, Bg1, B,
+                                                      g1, g2);
     return cudaGetLastError();
 }
 
@@ -448,9 +590,11 @@ cudaError_t born_launch_pert(const BornArgs& a, const float* rvp, const float* r
 
 namespace {
 template <int R, int NM>
-void step_r(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
+void step_r(const BornArgs& a0, int it, bool born, bool keep, cudaStream_t s)
 {
-    const dim3 g = born_grid(a, a.nshot), b(32, 8);
+    dim3 g;
+    const BornArgs a = march(a0, g);
+    const dim3 b(32, WPB);
     if (born) k_born_stress<R, true, NM><<<g, b, 0, s>>>(a, it);
     else k_born_stress<R, false, NM><<<g, b, 0, s>>>(a, it);
     if (born) k_born_velocity<R, true, false><<<g, b, 0, s>>>(a, it);
@@ -458,9 +602,11 @@ void step_r(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s)
     else k_born_velocity<R, false, false><<<g, b, 0, s>>>(a, it);
 }
 template <int R, int NM>
-void adj_r(const BornArgs& a, int it, cudaStream_t s)
+void adj_r(const BornArgs& a0, int it, cudaStream_t s)
 {
-    const dim3 g = born_grid(a, a.nshot), b(32, 8);
+    dim3 g;
+    const BornArgs a = march(a0, g);
+    const dim3 b(32, WPB);
     k_adj_vel<R><<<g, b, 0, s>>>(a);
     k_adj_mem<R, NM><<<g, b, 0, s>>>(a);
     k_adj_str<R><<<g, b, 0, s>>>(a, it - 1);

@@ -13,7 +13,7 @@ struct BornArgs {
     long long px;                          // row pitch; cell (i,k) at (k+R)*px + i + BXH
     float cx[8], cz[8];                    // c_n / h
     float dt;
-    const float *M, *U, *L, *B, *g1, *g2;  // model products and damping factors
+    const float *M, *U, *Bg1, *B, *g1, *g2;// model products (Bg1 = B g1) and damping factors
     float *v0x, *v0z, *s0xx, *s0zz, *s0xz; // background state
     float *vx, *vz, *sxx, *szz, *sxz;      // scattered state
     const float *dM, *dU, *rr;             // perturbation products
@@ -43,11 +43,12 @@ struct BornArgs {
     long long ss;
     const int* shot_tab;
     long long tstride;
+    int kc;                                // rows per warp of the step kernels (set by the launcher)
 };
 
 cudaError_t born_launch_model(const BornArgs& a, const float* Mc, const float* Uc, const float* Bc,
                               long long csz, const float* att_x, const float* att_z, float* M,
-                              float* U, float* L, float* B, float* g1, float* g2, cudaStream_t s);
+                              float* U, float* Bg1, float* B, float* g1, float* g2, cudaStream_t s);
 cudaError_t born_launch_pert(const BornArgs& a, const float* rvp, const float* rvs,
                              const float* rrho, float* dM, float* dU, float* rr, cudaStream_t s);
 cudaError_t born_launch_step(const BornArgs& a, int it, bool born, bool keep, cudaStream_t s);

@@ -1285,7 +1285,7 @@ int ertm_set_wait_fault(ertm_ctx* c, int plane, uint32_t polls)
 namespace {
 
 // Shared compact volumes: model products, damping factors, perturbation products.
-enum { SV_M, SV_U, SV_L, SV_B, SV_G1, SV_G2, SV_DM, SV_DU, SV_RR, SV_N };
+enum { SV_M, SV_U, SV_BG1, SV_B, SV_G1, SV_G2, SV_DM, SV_DU, SV_RR, SV_N };
 // Per-shot compact volume types, each [shot][n] over a group of shots: background
 // state (5 fields + 9 memory variables, contiguous so that a checkpoint of every shot
 // is one copy), scattered state and memory variables, adjoint state, gradient
@@ -1365,7 +1365,7 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
         a.cz[q] = (float)(c->coef[q] / c->cfg.dz);
     }
     a.dt = c->cfg.dt_ms / 1000.f;
-    a.M = B.sv[SV_M]; a.U = B.sv[SV_U]; a.L = B.sv[SV_L]; a.B = B.sv[SV_B];
+    a.M = B.sv[SV_M]; a.U = B.sv[SV_U]; a.Bg1 = B.sv[SV_BG1]; a.B = B.sv[SV_B];
     a.g1 = B.sv[SV_G1]; a.g2 = B.sv[SV_G2];
     a.dM = B.sv[SV_DM]; a.dU = B.sv[SV_DU]; a.rr = B.sv[SV_RR];
     a.nm = c->cfg.visco_nmech;
@@ -1389,7 +1389,7 @@ int born_prepare(ertm_ctx* c, BornArgs& a)
     a.nshot = 1;
     a.ss = B.n;
     CK(c, born_launch_model(a, c->m[1][0], c->m[1][1], c->m[1][2], g.sz, c->att[0], c->att[2],
-                            B.sv[SV_M], B.sv[SV_U], B.sv[SV_L], B.sv[SV_B], B.sv[SV_G1], B.sv[SV_G2],
+                            B.sv[SV_M], B.sv[SV_U], B.sv[SV_BG1], B.sv[SV_B], B.sv[SV_G1], B.sv[SV_G2],
                             c->stream));
     c->launches++;
     return ERTM_OK;

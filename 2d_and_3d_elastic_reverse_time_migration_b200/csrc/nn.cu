@@ -485,15 +485,22 @@ cudaError_t gemm_bn(const LA& la, const LB& lb, const EP& ep, int M, int N, int 
     static unsigned long long opted = 0;   // devices with the opt-in made
     cudaError_t attr = ertm::smem_opt_in(k_gemm<BN, LA, LB, EP>, smem, &opted);
     if (attr != cudaSuccess) return attr;
-    // persistent CTAs: about two per SM over the M tiles of each (N tile, K range)
-    int dev = 0, sms = 148;
+    // persistent CTAs: as many as fit on the device at once (shared memory and
+    // TMEM columns bound the CTAs per SM), spread over the M tiles of each
+    // (N tile, K range)
+    int dev = 0, sms = 148, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm<BN, LA, LB, EP>, NT, smem) !=
+            cudaSuccess) {
         cudaGetLastError();
         sms = 148;
+        per_sm = 2;
     }
+    constexpr int TCOLS = BN < 32 ? 32 : BN;
+    per_sm = per_sm < 1 ? 1 : (per_sm > 512 / TCOLS ? 512 / TCOLS : per_sm);
     const int MT = (M + BM - 1) / BM, NTL = (N + BN - 1) / BN;
-    long long gx = (2LL * sms + (long long)NTL * gz - 1) / ((long long)NTL * gz);
+    long long gx = ((long long)per_sm * sms + (long long)NTL * gz - 1) / ((long long)NTL * gz);
     if (gx < 1) gx = 1;
     if (gx > MT) gx = MT;
     dim3 grid((unsigned)gx, NTL, gz);

@@ -117,3 +117,27 @@ def test_shot_batch_device_arrays(ertm, orc):
     ctx.born_adjoint_shots(shots, dev, *gd)
     for a, b in zip(gd, gh):
         assert np.array_equal(a.cpu().numpy(), b)
+
+
+def test_chunk_length_does_not_change_the_results(ertm, orc):
+    """The step kernels march each warp down a chunk of rows whose length follows the
+    size of the launch (32, 16 or 8 rows, the longest that still gives about two
+    waves of blocks): 8 shots on a 1000 x 1100 grid run in 32-row chunks, one shot
+    in 8-row chunks.  The traces are bit-identical (the per-cell arithmetic does not
+    depend on the chunk), the batched gradient equals the sum of the single-shot
+    ones to float rounding."""
+    c = born_case(orc, nz=1100, nx=1000, nt=100)
+    rng = c["rng"]
+    m = [(0.05 * rng.standard_normal(c["shape"])).astype(np.float32) for _ in range(3)]
+    ctx, _ = _ctx(ertm, c, K=20)
+    rec = c["geo"]["rec"]
+    shots = [ertm.Shot(int(x), 0, 12, wavelet=c["w"], **rec) for x in np.linspace(20, 979, 8).astype(int)]
+    batch = ctx.born_forward_shots(shots, *m)
+    for k in (0, 5):
+        assert np.array_equal(batch[k], ctx.born_forward(shots[k], *m)), k
+    dh = rng.standard_normal(batch.shape).astype(np.float32)
+    dh[:, 1] = 0
+    g_batch = ctx.born_adjoint_shots(shots, dh)
+    g_single = [ctx.born_adjoint(s, d) for s, d in zip(shots, dh)]
+    for q in range(3):
+        assert rel(g_batch[q], sum(g[q].astype(np.float64) for g in g_single)) <= 1e-6, q
