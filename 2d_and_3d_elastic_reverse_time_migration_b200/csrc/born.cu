@@ -208,8 +208,31 @@ __global__ void __launch_bounds__(32 * WPB) k_born_stress(BornArgs a, int it)
         const float e0xx = dpx<R>(v0x, c, a), e0zz = w0z.dmz(a.cz);
         const float e0xz = w0x.dpz(a.cz) + dmx<R>(v0z, c, a);
         if (S.act) {
-            const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
+            // every load of the row before any store: a store through one of the
+            // state pointers could alias a later load, which would serialise the
+            // memory-variable updates into one round trip each
+            const float g1 = __ldg(a.g1 + c), g2 = __ldg(a.g2 + c), pi = __ldg(a.M + c), mu = __ldg(a.U + c);
             float o[3] = {a.s0xx[cz], a.s0zz[cz], a.s0xz[cz]};
+            float r0v[3][NM > 0 ? NM : 1], rv[3][NM > 0 ? NM : 1], so[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int l = 0; l < NM; l++) r0v[q][l] = a.r0[q * 3 + l][cz];
+            float exx = 0.f, ezz = 0.f, exz = 0.f, dpi = 0.f, dmu = 0.f;
+            if (BORN) {
+                so[0] = a.sxx[cz];
+                so[1] = a.szz[cz];
+                so[2] = a.sxz[cz];
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+#pragma unroll
+                    for (int l = 0; l < NM; l++) rv[q][l] = a.r[q * 3 + l][cz];
+                exx = dpx<R>(vx, c, a);
+                ezz = wz.dmz(a.cz);
+                exz = wx.dpz(a.cz) + dmx<R>(vz, c, a);
+                dpi = __ldg(a.dM + c);
+                dmu = __ldg(a.dU + c);
+            }
             if (src_step && S.i == sx && k == sz) {
                 // explosive source into the background
                 const float w = __ldg(a.wavelet + (long long)blockIdx.z * a.wstride + it);
@@ -219,23 +242,19 @@ __global__ void __launch_bounds__(32 * WPB) k_born_stress(BornArgs a, int it)
             float E0[3], F0[3];
             iso(pi * a.kp, mu * a.ks, e0xx, e0zz, e0xz, E0);
             if (NM) iso(pi * a.tp, mu * a.ts, e0xx, e0zz, e0xz, F0);
-            float* s0[3] = {a.s0xx, a.s0zz, a.s0xz};
+            float ns0[3];
 #pragma unroll
             for (int q = 0; q < 3; q++) {
                 float sum = 0.f;
 #pragma unroll
                 for (int l = 0; l < NM; l++) {
-                    float* r = a.r0[q * 3 + l];
-                    const float v = a.ra[l] * r[cz] + a.rb[l] * F0[q];
-                    r[cz] = v;
-                    sum += v;
+                    r0v[q][l] = a.ra[l] * r0v[q][l] + a.rb[l] * F0[q];
+                    sum += r0v[q][l];
                 }
-                s0[q][cz] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
+                ns0[q] = g1 * (g2 * o[q] + dt * (E0[q] + sum));
             }
+            float nsc[3];
             if (BORN) {
-                const float exx = dpx<R>(vx, c, a), ezz = wz.dmz(a.cz);
-                const float exz = wx.dpz(a.cz) + dmx<R>(vz, c, a);
-                const float dpi = a.dM[c], dmu = a.dU[c];
                 float E[3], dE[3], F[3], dF[3];
                 iso(pi * a.kp, mu * a.ks, exx, ezz, exz, E);
                 // the reference's stress sources (dem_p), scaled by the GSLS strengths
@@ -244,19 +263,33 @@ __global__ void __launch_bounds__(32 * WPB) k_born_stress(BornArgs a, int it)
                     iso(pi * a.tp, mu * a.ts, exx, ezz, exz, F);
                     iso(dpi * a.tp, dmu * a.ts, e0xx, e0zz, e0xz, dF);
                 }
-                float* sc[3] = {a.sxx, a.szz, a.sxz};
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     float sum = 0.f;
 #pragma unroll
                     for (int l = 0; l < NM; l++) {
-                        float* r = a.r[q * 3 + l];
-                        const float v = a.ra[l] * r[cz] + a.rb[l] * (F[q] + dF[q]);
-                        r[cz] = v;
-                        sum += v;
+                        rv[q][l] = a.ra[l] * rv[q][l] + a.rb[l] * (F[q] + dF[q]);
+                        sum += rv[q][l];
                     }
-                    sc[q][cz] = g1 * (g2 * sc[q][cz] + dt * (E[q] + dE[q] + sum));
+                    nsc[q] = g1 * (g2 * so[q] + dt * (E[q] + dE[q] + sum));
                 }
+            }
+            // stores
+            a.s0xx[cz] = ns0[0];
+            a.s0zz[cz] = ns0[1];
+            a.s0xz[cz] = ns0[2];
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int l = 0; l < NM; l++) a.r0[q * 3 + l][cz] = r0v[q][l];
+            if (BORN) {
+                a.sxx[cz] = nsc[0];
+                a.szz[cz] = nsc[1];
+                a.sxz[cz] = nsc[2];
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+#pragma unroll
+                    for (int l = 0; l < NM; l++) a.r[q * 3 + l][cz] = rv[q][l];
             }
         }
         if (k + 1 < S.k1) {
@@ -294,7 +327,7 @@ __global__ void __launch_bounds__(32 * WPB) k_born_velocity(BornArgs a, int it)
     long long c = S.c;
     for (int k = S.k0; k < S.k1; k++, c += p) {
         const long long cz = c + zo;
-        const float b = a.B[c];
+        const float b = __ldg(a.B + c);
         const float a0x = b * (dmx<R>(s0xx, c, a) + w0xz.dmz(a.cz));
         const float a0z = b * (dpx<R>(s0xz, c, a) + w0zz.dpz(a.cz));
         float ax = 0.f, az = 0.f;
@@ -303,8 +336,15 @@ __global__ void __launch_bounds__(32 * WPB) k_born_velocity(BornArgs a, int it)
             az = b * (dpx<R>(sxz, c, a) + wzz.dpz(a.cz));
         }
         if (S.act) {
-            const float g1 = a.g1[c], g2 = a.g2[c];
+            // every load of the row before any store (see k_born_stress)
+            const float g1 = __ldg(a.g1 + c), g2 = __ldg(a.g2 + c);
             const float ov0x = a.v0x[cz], ov0z = a.v0z[cz];
+            float ovx = 0.f, ovz = 0.f, r = 0.f;
+            if (BORN) {
+                ovx = a.vx[cz];
+                ovz = a.vz[cz];
+                r = __ldg(a.rr + c);
+            }
             if (KEEP) {   // background history for the adjoint: v0 at the start of the step, a0
                 a.kv0x[cz] = ov0x;
                 a.kv0z[cz] = ov0z;
@@ -314,9 +354,8 @@ __global__ void __launch_bounds__(32 * WPB) k_born_velocity(BornArgs a, int it)
             a.v0x[cz] = g1 * (g2 * ov0x + dt * a0x);
             a.v0z[cz] = g1 * (g2 * ov0z + dt * a0z);
             if (BORN) {
-                const float r = a.rr[c];
-                const float nvx = g1 * (g2 * a.vx[cz] + dt * (ax - r * a0x));
-                const float nvz = g1 * (g2 * a.vz[cz] + dt * (az - r * a0z));
+                const float nvx = g1 * (g2 * ovx + dt * (ax - r * a0x));
+                const float nvz = g1 * (g2 * ovz + dt * (az - r * a0z));
                 a.vx[cz] = nvx;
                 a.vz[cz] = nvz;
                 const int rec = k == rz ? recv_of(a, S.i, k) : -1;
@@ -379,12 +418,16 @@ __global__ void __launch_bounds__(32 * WPB) k_adj_vel(BornArgs a)
         const float dxz = wx.dpz(a.cz) + tdmx<R>(tz, cz, a);
         const float dzz = wz.dmz(a.cz);
         if (S.act) {
-            const float g1 = a.g1[c];
+            // every load of the row before any store (see k_born_stress)
+            const float g1 = __ldg(a.g1 + c);
+            const float gr = a.gR[cz], hxx = a.hxx[cz], hxz = a.hxz[cz], hzz = a.hzz[cz];
+            const float vax = __ldg(a.ax + cz), vaz = __ldg(a.az + cz);
+            const float h0x = __ldg(a.ha0x + cz), h0z = __ldg(a.ha0z + cz);
             // rho gradient: -dt g1 (vx^ a0x + vz^ a0z)
-            a.gR[cz] += -dt * (g1 * a.ax[cz] * __ldg(a.ha0x + cz) + g1 * a.az[cz] * __ldg(a.ha0z + cz));
-            a.hxx[cz] = a.hxx[cz] - dt * dxx;
-            a.hxz[cz] = a.hxz[cz] - dt * dxz;
-            a.hzz[cz] = a.hzz[cz] - dt * dzz;
+            a.gR[cz] = gr + -dt * (g1 * vax * h0x + g1 * vaz * h0z);
+            a.hxx[cz] = hxx - dt * dxx;
+            a.hxz[cz] = hxz - dt * dxz;
+            a.hzz[cz] = hzz - dt * dzz;
         }
         if (k + 1 < S.k1) {
             wx.shift(tx, cz + p, p);
@@ -416,25 +459,37 @@ __global__ void __launch_bounds__(32 * WPB) k_adj_mem(BornArgs a)
         const float e0xx = dpx<R>(hv0x, c, a), e0zz = wz.dmz(a.cz);
         const float e0xz = wx.dpz(a.cz) + dmx<R>(hv0z, c, a);
         if (S.act) {
-            const float g1 = a.g1[c], g2 = a.g2[c], pi = a.M[c], mu = a.U[c];
+            // every load of the row before any store (see k_born_stress)
+            const float g1 = __ldg(a.g1 + c), g2 = __ldg(a.g2 + c), pi = __ldg(a.M + c), mu = __ldg(a.U + c);
             const float Q[3] = {g1 * a.hxx[cz], g1 * a.hzz[cz], g1 * a.hxz[cz]};
+            float lv[3][NM > 0 ? NM : 1];
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int l = 0; l < NM; l++) lv[q][l] = a.lr[q * 3 + l][cz];
+            const float gm = a.gM[cz], gu = a.gU[cz];
             float P[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int q = 0; q < 3; q++)
 #pragma unroll
                 for (int l = 0; l < NM; l++) {
-                    float* lr = a.lr[q * 3 + l];
-                    const float lam = lr[cz] + dt * Q[q];
+                    const float lam = lv[q][l] + dt * Q[q];
                     P[q] += a.rb[l] * lam;
-                    lr[cz] = a.ra[l] * lam;
+                    lv[q][l] = a.ra[l] * lam;
                 }
             const float tq0 = dt * Q[0], tq1 = dt * Q[1], tq2 = dt * Q[2];
-            a.gM[cz] += (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
-            a.gU[cz] += a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
-                        a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz);
+            const float ngm = gm + (a.kp * (tq0 + tq1) + a.tp * (P[0] + P[1])) * (e0xx + e0zz);
+            const float ngu = gu + (a.ks * (-2.f * tq0 * e0zz - 2.f * tq1 * e0xx + tq2 * e0xz) +
+                                    a.ts * (-2.f * P[0] * e0zz - 2.f * P[1] * e0xx + P[2] * e0xz));
             float E[3], F[3] = {0.f, 0.f, 0.f};
             iso(pi * a.kp, mu * a.ks, tq0, tq1, tq2, E);
             if (NM) iso(pi * a.tp, mu * a.ts, P[0], P[1], P[2], F);
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int l = 0; l < NM; l++) a.lr[q * 3 + l][cz] = lv[q][l];
+            a.gM[cz] = ngm;
+            a.gU[cz] = ngu;
             a.Sxx[cz] = E[0] + F[0];
             a.Szz[cz] = E[1] + F[1];
             a.Sxz[cz] = E[2] + F[2];
@@ -468,7 +523,7 @@ __global__ void __launch_bounds__(32 * WPB) k_adj_str(BornArgs a, int it_next)
         const float dx = tdmx<R>(sxx, c, a) + wxz.dmz(a.cz);
         const float dz = wzz.dpz(a.cz) + tdpx<R>(sxz, c, a);
         if (S.act) {
-            const float g12 = a.g2[c] * a.g1[c];
+            const float g12 = __ldg(a.g2 + c) * __ldg(a.g1 + c);
             float nx = g12 * a.ax[cz] - dx;
             float nz = g12 * a.az[cz] - dz;
             const int rec = k == rz ? recv_of(a, S.i, k) : -1;

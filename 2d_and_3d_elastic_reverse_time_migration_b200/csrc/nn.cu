@@ -332,7 +332,6 @@ struct Smem {
     alignas(128) uint8_t a[NS][BM * BK * 2];
     alignas(128) uint8_t b[NS][BN * BK * 2];
     uint64_t bar[NS];
-    uint64_t accbar;   // the MMAs of an M tile have completed (one phase per tile)
     uint32_t tmem;
 };
 
@@ -371,11 +370,6 @@ __device__ __forceinline__ void stage(uint8_t* dst, const L& ld, int r0, int k0)
     }
 }
 
-// Persistent over M tiles: CTA x takes the M tiles x, x + gridDim.x, ... (one N
-// tile, one split-K range), so the barriers and the TMEM accumulator are set up
-// once and the operand ring runs on across tile boundaries: while the warps read
-// one tile's accumulator out of TMEM, the copies of the next tile's first K tiles
-// are already in flight.
 template <int BN, class LA, class LB, class EP>
 __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, int K, int kt_per, int* err)
 {
@@ -383,19 +377,13 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
     Smem<BN>& S = *reinterpret_cast<Smem<BN>*>(smraw);
     constexpr int TCOLS = BN < 32 ? 32 : BN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.y * BN;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int KT = (K + BK - 1) / BK;
     const int kt0 = blockIdx.z * kt_per, kt1 = min(KT, kt0 + kt_per);
-    const int nu = kt1 > kt0 ? kt1 - kt0 : 0;          // K tiles per M tile
-    const int MT = (M + BM - 1) / BM;
-    const int ntile = (int)blockIdx.x < MT ? (MT - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    const int U = ntile * nu;                          // (M tile, K tile) steps of this CTA
-    auto m0_of = [&](int t) { return ((int)blockIdx.x + t * (int)gridDim.x) * BM; };
 
     constexpr int NS = Smem<BN>::NS;
     if (threadIdx.x == 0) {
         for (int q = 0; q < NS; q++) mbar_init(&S.bar[q], 1);
-        mbar_init(&S.accbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -410,22 +398,22 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
     const uint32_t tmem = S.tmem;
     constexpr uint32_t IDESC = idesc_bf16(BN) | (LA::MN ? 1u << 15 : 0u) | (LB::MN ? 1u << 16 : 0u);
     bool ok = true;
-    // every thread copies its chunks of step u into slot u % NS with cp.async, one
-    // commit group per step (empty groups keep the count uniform)
+    const int nu = kt1 - kt0;
+    // every thread copies its chunks of K tile u into slot u % NS with cp.async, one
+    // commit group per tile (empty groups keep the count uniform)
     auto issue = [&](int u) {
-        if (u < U) {
-            const int sl = u % NS, t = u / nu, kt = u - t * nu;
-            stage<BM>(S.a[sl], la, m0_of(t), (kt0 + kt) * BK);
-            stage<BN>(S.b[sl], lb, n0, (kt0 + kt) * BK);
+        if (u < nu) {
+            const int sl = u % NS;
+            stage<BM>(S.a[sl], la, m0, (kt0 + u) * BK);
+            stage<BN>(S.b[sl], lb, n0, (kt0 + u) * BK);
         }
         cp_commit();
     };
     for (int u = 0; u < NS - 1; u++) issue(u);
-    for (int u = 0; u < U; ++u) {
-        const int t = u / nu, kt = u - t * nu;
-        cp_wait<NS - 2>();        // this thread's copies of step u have landed
+    for (int u = 0; u < nu; ++u) {
+        cp_wait<NS - 2>();        // this thread's copies of tile u have landed
         proxy_fence();            // ... and are visible to the tensor core's async proxy
-        __syncthreads();          // ... for every thread's chunks (and the previous epilogue is done)
+        __syncthreads();          // ... for every thread's chunks
         const int sl = u % NS;
         if (threadIdx.x == 0 && ok) {
             tc_fence_after();
@@ -435,37 +423,31 @@ __global__ void __launch_bounds__(NT) k_gemm(LA la, LB lb, EP ep, int M, int N, 
                 // K step j covers the core-matrix columns 2j, 2j+1
                 const uint64_t da = sdesc(a0 + (uint32_t)(2 * j * BM * 16), BM * 16);
                 const uint64_t db = sdesc(b0 + (uint32_t)(2 * j * BN * 16), BN * 16);
-                umma(tmem, da, db, IDESC, (kt > 0 || j > 0) ? 1u : 0u);
+                umma(tmem, da, db, IDESC, (u > 0 || j > 0) ? 1u : 0u);
             }
             umma_commit(&S.bar[sl]);
-            if (kt == nu - 1) umma_commit(&S.accbar);   // the tile's accumulator is complete
         }
-        // refill slot (u - 1) % NS with step u + NS - 1 once step u-1's MMAs read it
+        // refill slot (u - 1) % NS with tile u + NS - 1 once tile u-1's MMAs read it
         const int un = u + NS - 1;
-        if (un < U && u >= 1 && ok) ok = mbar_wait(&S.bar[(u - 1) % NS], ((u - 1) / NS) & 1);
-        issue(ok ? un : U);
-        if (kt == nu - 1) {
-            // epilogue of M tile t; the TMEM loads are warp-collective, so the
-            // decision is block-uniform
-            if (ok) ok = mbar_wait(&S.accbar, t & 1);
-            const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
-            tc_fence_after();
-            if (!all_ok) {
-                ok = false;
-                break;
-            }
-            const int m = m0_of(t) + warp * 32 + lane;
-            const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-            for (int c = 0; c < BN; c += 8) {
-                float v[8];
-                tmem_ld8(trow + c, v);
-                ep(m, n0 + c, v);
-            }
-            tc_fence_before();   // the next tile's MMAs follow the next barrier
-        }
+        if (un < nu && u >= 1 && ok) ok = mbar_wait(&S.bar[(u - 1) % NS], ((u - 1) / NS) & 1);
+        issue(ok ? un : nu);
     }
     cp_wait<0>();
+    if (nu > 0 && ok) ok = mbar_wait(&S.bar[(nu - 1) % NS], ((nu - 1) / NS) & 1);
+    // the other stage's last commit precedes it, so every MMA has completed;
+    // the TMEM loads below are warp-collective, so the decision is block-uniform
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    tc_fence_after();
+    if (nu > 0 && all_ok) {
+        const int m = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 8) {
+            float v[8];
+            tmem_ld8(trow + c, v);
+            ep(m, n0 + c, v);
+        }
+    }
     if (!ok && err) atomicExch(err, NN_WAIT);
     tc_fence_before();
     __syncthreads();
@@ -485,25 +467,7 @@ cudaError_t gemm_bn(const LA& la, const LB& lb, const EP& ep, int M, int N, int 
     static unsigned long long opted = 0;   // devices with the opt-in made
     cudaError_t attr = ertm::smem_opt_in(k_gemm<BN, LA, LB, EP>, smem, &opted);
     if (attr != cudaSuccess) return attr;
-    // persistent CTAs: as many as fit on the device at once (shared memory and
-    // TMEM columns bound the CTAs per SM), spread over the M tiles of each
-    // (N tile, K range)
-    int dev = 0, sms = 148, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm<BN, LA, LB, EP>, NT, smem) !=
-            cudaSuccess) {
-        cudaGetLastError();
-        sms = 148;
-        per_sm = 2;
-    }
-    constexpr int TCOLS = BN < 32 ? 32 : BN;
-    per_sm = per_sm < 1 ? 1 : (per_sm > 512 / TCOLS ? 512 / TCOLS : per_sm);
-    const int MT = (M + BM - 1) / BM, NTL = (N + BN - 1) / BN;
-    long long gx = ((long long)per_sm * sms + (long long)NTL * gz - 1) / ((long long)NTL * gz);
-    if (gx < 1) gx = 1;
-    if (gx > MT) gx = MT;
-    dim3 grid((unsigned)gx, NTL, gz);
+    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, gz);
     k_gemm<BN, LA, LB, EP><<<grid, NT, smem, st>>>(la, lb, ep, M, N, K, kt_per, err);
     return cudaGetLastError();
 }

@@ -359,6 +359,7 @@ def run_lsrtm(args):
         case = L.make_case(5000 + k, geo)
         rows.append(L.compare(case, net, niter=niter, target=target))
         case.ctx.close()
+        print(json.dumps({"event": "test_case", "seed": 5000 + k, **_fmt_case(rows[-1])}), flush=True)
     def med(key):
         v = [r[key] for r in rows if r[key] is not None]
         return float(np.median(v)) if v else None
