@@ -32,6 +32,7 @@ BOUNDARY_CPML, BOUNDARY_SPONGE_COS, BOUNDARY_SPONGE_CUBIC = 0, 1, 2
 COEF_TAYLOR, COEF_REFERENCE12, COEF_USER = 0, 1, 2
 INJECT_ADD, INJECT_REPLACE = 1, 2
 STEP_SINGLE, STEP_PAIRS = 0, 1
+MULTI_MAX = 10          # shots per ertm_rtm_multi call (ERTM_MULTI_MAX)
 FIELDS = ("vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz", "tp", "vxp", "vyp", "vzp")
 ERRORS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENOTSUP",
           -6: "EDEVICE"}
@@ -91,6 +92,8 @@ SIGNATURES = {
     "ertm_backward_together_using_smoothed_model": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_rtm_shot": (C.c_int, [_P, C.POINTER(_Shot), _P, _P, _P, _P]),
     "ertm_rtm_batch": (C.c_int, [_P, C.POINTER(_Shot), C.c_int, C.POINTER(_P), _P, _P, _P]),
+    "ertm_rtm_multi": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_Shot), C.POINTER(_P), C.POINTER(_P),
+                                 C.POINTER(_P), C.POINTER(_P)]),
     "ertm_get_wavefield": (C.c_int, [_P, C.c_int, _P]),
     "ertm_get_excitation": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "ertm_set_angles": (C.c_int, [_P, C.c_int]),
@@ -586,11 +589,40 @@ class Window:
         return w
 
 
-def rtm_windows(base: Config, vp, vs, rho, windows: list, shots: list, data: list, lanes: int = 2,
-                pp=None, ps=None, tp=None):
+def rtm_multi(contexts: list, shots: list, data: list, outs: list | None = None):
+    """Several 3D shots migrated together, shot q on contexts[q] (its own grid and
+    migration model), one launch of each step kernel per time step for all of them
+    (ertm_rtm_multi in include/ertm.h).  Returns [(pp, ps, tp)] per shot, into
+    `outs` when given (host or device volumes of each context's grid)."""
+    L = lib()
+    n = len(contexts)
+    if not (1 <= n <= MULTI_MAX) or len(shots) != n or len(data) != n:
+        raise ValueError(f"rtm_multi: 1 .. {MULTI_MAX} contexts, one shot and one record each")
+    outs = outs or [tuple(c._vol(None) for _ in range(3)) for c in contexts]
+    hs = (C.c_void_p * n)(*[c._h for c in contexts])
+    arr = (_Shot * n)(*[sh.struct() for sh in shots])
+    keep, dp = [], (C.c_void_p * n)()
+    for q, (c, sh, d) in enumerate(zip(contexts, shots, data)):
+        d = d if _is_torch(d) else np.ascontiguousarray(d, np.float32)
+        keep.append(d)
+        dp[q] = _ptr(d, 3 * c.cfg.nt * sh.nrec)
+    op = [(C.c_void_p * n)() for _ in range(3)]
+    for q, (c, o) in enumerate(zip(contexts, outs)):
+        for k in range(3):
+            op[k][q] = _ptr(o[k], c.ncell, True)
+    rc = L.ertm_rtm_multi(hs, n, arr, dp, op[0], op[1], op[2])
+    del keep
+    if rc != 0:
+        raise ErtmError(rc, contexts[0]._msg(contexts[0]._h))
+    return outs
+
+
+def rtm_windows(base: Config, vp, vs, rho, windows: list, shots: list, data: list,
+                lanes: int = MULTI_MAX, pp=None, ps=None, tp=None):
     """Batched RTM over aperture windows of one shared migration model (model cells,
     no absorbing layers, shape (nz, ny, nx) = base.shape); images stacked into
-    pp, ps, tp of the model's shape.  See ertm_rtm_windows in include/ertm.h."""
+    pp, ps, tp of the model's shape; `lanes` 3D shots per launch (up to MULTI_MAX).
+    See ertm_rtm_windows in include/ertm.h."""
     L = lib()
     n = base.nx * base.ny * base.nz
     outs = [np.zeros(base.shape, np.float32) if o is None else o for o in (pp, ps, tp)]

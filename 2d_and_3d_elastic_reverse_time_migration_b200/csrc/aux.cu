@@ -290,4 +290,15 @@ cudaError_t launch_velocity(int R, const Geom& g, const KArgs& a, const VelMaps&
                   : launch_velocity_r6(g, a, m, cpml, epi, record, s);
 }
 
+cudaError_t launch_stress_multi(int R, dim3 grid, const StressMulti& P, bool cpml, cudaStream_t s)
+{
+    return R == 4 ? launch_stress_multi_r4(grid, P, cpml, s) : launch_stress_multi_r6(grid, P, cpml, s);
+}
+
+cudaError_t launch_velocity_multi(int R, dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t s)
+{
+    return R == 4 ? launch_velocity_multi_r4(grid, P, cpml, epi, s)
+                  : launch_velocity_multi_r6(grid, P, cpml, epi, s);
+}
+
 }  // namespace ertm

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -618,6 +619,40 @@ struct Range {
 
 // One pass of `nsteps` steps.  MODE_MODEL records into `traces` ([3][nt][nrec],
 // device), MODE_RECEIVER injects from it.
+// The time loop of a pass: `one_step` (which launches one step's kernels on
+// c->stream) runs nsteps times, as a CUDA graph of kGraphSteps steps replayed
+// back to back (the kernels read the step index from device memory, so one graph
+// serves every chunk); the first step and the remainder are launched directly.
+template <typename F>
+int time_loop(ertm_ctx* c, int nsteps, F&& one_step)
+{
+    constexpr int kGraphSteps = 32;
+    int done = 0;
+    if (nsteps > 0) {
+        CK(c, one_step());
+        done = 1;
+    }
+    if (nsteps - done >= 2 * kGraphSteps) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int q = 0; q < kGraphSteps && e == cudaSuccess; q++) e = one_step();
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        while (e == cudaSuccess && nsteps - done >= kGraphSteps) {
+            e = cudaGraphLaunch(exec, c->stream);
+            done += kGraphSteps;
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "graph time loop: %s", cudaGetErrorString(e));
+    }
+    for (; done < nsteps; done++) CK(c, one_step());
+    return ERTM_OK;
+}
+
 int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, float* traces)
 {
     if (!c->model_set[which])
@@ -664,33 +699,7 @@ int run_pass(ertm_ctx* c, int which, const ertm_shot* s, int mode, int nsteps, f
         if (e == cudaSuccess) e = launch_advance(c->it_d, dir, c->stream);
         return e;
     };
-    // The time loop runs as a CUDA graph of kGraphSteps steps replayed back to back
-    // (the kernels read the step index from device memory, so one graph serves every
-    // chunk); the first step and the remainder are launched directly.
-    constexpr int kGraphSteps = 32;
-    int done = 0;
-    if (nsteps > 0) {
-        CK(c, one_step());
-        done = 1;
-    }
-    if (nsteps - done >= 2 * kGraphSteps) {
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = cudaSuccess;
-        for (int q = 0; q < kGraphSteps && e == cudaSuccess; q++) e = one_step();
-        cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
-        if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-        while (e == cudaSuccess && nsteps - done >= kGraphSteps) {
-            e = cudaGraphLaunch(exec, c->stream);
-            done += kGraphSteps;
-        }
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return fail(c, ERTM_ECUDA, "graph time loop: %s", cudaGetErrorString(e));
-    }
-    for (; done < nsteps; done++) CK(c, one_step());
+    if ((rc = time_loop(c, nsteps, one_step))) return rc;
     c->launches += (ang ? 4LL : 3LL) * nsteps;
     return check_device_error(c);
 }
@@ -1114,6 +1123,171 @@ int ertm_rtm_batch(ertm_ctx* c, const ertm_shot* shots, int nshots, const float*
     cudaFree(acc);
     (void)n;
     return rc;
+}
+
+int ertm_rtm_multi(ertm_ctx* const* ctx, int n, const ertm_shot* shots, const float* const* data,
+                   float* const* img_pp, float* const* img_ps, float* const* img_tp)
+{
+    if (!ctx || !ctx[0]) return fail(nullptr, ERTM_EINVAL, "ertm_rtm_multi: no contexts");
+    ertm_ctx* c0 = ctx[0];
+    if (n < 1 || n > ERTM_MULTI_MAX)
+        return fail(c0, ERTM_EINVAL, "ertm_rtm_multi: %d shots (1 .. %d per call)", n, ERTM_MULTI_MAX);
+    if (!shots || !data) return fail(c0, ERTM_EINVAL, "ertm_rtm_multi: shots or data is NULL");
+    for (int q = 0; q < n; q++) {
+        const ertm_ctx* c = ctx[q];
+        if (!c) return fail(c0, ERTM_EINVAL, "ertm_rtm_multi: context %d is NULL", q);
+        for (int r = 0; r < q; r++)
+            if (ctx[r] == c) return fail(c0, ERTM_EINVAL, "ertm_rtm_multi: context %d repeats context %d", q, r);
+        if (c->g.two_d) return fail(c0, ERTM_ENOTSUP, "ertm_rtm_multi: 3D grids only (context %d is 2D)", q);
+        if (c->device != c0->device || c->g.nz != c0->g.nz || c->R != c0->R ||
+            c->cfg.boundary != c0->cfg.boundary)
+            return fail(c0, ERTM_EINVAL,
+                        "ertm_rtm_multi: context %d differs from context 0 in device, nz, order or boundary", q);
+        if (!c->model_set[1]) return fail(c0, ERTM_ESTATE, "ertm_rtm_multi: context %d has no migration model", q);
+    }
+    CK(c0, cudaSetDevice(c0->device));
+    int rc;
+    for (int q = 0; q < n; q++) {
+        if ((rc = validate_shot(ctx[q], &shots[q], true))) {
+            const std::string m = ctx[q]->err;
+            return fail(c0, rc, "ertm_rtm_multi: shot %d: %s", q, m.c_str());
+        }
+        if (nrec_of(&shots[q]) > 0 && !data[q]) return fail(c0, ERTM_EINVAL, "ertm_rtm_multi: data %d is NULL", q);
+    }
+    // every context's earlier work is done; this call issues all of its work on
+    // context 0's stream (the per-context helpers below use c->stream)
+    for (int q = 0; q < n; q++) CK(c0, cudaStreamSynchronize(ctx[q]->stream));
+    struct StreamSwap {
+        ertm_ctx* const* ctx;
+        int n;
+        cudaStream_t saved[ERTM_MULTI_MAX];
+        StreamSwap(ertm_ctx* const* c, int k, cudaStream_t st) : ctx(c), n(k)
+        {
+            for (int q = 0; q < n; q++) {
+                saved[q] = ctx[q]->stream;
+                ctx[q]->stream = st;
+            }
+        }
+        ~StreamSwap()
+        {
+            for (int q = 0; q < n; q++) ctx[q]->stream = saved[q];
+        }
+    } swap(ctx, n, c0->stream);
+    Range range("ertm rtm multi");
+    const cudaStream_t st = c0->stream;
+    const bool cpml = c0->cfg.boundary == ERTM_BOUNDARY_CPML;
+    int kchunk = choose_kchunk(c0->g, c0->R, c0->device);
+    if (c0->cfg.autotune == 1 && (rc = autotune_kchunk(c0, 1, &kchunk))) return rc;
+    const int chunks = (c0->g.nz + kchunk - 1) / kchunk;
+    unsigned gx = 0, gy = 0;
+    for (int q = 0; q < n; q++) {
+        gx = std::max(gx, (unsigned)((ctx[q]->g.nx + TX - 1) / TX));
+        gy = std::max(gy, (unsigned)((ctx[q]->g.ny + TY3 - 1) / TY3));
+    }
+    const dim3 grid(gx, gy, (unsigned)(n * chunks));
+    // the argument blocks travel by value in the kernels' parameter space
+    std::unique_ptr<StressMulti> SP(new StressMulti());
+    std::unique_ptr<VelMulti> VP(new VelMulti());
+    std::memset(SP.get(), 0, sizeof(StressMulti));
+    std::memset(VP.get(), 0, sizeof(VelMulti));
+    SP->chunks = VP->chunks = chunks;
+    auto args_of = [&](int q, float* traces, int it_hi, int epi) {
+        ertm_ctx* c = ctx[q];
+        KArgs& a = SP->a[q];
+        fill_args(c, 1, &shots[q], a);
+        a.kchunk = kchunk;
+        a.traces = traces;
+        a.it_ptr = c0->it_d;   // one step index for every shot of the call
+        a.it_hi = it_hi;
+        a.pairs = 0;
+        if (epi == EPI_IMAGE) a.nw = 0;
+        VP->a[q] = a;
+        SP->m[q] = stress_maps(c, 1);
+        VP->m[q] = vel_maps(c, 1, epi);
+    };
+    auto loop = [&](int epi, int nsteps, int dir) -> int {
+        auto one_step = [&]() -> cudaError_t {
+            cudaError_t e = launch_stress_multi(c0->R, grid, *SP, cpml, st);
+            if (e == cudaSuccess) e = launch_velocity_multi(c0->R, grid, *VP, cpml, epi, st);
+            if (e == cudaSuccess) e = launch_advance(c0->it_d, dir, st);
+            return e;
+        };
+        int r = time_loop(c0, nsteps, one_step);
+        c0->launches += 3LL * nsteps;
+        return r;
+    };
+
+    // source pass: every shot from step 0; a shot with fewer source steps idles
+    // (its CTAs return at once) for the rest of the pass
+    int nsrc_max = 0;
+    for (int q = 0; q < n; q++) {
+        ertm_ctx* c = ctx[q];
+        const Geom& g = c->g;
+        if ((rc = ensure_excitation(c))) return rc;
+        CK(c0, cudaMemsetAsync(c->ex_amp2_base, 0, sizeof(float) * g.total, st));
+        CK(c0, cudaMemsetAsync(c->ex_time_base, 0, sizeof(int) * g.total, st));
+        for (int k = 0; k < 3; k++)
+            if (c->ex_v_base[k]) CK(c0, cudaMemsetAsync(c->ex_v_base[k], 0, sizeof(float) * g.total, st));
+        CK(c0, cudaMemsetAsync(c->ex_tp_base, 0, sizeof(float) * g.total, st));
+        c->have_excitation = false;
+        const float vmax = c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[1];
+        if ((rc = upload_profiles(c, vmax))) return rc;
+        if ((rc = reset_state(c))) return rc;
+        if ((rc = upload_wavelet(c, &shots[q]))) return rc;
+        const int nsrc = c->cfg.src_steps > 0 ? c->cfg.src_steps : 2 * c->cfg.nt / 3;
+        args_of(q, nullptr, nsrc, EPI_EXCITE);
+        nsrc_max = std::max(nsrc_max, nsrc);
+    }
+    CK(c0, launch_set_int(c0->it_d, 0, st));
+    c0->launches++;
+    if ((rc = loop(EPI_EXCITE, nsrc_max, 1))) return rc;
+    for (int q = 0; q < n; q++) ctx[q]->have_excitation = true;
+
+    // receiver pass: the step index runs down from the longest shot's last step;
+    // a shot joins when it reaches its own last step (its first residual sample is
+    // injected up front: its wavefields stay untouched until it joins)
+    int nt_max = 0;
+    for (int q = 0; q < n; q++) {
+        ertm_ctx* c = ctx[q];
+        const Geom& g = c->g;
+        if ((rc = ensure_images(c))) return rc;
+        for (int k = 0; k < 3; k++) CK(c0, cudaMemsetAsync(c->img_base[k], 0, sizeof(float) * g.total, st));
+        const long long nrec = nrec_of(&shots[q]);
+        const size_t nd = 3 * (size_t)c->cfg.nt * nrec;
+        float* traces = nullptr;
+        if (nd) {
+            if (is_device_ptr(data[q])) traces = const_cast<float*>(data[q]);
+            else {
+                if ((rc = ensure_traces(c, nd))) return rc;
+                CK(c0, cudaMemcpyAsync(c->traces, data[q], sizeof(float) * nd, cudaMemcpyHostToDevice, st));
+                traces = c->traces;
+            }
+        }
+        if ((rc = reset_state(c))) return rc;
+        args_of(q, traces, c->cfg.nt, EPI_IMAGE);
+        if (c->cfg.nt > 0) {
+            CK(c0, launch_inject(SP->a[q], c->cfg.nt - 1, st));
+            c0->launches++;
+        }
+        nt_max = std::max(nt_max, c->cfg.nt);
+    }
+    CK(c0, launch_set_int(c0->it_d, nt_max - 1, st));
+    c0->launches++;
+    if ((rc = loop(EPI_IMAGE, nt_max, -1))) return rc;
+    for (int q = 0; q < n; q++) {
+        ertm_ctx* c = ctx[q];
+        float* outs[3] = {img_pp ? img_pp[q] : nullptr, img_ps ? img_ps[q] : nullptr,
+                          img_tp ? img_tp[q] : nullptr};
+        for (int k = 0; k < 3; k++)
+            if ((rc = copy_out_volume(c, c->img_base[k] + c->g.off0, outs[k]))) return rc;
+    }
+    for (int q = 0; q < n; q++)
+        if ((rc = check_device_error(ctx[q]))) {
+            const std::string m = ctx[q]->err;
+            return fail(c0, rc, "ertm_rtm_multi: shot %d: %s", q, m.c_str());
+        }
+    CK(c0, cudaStreamSynchronize(st));
+    return ERTM_OK;
 }
 
 int ertm_get_wavefield(ertm_ctx* c, int field, float* out)

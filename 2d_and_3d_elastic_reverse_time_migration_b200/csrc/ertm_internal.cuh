@@ -90,6 +90,8 @@ struct KArgs {
     unsigned wait_polls;
     // 3D step-kernel variant: 0 = one cell per thread (default), 1 = cell pairs
     int pairs;
+    // several shots per launch only: the shot is idle while *it_ptr >= it_hi
+    int it_hi;
 };
 
 // Device error codes written to KArgs::err
@@ -114,6 +116,23 @@ struct VelMaps {
     CUtensorMap c[8];      // C boxes: vx vz vy vxp vzp vyp b excitation(amp2 or time)
     CUtensorMap fr[4];     // C boxes of txz tzz tyz tp: z-queue fronts
 };
+
+// Argument blocks of the multi-shot step kernels: up to kMultiMax shots per
+// launch, each with its own argument block and TMA maps, all passed by value in
+// the kernel's parameter block (3.1 KB per shot of the 32 KB it can hold), so
+// that the TMA unit reads every descriptor from parameter space.
+constexpr int kMultiMax = ERTM_MULTI_MAX;
+struct StressMulti {
+    KArgs a[kMultiMax];
+    StressMaps m[kMultiMax];
+    int chunks;                      // z chunks per shot
+};
+struct VelMulti {
+    KArgs a[kMultiMax];
+    VelMaps m[kMultiMax];
+    int chunks;
+};
+static_assert(sizeof(VelMulti) <= 32764 && sizeof(StressMulti) <= 32764, "kernel parameter limit");
 
 // x halo of the staged tiles: >= R and a multiple of 4 floats (16-byte TMA x start)
 constexpr int xb_of(int R) { return R <= 4 ? 4 : 8; }
@@ -162,6 +181,13 @@ cudaError_t launch_velocity_r4(const Geom& g, const KArgs& a, const VelMaps& m, 
                                bool record, cudaStream_t s);
 cudaError_t launch_velocity_r6(const Geom& g, const KArgs& a, const VelMaps& m, bool cpml, int epi,
                                bool record, cudaStream_t s);
+cudaError_t launch_stress_multi_r4(dim3 grid, const StressMulti& P, bool cpml, cudaStream_t s);
+cudaError_t launch_stress_multi_r6(dim3 grid, const StressMulti& P, bool cpml, cudaStream_t s);
+cudaError_t launch_velocity_multi_r4(dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t s);
+cudaError_t launch_velocity_multi_r6(dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t s);
+// several 3D shots per launch (RTM passes): grid (x tiles, y tiles, shots x chunks)
+cudaError_t launch_stress_multi(int R, dim3 grid, const StressMulti& P, bool cpml, cudaStream_t s);
+cudaError_t launch_velocity_multi(int R, dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t s);
 
 // Small kernels (aux.cu)
 cudaError_t launch_scatter(const Geom& g, const float* src, float* dst, cudaStream_t s);

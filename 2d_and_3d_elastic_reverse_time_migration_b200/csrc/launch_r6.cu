@@ -15,4 +15,14 @@ cudaError_t launch_velocity_r6(const Geom& g, const KArgs& a, const VelMaps& m, 
     return launch_velocity_any<6>(g, a, m, cpml, epi, record, s);
 }
 
+cudaError_t launch_stress_multi_r6(dim3 grid, const StressMulti& P, bool cpml, cudaStream_t s)
+{
+    return launch_stress_multi_t<6>(grid, P, cpml, s);
+}
+
+cudaError_t launch_velocity_multi_r6(dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t s)
+{
+    return launch_velocity_multi_t<6>(grid, P, cpml, epi, s);
+}
+
 }  // namespace ertm

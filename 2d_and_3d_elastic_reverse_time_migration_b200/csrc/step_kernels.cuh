@@ -220,9 +220,10 @@ struct StressShape {
     static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 3 * PSI) + 16 * NS;
 };
 
+// The stress step of one CTA: tile (blockIdx.x, blockIdx.y) of the x-y plane, z
+// chunk bz of the grid described by `a`, whose TMA maps are `maps`.
 template <int R, bool Y, bool CPML, bool PS>
-__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
-k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
+__device__ __forceinline__ void stress_body(const StressMaps& maps, const KArgs& a, int bz)
 {
     using SS = StressShape<R, Y, CPML, PS>;
     using B = typename SS::B;
@@ -238,7 +239,7 @@ k_stress(const __grid_constant__ StressMaps maps, const KArgs a)
     const bool leader = (tx == 0 && ty == TYB);
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TYB;
     const int i = i0 + tx, j = j0 + ty;
-    const int k0 = blockIdx.z * a.kchunk;
+    const int k0 = bz * a.kchunk;
     const int k1 = min(k0 + a.kchunk, a.nz);
     const int nk = k1 - k0;
     const int sy = (int)a.sy, sz = (int)a.sz;
@@ -515,9 +516,9 @@ struct VelShape {
     static constexpr size_t BYTES = 4 * (size_t)(NS * STAGE + 3 * PSI) + 16 * NS;
 };
 
+// The velocity step of one CTA (tile and chunk as in stress_body).
 template <int R, bool Y, bool CPML, int EPI, bool REC>
-__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
-k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
+__device__ __forceinline__ void velocity_body(const VelMaps& maps, const KArgs& a, int bz)
 {
     using VS = VelShape<R, Y, CPML, EPI>;
     using B = typename VS::B;
@@ -532,7 +533,7 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
     const bool leader = (tx == 0 && ty == TYB);
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TYB;
     const int i = i0 + tx, j = j0 + ty;
-    const int k0 = blockIdx.z * a.kchunk;
+    const int k0 = bz * a.kchunk;
     const int k1 = min(k0 + a.kchunk, a.nz);
     const int nk = k1 - k0;
     const int sy = (int)a.sy, sz = (int)a.sz;
@@ -836,6 +837,47 @@ k_velocity(const __grid_constant__ VelMaps maps, const KArgs a)
 }
 
 // ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+template <int R, bool Y, bool CPML, bool PS>
+__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
+k_stress(const __grid_constant__ StressMaps maps, const __grid_constant__ KArgs a)
+{
+    stress_body<R, Y, CPML, PS>(maps, a, blockIdx.z);
+}
+
+template <int R, bool Y, bool CPML, int EPI, bool REC>
+__global__ void __launch_bounds__(TX * ((Y ? TY3 : TY2) + 1), Y ? CTAS3 : 1)
+k_velocity(const __grid_constant__ VelMaps maps, const __grid_constant__ KArgs a)
+{
+    velocity_body<R, Y, CPML, EPI, REC>(maps, a, blockIdx.z);
+}
+
+// Several 3D shots in one launch (the RTM passes: P/S split on, excitation or
+// imaging epilogue).  Every shot has its own context-sized volumes, argument
+// block and TMA maps, all in the parameter block (StressMulti / VelMulti);
+// blockIdx.z covers the `chunks` z chunks of every shot in turn.  A CTA whose tile lies outside its
+// shot's grid, or whose shot is idle at this step (step index >= it_hi: a shot
+// with fewer steps than the launch), returns before touching anything.
+template <int R, bool CPML>
+__global__ void __launch_bounds__(TX * (TY3 + 1), CTAS3) k_stress_multi(const __grid_constant__ StressMulti P)
+{
+    const int shot = blockIdx.z / P.chunks;
+    const KArgs& a = P.a[shot];
+    if ((int)blockIdx.x * TX >= a.nx || (int)blockIdx.y * TY3 >= a.ny || __ldg(a.it_ptr) >= a.it_hi) return;
+    stress_body<R, true, CPML, true>(P.m[shot], a, blockIdx.z - shot * P.chunks);
+}
+
+template <int R, bool CPML, int EPI>
+__global__ void __launch_bounds__(TX * (TY3 + 1), CTAS3) k_velocity_multi(const __grid_constant__ VelMulti P)
+{
+    const int shot = blockIdx.z / P.chunks;
+    const KArgs& a = P.a[shot];
+    if ((int)blockIdx.x * TX >= a.nx || (int)blockIdx.y * TY3 >= a.ny || __ldg(a.it_ptr) >= a.it_hi) return;
+    velocity_body<R, true, CPML, EPI, false>(P.m[shot], a, blockIdx.z - shot * P.chunks);
+}
+
+// ---------------------------------------------------------------------------
 // Launch helpers (instantiated per R in launch_r4.cu / launch_r6.cu)
 // ---------------------------------------------------------------------------
 // One instantiation per kernel, so the shared-memory opt-in below is made for
@@ -911,6 +953,40 @@ cudaError_t launch_velocity_t(const Geom& g, const KArgs& a, const VelMaps& m, b
                        : launch_velocity_y<R, true, false>(grid, block, m, a, epi, rec, st);
     return cpml ? launch_velocity_y<R, false, true>(grid, block, m, a, epi, rec, st)
                 : launch_velocity_y<R, false, false>(grid, block, m, a, epi, rec, st);
+}
+
+template <typename P, void (*K)(P)>
+static cudaError_t launch_dyn_multi(dim3 grid, size_t smem, const P& prm, cudaStream_t st)
+{
+    static unsigned long long opted = 0;
+    cudaError_t attr = smem_opt_in(K, smem, &opted);
+    if (attr != cudaSuccess) return attr;
+    K<<<grid, dim3(TX, TY3 + 1), smem, st>>>(prm);
+    return cudaGetLastError();
+}
+
+template <int R>
+cudaError_t launch_stress_multi_t(dim3 grid, const StressMulti& P, bool cpml, cudaStream_t st)
+{
+    if (cpml)
+        return launch_dyn_multi<StressMulti, k_stress_multi<R, true>>(grid, StressShape<R, true, true, true>::BYTES, P, st);
+    return launch_dyn_multi<StressMulti, k_stress_multi<R, false>>(grid, StressShape<R, true, false, true>::BYTES, P, st);
+}
+
+template <int R>
+cudaError_t launch_velocity_multi_t(dim3 grid, const VelMulti& P, bool cpml, int epi, cudaStream_t st)
+{
+    if (epi == EPI_EXCITE)
+        return cpml ? launch_dyn_multi<VelMulti, k_velocity_multi<R, true, EPI_EXCITE>>(
+                          grid, VelShape<R, true, true, EPI_EXCITE>::BYTES, P, st)
+                    : launch_dyn_multi<VelMulti, k_velocity_multi<R, false, EPI_EXCITE>>(
+                          grid, VelShape<R, true, false, EPI_EXCITE>::BYTES, P, st);
+    if (epi == EPI_IMAGE)
+        return cpml ? launch_dyn_multi<VelMulti, k_velocity_multi<R, true, EPI_IMAGE>>(
+                          grid, VelShape<R, true, true, EPI_IMAGE>::BYTES, P, st)
+                    : launch_dyn_multi<VelMulti, k_velocity_multi<R, false, EPI_IMAGE>>(
+                          grid, VelShape<R, true, false, EPI_IMAGE>::BYTES, P, st);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace ertm

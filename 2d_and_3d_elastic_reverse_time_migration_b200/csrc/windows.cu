@@ -3,22 +3,21 @@
 // Every shot migrates on its own window: the shared migration model cropped to
 // the window laterally (full depth), extended by the absorbing layers with edge
 // values, and its images are added into one stacked volume of the model's size.
-// Shots run on `lanes` contexts at once, one host thread and one CUDA stream per
-// lane, each context allocated for the largest window and shrunk to each shot's
-// window with ertm_set_grid; a lane keeps its own stack and the stacks are summed
-// in lane order at the end, so the result does not depend on how the shots were
-// spread over the lanes beyond float summation order.  Built on the public C ABI
-// plus two small kernels (crop, stack); the reference migrates one shot per run
-// on the full grid (3D_elastic_RTM/3D_output_file.cu:339-365).
+// The shots run in groups of up to ERTM_MULTI_MAX through ertm_rtm_multi: one
+// context per shot of a group (allocated once for the largest window and shrunk
+// to each shot's window with ertm_set_grid), all on one stream, and every time
+// step of a group is one launch of each step kernel covering all of its shots.
+// Shots are taken in decreasing order of cost, so a group's shots have similar
+// sizes and step counts, and their images are stacked in that order: the sum
+// does not depend on the group size.  Built on the public C ABI plus two small
+// kernels (crop, stack); the reference migrates one shot per run on the full
+// grid (3D_elastic_RTM/3D_output_file.cu:339-365).
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "ertm.h"
@@ -59,13 +58,6 @@ __global__ void k_stack_window(const float* __restrict__ img, int nx, int ny, in
     }
 }
 
-__global__ void k_add(const float* __restrict__ a, float* __restrict__ b, long long n)
-{
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-         q += (long long)gridDim.x * blockDim.x)
-        b[q] += a[q];
-}
-
 void put_err(char* buf, size_t len, const std::string& m)
 {
     if (!buf || !len) return;
@@ -74,12 +66,10 @@ void put_err(char* buf, size_t len, const std::string& m)
     buf[n] = 0;
 }
 
-struct Lane {
+struct Slot {
     ertm_ctx* ctx = nullptr;
-    cudaStream_t st = nullptr;
     float* model = nullptr;   // 3 x cap cells (window grid)
     float* img = nullptr;     // 3 x cap cells (window grid)
-    float* stack = nullptr;   // 3 x model cells
 };
 
 }  // namespace
@@ -131,16 +121,18 @@ extern "C" int ertm_rtm_windows(const ertm_config* base, const float* vp, const 
     }
     const int nz_w = NZ + pzt + pzb;
     const long long ncap = (long long)cap_nx * cap_ny * nz_w, nmod = (long long)NX * NY * NZ;
-    lanes = std::max(1, std::min(lanes, std::max(nshots, 1)));
+    const int G = std::max(1, std::min({lanes, ERTM_MULTI_MAX, std::max(nshots, 1)}));
     if (cudaSetDevice(B.device) != cudaSuccess) {
         cudaGetLastError();
         return bad(ERTM_ECUDA, "cudaSetDevice");
     }
 
-    // shared model on the device
+    // shared model, stack and one stream on the device
     const float* mdl[3] = {vp, vs, rho};
     float* dmodel = nullptr;
-    std::vector<Lane> L(lanes);
+    float* stack = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<Slot> S(G);
     int rc = ERTM_OK;
     std::string err;
     auto cuda_fail = [&](cudaError_t e, const char* what) {
@@ -149,12 +141,24 @@ extern "C" int ertm_rtm_windows(const ertm_config* base, const float* vp, const 
             err = std::string(what) + ": " + cudaGetErrorString(e);
         }
     };
-    cudaError_t e = cudaMalloc(&dmodel, sizeof(float) * 3 * nmod);
-    if (e != cudaSuccess) cuda_fail(e, "model");
+    auto api_fail = [&](int r, ertm_ctx* c, const std::string& head) {
+        if (rc == ERTM_OK) {
+            char b[512];
+            ertm_last_error(c, b, sizeof b);
+            rc = r;
+            err = head + b;
+        }
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) cuda_fail(e, "stream");
+    if (rc == ERTM_OK && (e = cudaMalloc(&dmodel, sizeof(float) * 3 * nmod)) != cudaSuccess) cuda_fail(e, "model");
     for (int q = 0; q < 3 && rc == ERTM_OK; q++)
         if ((e = cudaMemcpy(dmodel + q * nmod, mdl[q], sizeof(float) * nmod, cudaMemcpyDefault)) != cudaSuccess)
             cuda_fail(e, "model copy");
-    for (int l = 0; l < lanes && rc == ERTM_OK; l++) {
+    if (rc == ERTM_OK && (e = cudaMalloc(&stack, sizeof(float) * 3 * nmod)) != cudaSuccess) cuda_fail(e, "stack");
+    if (rc == ERTM_OK && (e = cudaMemsetAsync(stack, 0, sizeof(float) * 3 * nmod, st)) != cudaSuccess)
+        cuda_fail(e, "memset");
+    for (int l = 0; l < G && rc == ERTM_OK; l++) {
         ertm_config c = B;
         c.nx = cap_nx;
         c.ny = cap_ny;
@@ -162,23 +166,17 @@ extern "C" int ertm_rtm_windows(const ertm_config* base, const float* vp, const 
         c.nt = cap_nt;
         c.src_steps = 0;
         if (two_d) c.pml[2] = c.pml[3] = 0;
-        int r = ertm_create(&c, &L[l].ctx);
+        int r = ertm_create(&c, &S[l].ctx);
         if (r) {
-            char b[512];
-            ertm_last_error(nullptr, b, sizeof b);
-            rc = r;
-            err = std::string("lane context: ") + b;
+            api_fail(r, nullptr, "window context: ");
             break;
         }
-        if ((e = cudaStreamCreateWithFlags(&L[l].st, cudaStreamNonBlocking)) != cudaSuccess) { cuda_fail(e, "stream"); break; }
-        ertm_set_stream(L[l].ctx, L[l].st);
-        if ((e = cudaMalloc(&L[l].model, sizeof(float) * 3 * ncap)) != cudaSuccess) { cuda_fail(e, "lane model"); break; }
-        if ((e = cudaMalloc(&L[l].img, sizeof(float) * 3 * ncap)) != cudaSuccess) { cuda_fail(e, "lane image"); break; }
-        if ((e = cudaMalloc(&L[l].stack, sizeof(float) * 3 * nmod)) != cudaSuccess) { cuda_fail(e, "lane stack"); break; }
-        if ((e = cudaMemsetAsync(L[l].stack, 0, sizeof(float) * 3 * nmod, L[l].st)) != cudaSuccess) { cuda_fail(e, "memset"); break; }
+        ertm_set_stream(S[l].ctx, st);
+        if ((e = cudaMalloc(&S[l].model, sizeof(float) * 3 * ncap)) != cudaSuccess) { cuda_fail(e, "window model"); break; }
+        if ((e = cudaMalloc(&S[l].img, sizeof(float) * 3 * ncap)) != cudaSuccess) { cuda_fail(e, "window image"); break; }
     }
 
-    // largest windows first, handed out dynamically
+    // largest windows first
     std::vector<int> order(nshots);
     for (int i = 0; i < nshots; i++) order[i] = i;
     auto cost = [&](int i) {
@@ -187,39 +185,36 @@ extern "C" int ertm_rtm_windows(const ertm_config* base, const float* vp, const 
         return (double)(w.wx + pxl + pxr) * (two_d ? 1 : w.wy + pyl + pyr) * (ss + w.nt);
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
-    std::atomic<int> next{0};
-    std::atomic<bool> stop{rc != ERTM_OK};
-    std::mutex mu;
 
-    auto worker = [&](int l) {
-        cudaSetDevice(B.device);
-        Lane& ln = L[l];
-        auto lane_fail = [&](int code, const std::string& m) {
-            std::lock_guard<std::mutex> lk(mu);
-            if (rc == ERTM_OK) {
-                rc = code;
-                err = m;
-            }
-            stop = true;
-        };
-        while (!stop) {
-            const int q = next.fetch_add(1);
-            if (q >= nshots) break;
-            const int i = order[q];
+    for (int g0 = 0; g0 < nshots && rc == ERTM_OK; g0 += G) {
+        const int m = std::min(G, nshots - g0);
+        ertm_ctx* cx[ERTM_MULTI_MAX];
+        ertm_shot sh[ERTM_MULTI_MAX];
+        const float* dd[ERTM_MULTI_MAX];
+        float* pp[ERTM_MULTI_MAX];
+        float* ps[ERTM_MULTI_MAX];
+        float* tp[ERTM_MULTI_MAX];
+        for (int j = 0; j < m && rc == ERTM_OK; j++) {
+            const int i = order[g0 + j];
             const ertm_window& w = win[i];
+            Slot& sl = S[j];
             const int nx = w.wx + pxl + pxr, ny = two_d ? 1 : w.wy + pyl + pyr;
             const long long n = (long long)nx * ny * nz_w;
-            int r = ertm_set_grid(ln.ctx, nx, ny, w.nt, w.src_steps);
+            int r = ertm_set_grid(sl.ctx, nx, ny, w.nt, w.src_steps);
             if (!r) {
-                k_crop_pad<<<592, 256, 0, ln.st>>>(dmodel, dmodel + nmod, dmodel + 2 * nmod, NX, NY, NZ,
-                                                    w.x0 - pxl, two_d ? 0 : w.y0 - pyl, -pzt, ln.model, nx,
-                                                    ny, nz_w);
-                cudaError_t ke = cudaGetLastError();
-                if (ke != cudaSuccess) {
-                    lane_fail(ERTM_ECUDA, std::string("crop: ") + cudaGetErrorString(ke));
+                k_crop_pad<<<592, 256, 0, st>>>(dmodel, dmodel + nmod, dmodel + 2 * nmod, NX, NY, NZ,
+                                                w.x0 - pxl, two_d ? 0 : w.y0 - pyl, -pzt, sl.model, nx, ny, nz_w);
+                if ((e = cudaGetLastError()) != cudaSuccess) {
+                    cuda_fail(e, "crop");
                     break;
                 }
-                r = ertm_set_model(ln.ctx, 1, ln.model, ln.model + n, ln.model + 2 * n);
+                r = ertm_set_model(sl.ctx, 1, sl.model, sl.model + n, sl.model + 2 * n);
+            }
+            if (r) {
+                char head[64];
+                snprintf(head, sizeof head, "shot %d: ", i);
+                api_fail(r, sl.ctx, head);
+                break;
             }
             ertm_shot s = shots[i];
             s.sx = s.sx - w.x0 + pxl;
@@ -228,86 +223,51 @@ extern "C" int ertm_rtm_windows(const ertm_config* base, const float* vp, const 
             s.rx0 = s.rx0 - w.x0 + pxl;
             s.ry0 = two_d ? 0 : s.ry0 - w.y0 + pyl;
             s.rz = s.rz + pzt;
-            if (!r) r = ertm_rtm_shot(ln.ctx, &s, data[i], ln.img, ln.img + n, ln.img + 2 * n);
-            if (r) {
-                char b[512];
-                ertm_last_error(ln.ctx, b, sizeof b);
-                char head[64];
-                snprintf(head, sizeof head, "shot %d: ", i);
-                lane_fail(r, std::string(head) + b);
-                break;
-            }
-            k_stack_window<<<592, 256, 0, ln.st>>>(ln.img, nx, ny, nz_w, pxl, two_d ? 0 : pyl, pzt,
-                                                    ln.stack, NX, NY, NZ, w.x0, two_d ? 0 : w.y0, w.wx,
-                                                    two_d ? 1 : w.wy);
-            cudaError_t ke = cudaGetLastError();
-            if (ke != cudaSuccess) {
-                lane_fail(ERTM_ECUDA, std::string("stack: ") + cudaGetErrorString(ke));
-                break;
-            }
+            cx[j] = sl.ctx;
+            sh[j] = s;
+            dd[j] = data[i];
+            pp[j] = sl.img;
+            ps[j] = sl.img + n;
+            tp[j] = sl.img + 2 * n;
         }
-        cudaError_t se = cudaStreamSynchronize(ln.st);
-        if (se != cudaSuccess) lane_fail(ERTM_ECUDA, std::string("lane: ") + cudaGetErrorString(se));
-    };
-    // Autotuning (base->autotune): tune every distinct window shape up front on
-    // lane 0 alone, so no other lane's work disturbs the trial timings (a
-    // zero-step pass runs the tuner, whose choice is cached per shape).
-    if (rc == ERTM_OK && B.autotune == 1) {
-        std::vector<std::pair<int, int>> shapes;
-        for (int i = 0; i < nshots; i++)
-            shapes.emplace_back(win[i].wx + pxl + pxr, two_d ? 1 : win[i].wy + pyl + pyr);
-        std::sort(shapes.begin(), shapes.end());
-        shapes.erase(std::unique(shapes.begin(), shapes.end()), shapes.end());
-        for (auto& sh : shapes) {
-            const long long n = (long long)sh.first * sh.second * nz_w;
-            int r = ertm_set_grid(L[0].ctx, sh.first, sh.second, 1, 0);
-            if (!r) {
-                k_crop_pad<<<592, 256, 0, L[0].st>>>(dmodel, dmodel + nmod, dmodel + 2 * nmod, NX, NY, NZ, 0, 0,
-                                                      0, L[0].model, sh.first, sh.second, nz_w);
-                r = ertm_set_model(L[0].ctx, 1, L[0].model, L[0].model + n, L[0].model + 2 * n);
+        if (rc != ERTM_OK) break;
+        if (two_d) {
+            // 2D windows: one shot per call through the single-shot path
+            for (int j = 0; j < m && rc == ERTM_OK; j++) {
+                int r = ertm_rtm_shot(cx[j], &sh[j], dd[j], pp[j], ps[j], tp[j]);
+                if (r) api_fail(r, cx[j], "shot: ");
             }
-            ertm_shot s{};
-            s.nrx = s.nry = 0;
-            s.drx = s.dry = 1;
-            if (!r) r = ertm_propagate(L[0].ctx, 1, &s, 0);
-            if (r) {
-                char b[512];
-                ertm_last_error(L[0].ctx, b, sizeof b);
-                rc = r;
-                err = std::string("autotune: ") + b;
-                break;
-            }
+        } else {
+            int r = ertm_rtm_multi(cx, m, sh, dd, pp, ps, tp);
+            if (r) api_fail(r, cx[0], "shots: ");
         }
-    }
-    if (rc == ERTM_OK) {
-        std::vector<std::thread> th;
-        for (int l = 0; l < lanes; l++) th.emplace_back(worker, l);
-        for (auto& t : th) t.join();
+        for (int j = 0; j < m && rc == ERTM_OK; j++) {
+            const ertm_window& w = win[order[g0 + j]];
+            const int nx = w.wx + pxl + pxr, ny = two_d ? 1 : w.wy + pyl + pyr;
+            k_stack_window<<<592, 256, 0, st>>>(pp[j], nx, ny, nz_w, pxl, two_d ? 0 : pyl, pzt, stack, NX, NY,
+                                                NZ, w.x0, two_d ? 0 : w.y0, w.wx, two_d ? 1 : w.wy);
+            if ((e = cudaGetLastError()) != cudaSuccess) cuda_fail(e, "stack");
+        }
     }
 
-    // sum the lane stacks in lane order, then write the outputs
+    // the outputs
     if (rc == ERTM_OK) {
-        for (int l = 1; l < lanes; l++) {
-            cudaStreamSynchronize(L[l].st);
-            k_add<<<592, 256, 0, L[0].st>>>(L[l].stack, L[0].stack, 3 * nmod);
-        }
         float* outs[3] = {stack_pp, stack_ps, stack_tp};
         for (int q = 0; q < 3 && rc == ERTM_OK; q++) {
             if (!outs[q]) continue;
-            e = cudaMemcpyAsync(outs[q], L[0].stack + q * nmod, sizeof(float) * nmod, cudaMemcpyDefault,
-                                L[0].st);
+            e = cudaMemcpyAsync(outs[q], stack + q * nmod, sizeof(float) * nmod, cudaMemcpyDefault, st);
             if (e != cudaSuccess) cuda_fail(e, "output copy");
         }
-        if ((e = cudaStreamSynchronize(L[0].st)) != cudaSuccess) cuda_fail(e, "output");
     }
-    for (auto& ln : L) {
-        if (ln.ctx) ertm_destroy(ln.ctx);
-        if (ln.st) cudaStreamDestroy(ln.st);
-        cudaFree(ln.model);
-        cudaFree(ln.img);
-        cudaFree(ln.stack);
+    if (st && (e = cudaStreamSynchronize(st)) != cudaSuccess) cuda_fail(e, "windows");
+    for (auto& sl : S) {
+        if (sl.ctx) ertm_destroy(sl.ctx);
+        cudaFree(sl.model);
+        cudaFree(sl.img);
     }
+    cudaFree(stack);
     cudaFree(dmodel);
+    if (st) cudaStreamDestroy(st);
     if (rc != ERTM_OK) return bad(rc, err);
     put_err(errbuf, errlen, "");
     return ERTM_OK;

@@ -74,7 +74,8 @@ def parse():
                          "patch = 512x256 cells at 5 m, 8 shots, 2000 steps, one 256x512 patch per model")
     ap.add_argument("--train-batch", type=int, default=16)
     ap.add_argument("--shots", type=int, default=64, help="windows workload: shots")
-    ap.add_argument("--lanes", type=int, default=4, help="windows workload: shots in flight")
+    ap.add_argument("--lanes", type=int, default=10,
+                    help="windows workload: shots per launch (1 .. 10, ertm_rtm_multi groups)")
     ap.add_argument("--cg-iters", type=int, default=20, help="lsrtm-cg workload: CG iterations")
     return ap.parse_args()
 
@@ -282,7 +283,8 @@ def run_windows(args):
         "seconds": round(el, 2), "higher_is_better": True, "dtype": "f32",
         "data": "synthetic shared model (layered + ellipsoid); seeded random traces",
         "config": {"workload": f"windows-{args.shots}shots-{nx}x{ny}x{nz}", "shots": args.shots,
-                   "lanes": args.lanes, "window": "U[64,192]^2 + 40-cell C-PML", "nt": "U[2000,3500]",
+                   "shots_per_launch": min(args.lanes, ertm.MULTI_MAX),
+                   "window": "U[64,192]^2 + 40-cell C-PML", "nt": "U[2000,3500]",
                    "cell_updates": updates, "autotune": 1},
         "clocks": clk}), flush=True)
 

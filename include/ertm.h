@@ -153,8 +153,12 @@ int ertm_set_grid(ertm_ctx *ctx, int nx, int ny, int nt, int src_steps);
  *           model cells; each window grid is the model cropped to the window,
  *           all depths, extended by the absorbing layers with edge values.
  *  data[i]  observed data of shot i, [3][win[i].nt][nrx*nry] (host or device).
- *  lanes    shots in flight at once (one context, stream and host thread each,
- *           sized for the largest window).
+ *  lanes    shots per launch (1 .. ERTM_MULTI_MAX; larger values are clamped):
+ *           the shots run in groups of `lanes`, each group through
+ *           ertm_rtm_multi on contexts sized for the largest window, so every
+ *           time step of a group is one launch of each step kernel for all of
+ *           its shots.  Groups are formed from the shots in decreasing order of
+ *           cost (cells x steps) and their images are stacked in that order.
  *  stack_*  nz*ny*nx sums of the windows' PP / PS / TP images (host or device;
  *           NULL skips one).  errbuf receives a message on failure. */
 int ertm_rtm_windows(const ertm_config *base, const float *vp, const float *vs, const float *rho,
@@ -197,6 +201,23 @@ int ertm_rtm_shot(ertm_ctx *ctx, const ertm_shot *shot, const float *data_in,
  * split a shot list between contexts and add their stacks (one reduce). */
 int ertm_rtm_batch(ertm_ctx *ctx, const ertm_shot *shots, int nshots, const float *const *data,
                    float *stack_pp, float *stack_ps, float *stack_tp);
+
+/* Several 3D shots migrated together, each on its own context: one RTM shot
+ * (source pass, receiver pass) per context, as ertm_rtm_shot would run it, but
+ * every time step is one launch of each step kernel covering all n shots (the
+ * reference runs one shot per program invocation, 3D_forward_or_back_together.cu
+ * :29,34,125).  ctx[q] holds shot q's grid (its own nx, ny, nt, src_steps, e.g.
+ * through ertm_set_grid) and migration model; all contexts are 3D, distinct, on
+ * one device, with the same nz, order and boundary kind; 1 <= n <= ERTM_MULTI_MAX.
+ * Shots with fewer steps than the longest idle at the end of the source pass and
+ * at the start of the receiver pass.  data[q] is shot q's [3][nt_q][nrec_q]
+ * record (host or device).  img_pp/ps/tp: NULL, or arrays of n outputs of
+ * ctx[q]'s grid (host or device; NULL entries skip).  All work runs on ctx[0]'s
+ * stream; afterwards each context holds its shot's excitation and images, the
+ * same numbers as ertm_rtm_shot gives. */
+#define ERTM_MULTI_MAX 10
+int ertm_rtm_multi(ertm_ctx *const *ctx, int n, const ertm_shot *shots, const float *const *data,
+                   float *const *img_pp, float *const *img_ps, float *const *img_tp);
 
 /* ---- least-squares RTM operators (2D, sponge boundaries) ---------------
  * The linearised (Born) modelling of the reference's LSRTM
