@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--kernel-steps", type=int, default=60)
     ap.add_argument("--grid", default="", help="interior nx,ny,nz (profiling cases only)")
     ap.add_argument("--pml", type=int, default=40, help="C-PML width (profiling cases only)")
+    ap.add_argument("--step-variant", default="single", choices=["single", "pairs"],
+                    help="3D step kernels: one cell per thread (default) or x-adjacent cell pairs")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
     ap.add_argument("--workload", default="shot",
@@ -663,6 +665,7 @@ def main():
     ctx = ertm.Context(cfg)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_step_variant(ertm.STEP_PAIRS if args.step_variant == "pairs" else ertm.STEP_SINGLE)
     ctx.set_model(ertm.TRUE_MODEL, wl.vp, wl.vs, wl.rho)
     ctx.set_model(ertm.MIGRATION_MODEL, wl.svp, wl.svs, wl.srho)
     shot = _shot(ertm, wl, synth, rank)
@@ -791,6 +794,7 @@ def main():
                          "rtm_algorithmic_frac": round(160 * cells / (step_ms / 1e3) / 1e9 / peak, 4),
                          "traffic_bytes_per_cell": TRAFFIC_B_PER_CELL},
             "gpu_launches": launches,
+            "step_variant": args.step_variant,
             "clocks": clk,
         }
         if cpu is not None:
