@@ -484,6 +484,168 @@ cudaError_t gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, 
 }
 
 // ---------------------------------------------------------------------------
+// 3x3 convolution over rows of 128 pixels, taps as shifted operand windows
+// ---------------------------------------------------------------------------
+// For a layer whose width is a multiple of 128 and whose input channels come in
+// groups of 16, a CTA computes the 128 x BN output tile of 128 consecutive
+// pixels of one image row.  Per group of 16 input channels a stage holds the
+// three input rows around that output row, 130 pixels each (the padding column
+// on either side, zero outside the image), as planes of 16-byte chunks (8
+// channels of one pixel per chunk, plane [row][chunk]), and the group's weights
+// for the nine taps.  In the K-major no-swizzle layout of tcgen05 an operand row
+// is one 16-byte chunk and 8 consecutive rows form a core matrix, so the A
+// operand of tap (ky, kx) is the plane of row ky read from pixel kx on: nine
+// MMAs of K = 16 per stage read the staged rows in place.  A stage copies
+// 3 x 130 pixels of input against 128 x 9 for an im2col tile.
+constexpr int CV_PX = 130;                   // pixels per staged row
+constexpr int CV_PLANE = CV_PX * 16;         // bytes of one [row][chunk] plane
+constexpr int CV_A = 6 * CV_PLANE;           // 3 rows x 2 chunks
+template <int BN>
+struct ConvSmem {
+    static constexpr int NS = 3;
+    static constexpr int A_PAD = (CV_A + 127) / 128 * 128;
+    alignas(128) uint8_t a[NS][A_PAD];
+    alignas(128) uint8_t b[NS][9 * 2 * BN * 16];   // [tap][chunk][BN rows x 16 B]
+    uint64_t bar[NS];
+    uint32_t tmem;
+};
+
+template <int BN, class EP>
+__global__ void __launch_bounds__(NT) k_conv3s(Act x, const bf16* __restrict__ w, int N, EP ep, int* err)
+{
+    extern __shared__ __align__(128) uint8_t smraw[];
+    ConvSmem<BN>& S = *reinterpret_cast<ConvSmem<BN>*>(smraw);
+    constexpr int NS = ConvSmem<BN>::NS;
+    constexpr int TCOLS = BN < 32 ? 32 : BN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int x0 = m0 % x.w, t0 = m0 / x.w, y0 = t0 % x.h, nb = t0 / x.h;
+    const int G = x.c / 16, ldw = 9 * x.c;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NS; q++) mbar_init(&S.bar[q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&S.tmem)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    constexpr uint32_t IDESC = idesc_bf16(BN);
+    bool ok = true;
+    // every thread copies its 16-byte chunks of channel group g into slot g % NS,
+    // one commit group per group (empty groups keep the count uniform)
+    auto issue = [&](int g) {
+        if (g < G) {
+            uint8_t* A = S.a[g % NS];
+            uint8_t* Bs = S.b[g % NS];
+            const int c0 = x.off + 16 * g;
+            for (int q = threadIdx.x; q < 3 * CV_PX * 2; q += NT) {
+                // consecutive threads take the two chunks of consecutive pixels
+                const int kc = q & 1, pr = q >> 1, dy = pr / CV_PX, px = pr - dy * CV_PX;
+                const int yy = y0 + dy - 1, xx = x0 + px - 1;
+                const bf16* src = (yy >= 0 && yy < x.h && xx >= 0 && xx < x.w)
+                                      ? x.p + ((long long)(nb * x.h + yy) * x.w + xx) * x.cs + c0 + 8 * kc
+                                      : nullptr;
+                cp16(A + (dy * 2 + kc) * CV_PLANE + px * 16, src);
+            }
+            for (int q = threadIdx.x; q < 9 * 2 * BN; q += NT) {
+                const int r = q % BN, tk = q / BN, kc = tk & 1, tap = tk >> 1;
+                const bf16* src = n0 + r < N ? w + (long long)(n0 + r) * ldw + tap * x.c + 16 * g + 8 * kc : nullptr;
+                cp16(Bs + (tap * 2 + kc) * BN * 16 + r * 16, src);
+            }
+        }
+        cp_commit();
+    };
+    for (int g = 0; g < NS - 1; g++) issue(g);
+    for (int g = 0; g < G; ++g) {
+        cp_wait<NS - 2>();        // this thread's copies of group g have landed
+        proxy_fence();            // ... and are visible to the tensor core's async proxy
+        __syncthreads();          // ... for every thread's chunks
+        const int sl = g % NS;
+        if (threadIdx.x == 0 && ok) {
+            tc_fence_after();
+            const uint32_t a0 = su32(S.a[sl]), b0 = su32(S.b[sl]);
+#pragma unroll
+            for (int tap = 0; tap < 9; tap++) {
+                const int ky = tap / 3, kx = tap % 3;
+                const uint64_t da = sdesc(a0 + (uint32_t)(ky * 2 * CV_PLANE + kx * 16), CV_PLANE);
+                const uint64_t db = sdesc(b0 + (uint32_t)(tap * 2 * BN * 16), BN * 16);
+                umma(tmem, da, db, IDESC, (g > 0 || tap > 0) ? 1u : 0u);
+            }
+            umma_commit(&S.bar[sl]);
+        }
+        // refill slot (g - 1) % NS with group g + NS - 1 once group g-1's MMAs read it
+        const int gn = g + NS - 1;
+        if (gn < G && g >= 1 && ok) ok = mbar_wait(&S.bar[(g - 1) % NS], ((g - 1) / NS) & 1);
+        issue(ok ? gn : G);
+    }
+    cp_wait<0>();
+    if (G > 0 && ok) ok = mbar_wait(&S.bar[(G - 1) % NS], ((G - 1) / NS) & 1);
+    // the last group's commit follows every earlier one, so every MMA has completed;
+    // the TMEM loads below are warp-collective, so the decision is block-uniform
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    tc_fence_after();
+    if (G > 0 && all_ok) {
+        const int m = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 8) {
+            float v[8];
+            tmem_ld8(trow + c, v);
+            ep(m, n0 + c, v);
+        }
+    }
+    if (!ok && err) atomicExch(err, NN_WAIT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+// the layer fits the row kernel: width a multiple of 128, input channels in
+// groups of 16 starting on a 16-byte boundary of 16-byte-aligned pixels
+bool conv3s_fits(const Act& x)
+{
+    return x.w % BM == 0 && x.c % 16 == 0 && x.off % 8 == 0 && x.cs % 8 == 0 &&
+           (reinterpret_cast<uintptr_t>(x.p) & 15) == 0;
+}
+
+template <int BN, class EP>
+cudaError_t conv3s_bn(const Act& x, const bf16* w, int N, const EP& ep, int* err, cudaStream_t st)
+{
+    const size_t smem = sizeof(ConvSmem<BN>);
+    static unsigned long long opted = 0;
+    cudaError_t attr = ertm::smem_opt_in(k_conv3s<BN, EP>, smem, &opted);
+    if (attr != cudaSuccess) return attr;
+    const long long M = (long long)x.nb * x.h * x.w;
+    dim3 grid((unsigned)(M / BM), (N + BN - 1) / BN);
+    k_conv3s<BN, EP><<<grid, NT, smem, st>>>(x, w, N, ep, err);
+    return cudaGetLastError();
+}
+
+// 3x3 convolution of x with weights w [N][9 * x.c] (tap-major K): the row kernel
+// where the layer fits it, else the implicit-im2col GEMM
+template <class EP>
+cudaError_t conv3(const Act& x, const bf16* w, int N, const EP& ep, int* err, cudaStream_t st)
+{
+    if (conv3s_fits(x)) {
+        if (N <= 16) return conv3s_bn<16>(x, w, N, ep, err, st);
+        if (N <= 32) return conv3s_bn<32>(x, w, N, ep, err, st);
+        if (N <= 64) return conv3s_bn<64>(x, w, N, ep, err, st);
+        return conv3s_bn<128>(x, w, N, ep, err, st);
+    }
+    const int M = x.nb * x.h * x.w, K = 9 * x.c;
+    LoadConv3 la{x, M, K};
+    LoadRows lb{w, N, K, K};
+    return gemm(la, lb, ep, M, N, K, 1, err, st);
+}
+
+// ---------------------------------------------------------------------------
 // Elementwise kernels
 // ---------------------------------------------------------------------------
 // 2x2 max pooling of an NHWC view into a dense NHWC output with C channels
@@ -640,28 +802,25 @@ int ertm_nn_conv3x3(const ertm_nn_act* x, const void* w, const float* bias, cons
 {
     if (!act_ok(x) || !w || !y || (!y32 && !act_ok(y))) return ERTM_EINVAL;
     if (y->n != x->n || y->h != x->h || y->w != x->w) return ERTM_EINVAL;
-    const int M = x->n * x->h * x->w, N = y->c, K = 9 * x->c;
-    LoadConv3 la{act_of(x), M, K};
-    LoadRows lb{reinterpret_cast<const bf16*>(w), N, K, K};
+    const int M = x->n * x->h * x->w, N = y->c;
+    const bf16* wb = reinterpret_cast<const bf16*>(w);
     cudaStream_t st = (cudaStream_t)stream;
     if (y32) {
         EpiF32 ep{y32, y->cstride, N, M, bias};
-        return rc_of(gemm(la, lb, ep, M, N, K, 1, err, st));
+        return rc_of(conv3(act_of(x), wb, N, ep, err, st));
     }
     EpiAct ep{reinterpret_cast<bf16*>(const_cast<void*>(y->data)), y->cstride, y->coff, N, M, bias, relu};
-    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, st));
+    return rc_of(conv3(act_of(x), wb, N, ep, err, st));
 }
 
 int ertm_nn_conv3x3_dgrad(const ertm_nn_act* dy, const void* wflip, const ertm_nn_act* dx, const ertm_nn_act* mask,
                           int* err, void* stream)
 {
     if (!act_ok(dy) || !wflip || !act_ok(dx)) return ERTM_EINVAL;
-    const int M = dy->n * dy->h * dy->w, N = dx->c, K = 9 * dy->c;
-    LoadConv3 la{act_of(dy), M, K};
-    LoadRows lb{reinterpret_cast<const bf16*>(wflip), N, K, K};
+    const int M = dy->n * dy->h * dy->w, N = dx->c;
     EpiGrad ep{reinterpret_cast<bf16*>(const_cast<void*>(dx->data)), dx->cstride, dx->coff, N, M,
                mask ? reinterpret_cast<const bf16*>(mask->data) : nullptr};
-    return rc_of(gemm(la, lb, ep, M, N, K, 1, err, (cudaStream_t)stream));
+    return rc_of(conv3(act_of(dy), reinterpret_cast<const bf16*>(wflip), N, ep, err, (cudaStream_t)stream));
 }
 
 int ertm_nn_conv3x3_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* dw, int splitk, int* err, void* stream)

@@ -42,7 +42,12 @@ def _nchw(t):
     return t.permute(0, 3, 1, 2)
 
 
-@pytest.mark.parametrize("ci,co,h,w", [(8, 16, 16, 24), (32, 64, 8, 8), (16, 128, 20, 12)])
+# widths that are multiples of 128 with 16-channel groups run the row kernel (taps as
+# shifted operand windows), the others the implicit-im2col GEMM; (8, 16, 3, 128)
+# runs the forward on the GEMM (8 input channels) and the input gradient on the row kernel
+@pytest.mark.parametrize("ci,co,h,w", [(8, 16, 16, 24), (32, 64, 8, 8), (16, 128, 20, 12),
+                                       (16, 16, 4, 128), (32, 64, 3, 256), (128, 64, 2, 128),
+                                       (16, 128, 2, 128), (8, 16, 3, 128), (64, 32, 2, 384)])
 def test_conv3x3_forward_and_gradients(env, ci, co, h, w):
     torch, nn, ops, dev = env
     F = torch.nn.functional

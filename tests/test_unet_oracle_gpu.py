@@ -51,18 +51,18 @@ def _half(buf, key, c):
     return buf[key]
 
 
-def _setup():
+def _setup(shape=(2, 32, 48)):
     import torch
     nn = importlib.import_module(PKG + ".nn")
     dev = torch.device("cuda", 0)
     net = nn.UNet(dev, seed=5)
     g = torch.Generator(device="cpu").manual_seed(6)
-    x = torch.randn(2, 32, 48, 3, generator=g)
-    target = torch.randn(2, 32, 48, 3, generator=g)
+    x = torch.randn(*shape, 3, generator=g)
+    target = torch.randn(*shape, 3, generator=g)
     loss = float(net.loss_grad(x.to(dev), target.to(dev)))
     torch.cuda.synchronize()
     assert int(net.ops.err.item()) == 0
-    Bt, Gt = net.bufs[(2, 32, 48)]
+    Bt, Gt = net.bufs[tuple(shape)]
     B = {k: _np(v) for k, v in Bt.items()}
     G = {k: _np(v) for k, v in Gt.items()}
     params = {k: (p.w.cpu().numpy(), p.b.cpu().numpy()) for k, p in net.params.items()}
@@ -71,9 +71,12 @@ def _setup():
     return net, x.numpy().astype(np.float64), target.numpy().astype(np.float64), loss, B, G, params, mine
 
 
-def test_unet_layers_match_the_fp64_oracle():
+# (1, 16, 256): levels 0 and 1 (widths 256, 128) run their 3x3 convolutions on
+# the row kernel, the rest on the implicit-im2col GEMM
+@pytest.mark.parametrize("shape", [(2, 32, 48), (1, 16, 256)])
+def test_unet_layers_match_the_fp64_oracle(shape):
     import unet_oracle as U
-    net, x, target, loss, B, G, params, mine = _setup()
+    net, x, target, loss, B, G, params, mine = _setup(shape)
     ref = U.Net(params, bf16=True)
     xin = np.zeros(B["in0"].shape)
     xin[..., :U.IN_C] = x
