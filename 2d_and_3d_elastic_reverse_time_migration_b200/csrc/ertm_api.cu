@@ -1176,6 +1176,12 @@ int ertm_rtm_multi(ertm_ctx* const* ctx, int n, const ertm_shot* shots, const fl
     Range range("ertm rtm multi");
     const cudaStream_t st = c0->stream;
     const bool cpml = c0->cfg.boundary == ERTM_BOUNDARY_CPML;
+    // every context's boundary profiles on the device before any kernel reads them
+    // (the tuner's trial steps run on context 0)
+    for (int q = 0; q < n; q++) {
+        ertm_ctx* c = ctx[q];
+        if ((rc = upload_profiles(c, c->cfg.pml_vmax > 0 ? c->cfg.pml_vmax : c->vpmax[1]))) return rc;
+    }
     int kchunk = choose_kchunk(c0->g, c0->R, c0->device);
     if (c0->cfg.autotune == 1 && (rc = autotune_kchunk(c0, 1, &kchunk))) return rc;
     const int chunks = (c0->g.nz + kchunk - 1) / kchunk;
