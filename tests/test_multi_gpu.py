@@ -91,7 +91,7 @@ def test_multi_argument_checks(ertm, orc):
     vp, vs, rho = model(deeper.cfg.shape, seed=3)
     deeper.set_model(ertm.MIGRATION_MODEL, vp, vs, rho)
     with pytest.raises(ertm.ErtmError):
-        ertm.rtm_multi([ctxs[0], deeper], sh, data)
+        ertm.rtm_multi([ctxs[0], deeper], [sh[0], sh[0]], [data[0], data[0]])
     flat = ertm.Context(product_config(ertm, "2d_r4_cpml", 50))
     vp, vs, rho = model(flat.cfg.shape, seed=4)
     flat.set_model(ertm.MIGRATION_MODEL, vp, vs, rho)
