@@ -21,6 +21,11 @@
 // R-row, 64-column stage at byte ((k / 8) * R + r) * 16 + (k % 8) * 2, i.e. the
 // 8 x 16-byte core matrices of the canonical layout with SBO = 128 bytes
 // (next 8 rows) and LBO = R * 16 bytes (next 8 K elements).
+//
+// 3x3 convolutions of layers 128 pixels wide or wider (16-channel input
+// groups) skip the im2col gather: k_conv3s stages the three input rows around
+// a 128-pixel output row once per channel group and feeds the nine taps as
+// operand windows shifted by one pixel (16 bytes) each (see its comment).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -775,10 +780,19 @@ Act act_of(const ertm_nn_act* a)
     return Act{reinterpret_cast<const bf16*>(a->data), a->n, a->h, a->w, a->cstride, a->coff, a->c};
 }
 
+// the operand copies move 16-byte chunks: every matrix starts on a 16-byte boundary
+bool aligned16(const void* p) { return p && ((uintptr_t)p % 16) == 0; }
+bool same_grid(const ertm_nn_act* a, const ertm_nn_act* b) { return a->n == b->n && a->h == b->h && a->w == b->w; }
 bool act_ok(const ertm_nn_act* a)
 {
     return a && a->data && a->n > 0 && a->h > 0 && a->w > 0 && a->c > 0 && a->c % 8 == 0 && a->coff % 8 == 0 &&
            a->cstride % 8 == 0 && a->coff + a->c <= a->cstride && ((uintptr_t)a->data % 16) == 0;
+}
+// a ReLU mask is read at the output's own element offsets
+bool mask_ok(const ertm_nn_act* mask, const ertm_nn_act* dx)
+{
+    return !mask || (act_ok(mask) && same_grid(mask, dx) && mask->cstride == dx->cstride && mask->coff == dx->coff &&
+                     mask->c == dx->c);
 }
 
 }  // namespace
@@ -790,7 +804,7 @@ extern "C" {
 
 int ertm_nn_gemm(const void* a, const void* b, float* d, int M, int N, int K, int* err, void* stream)
 {
-    if (!a || !b || !d || M < 1 || N < 1 || K < 1 || K % 8) return ERTM_EINVAL;
+    if (!aligned16(a) || !aligned16(b) || !d || M < 1 || N < 1 || K < 1 || K % 8) return ERTM_EINVAL;
     LoadRows la{reinterpret_cast<const bf16*>(a), M, K, K};
     LoadRows lb{reinterpret_cast<const bf16*>(b), N, K, K};
     EpiF32 ep{d, N, N, M, nullptr};
@@ -800,7 +814,7 @@ int ertm_nn_gemm(const void* a, const void* b, float* d, int M, int N, int K, in
 int ertm_nn_conv3x3(const ertm_nn_act* x, const void* w, const float* bias, const ertm_nn_act* y, int relu,
                     float* y32, int* err, void* stream)
 {
-    if (!act_ok(x) || !w || !y || (!y32 && !act_ok(y))) return ERTM_EINVAL;
+    if (!act_ok(x) || !aligned16(w) || !y || (!y32 && !act_ok(y))) return ERTM_EINVAL;
     if (y->n != x->n || y->h != x->h || y->w != x->w) return ERTM_EINVAL;
     const int M = x->n * x->h * x->w, N = y->c;
     const bf16* wb = reinterpret_cast<const bf16*>(w);
@@ -816,7 +830,8 @@ int ertm_nn_conv3x3(const ertm_nn_act* x, const void* w, const float* bias, cons
 int ertm_nn_conv3x3_dgrad(const ertm_nn_act* dy, const void* wflip, const ertm_nn_act* dx, const ertm_nn_act* mask,
                           int* err, void* stream)
 {
-    if (!act_ok(dy) || !wflip || !act_ok(dx)) return ERTM_EINVAL;
+    if (!act_ok(dy) || !aligned16(wflip) || !act_ok(dx) || !same_grid(dy, dx)) return ERTM_EINVAL;
+    if (!mask_ok(mask, dx)) return ERTM_EINVAL;
     const int M = dy->n * dy->h * dy->w, N = dx->c;
     EpiGrad ep{reinterpret_cast<bf16*>(const_cast<void*>(dx->data)), dx->cstride, dx->coff, N, M,
                mask ? reinterpret_cast<const bf16*>(mask->data) : nullptr};
@@ -843,7 +858,8 @@ int ertm_nn_conv3x3_wgrad(const ertm_nn_act* x, const ertm_nn_act* dy, float* dw
 int ertm_nn_up2(const ertm_nn_act* x, const void* u, const float* bias, const ertm_nn_act* y, int relu, int* err,
                 void* stream)
 {
-    if (!act_ok(x) || !u || !act_ok(y) || y->h != 2 * x->h || y->w != 2 * x->w || y->n != x->n) return ERTM_EINVAL;
+    if (!act_ok(x) || !aligned16(u) || !act_ok(y) || y->h != 2 * x->h || y->w != 2 * x->w || y->n != x->n)
+        return ERTM_EINVAL;
     const int M = x->n * x->h * x->w, N = 4 * y->c, K = x->c;
     Act xa = act_of(x);
     // a plain-rows view of x works only for dense channels; use the 1x1 gather otherwise
@@ -860,7 +876,9 @@ int ertm_nn_up2(const ertm_nn_act* x, const void* u, const float* bias, const er
 int ertm_nn_up2_dgrad(const ertm_nn_act* dy, const void* ut, const ertm_nn_act* dx, const ertm_nn_act* mask,
                       int* err, void* stream)
 {
-    if (!act_ok(dy) || !ut || !act_ok(dx) || dy->h != 2 * dx->h || dy->w != 2 * dx->w) return ERTM_EINVAL;
+    if (!act_ok(dy) || !aligned16(ut) || !act_ok(dx) || dy->h != 2 * dx->h || dy->w != 2 * dx->w || dy->n != dx->n ||
+        !mask_ok(mask, dx))
+        return ERTM_EINVAL;
     const int M = dx->n * dx->h * dx->w, N = dx->c, K = 4 * dy->c;
     LoadUp2 la{act_of(dy), M, K};
     LoadRows lb{reinterpret_cast<const bf16*>(ut), N, K, K};

@@ -5,9 +5,11 @@ level, 2x2 max pooling down, 2x2 stride-2 transposed convolutions + ReLU up,
 skip connections by channel concatenation, a final 3x3 convolution) maps the
 first LSRTM gradient (g_vp, g_vs, g_rho) to the reflectivity (r_vp, r_vs, r_rho)
 that several CG iterations would reach.  Every convolution, its input and weight
-gradients run on the hand-written tcgen05 GEMM of csrc/nn.cu (BF16 activations
-and weights, FP32 accumulation); pooling, bias gradients, the loss and Adam are
-hand-written kernels too.  Torch only allocates the buffers (plumbing) and
+gradients run on the hand-written tcgen05 kernels of csrc/nn.cu (BF16 activations
+and weights, FP32 accumulation): an implicit-im2col GEMM, and for the 3x3
+convolutions of layers at least 128 pixels wide a row kernel that reads the
+nine taps from three staged input rows; pooling, bias gradients, the loss and
+Adam are hand-written kernels too.  Torch only allocates the buffers (plumbing) and
 calls nothing but the library on them.
 
 Activations are NHWC BF16; channel counts are padded to multiples of 8 (input

@@ -132,3 +132,27 @@ void err(const char *fmt, ...);
     src.write_text(body)
     subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-Wno-unused-function", "-I",
                     os.path.join(REPO, "include"), "-c", str(src), "-o", str(tmp_path / "shim.o")], check=True)
+
+
+def test_nn_entry_points_validate_before_touching_a_device(ertm):
+    """The tensor-core entry points refuse, before any launch, operands that their
+    16-byte copies or their epilogues cannot take: a weight pointer off a 16-byte
+    boundary, an input gradient of another grid than the output gradient, a ReLU
+    mask that is not laid out like the gradient it masks (host memory, no GPU)."""
+    import numpy as np
+    L = ertm.lib()
+    buf = np.zeros(1 << 14, np.uint16)
+    p = buf.ctypes.data + (-buf.ctypes.data % 16)
+
+    def act(n, h, w, c, cs=None, off=0):
+        a = ertm._NnAct()
+        a.data, a.n, a.h, a.w = p, n, h, w
+        a.cstride, a.coff, a.c = cs or c, off, c
+        return a
+
+    x, y = act(1, 4, 8, 16), act(1, 4, 8, 16)
+    assert L.ertm_nn_conv3x3(C.byref(x), p + 2, None, C.byref(y), 1, None, None, None) == -1
+    assert L.ertm_nn_gemm(p + 8, p, p, 16, 16, 16, None, None) == -1
+    assert L.ertm_nn_conv3x3_dgrad(C.byref(x), p, C.byref(act(1, 4, 4, 16)), None, None, None) == -1
+    dx, mask = act(1, 4, 8, 16, cs=32), act(1, 4, 8, 16, cs=32, off=16)
+    assert L.ertm_nn_conv3x3_dgrad(C.byref(x), p, C.byref(dx), C.byref(mask), None, None) == -1
