@@ -409,7 +409,10 @@ int ertm_mute_direct(const ertm_shot *shot, float *data, int nt, float dx, float
  * memory (tcgen05.mma), FP32 master weights.  All pointers are device
  * pointers; calls are asynchronous on `stream` (NULL: the legacy stream).
  * `err` (device int, may be NULL) is set non-zero if a kernel's bounded wait
- * gave up.  Channel counts, offsets and strides are multiples of 8. */
+ * gave up.  Channel counts, offsets and strides are multiples of 8; activation
+ * and weight pointers start on a 16-byte boundary; an input gradient has the
+ * grid of its output gradient, and a ReLU mask the layout (grid, stride,
+ * channel offset and count) of the gradient it masks (ERTM_EINVAL otherwise). */
 typedef struct {
     const void *data;        /* BF16, pixel p = (n*h + y)*w + x at data + p*cstride + coff */
     int n, h, w;             /* batch, height, width */
