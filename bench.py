@@ -62,7 +62,8 @@ def parse():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the step kernels (profiling cases)")
     ap.add_argument("--workload", default="shot",
-                    choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op", "lsrtm-cg", "refstep"],
+                    choices=["shot", "windows", "unet", "lsrtm", "lsrtm-op", "lsrtm-cg", "refstep",
+                             "passcheck"],
                     help="windows: batched aperture windows; unet: one U-Net training step at "
                          "256x512, batch 16; lsrtm: learned vs plain CG (each its own line); "
                          "lsrtm-op: Born forward + adjoint per shot on the 880x480 GSLS-3 LSRTM grid; "
@@ -128,9 +129,11 @@ class ClockSampler:
         sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
         mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        pw = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows),
+                "power_w": statistics.median(pw) if pw else None}
 
 
 class CpuOracle:
@@ -289,6 +292,48 @@ def run_windows(args):
                    "window": "U[64,192]^2 + 40-cell C-PML", "nt": "U[2000,3500]",
                    "cell_updates": updates, "autotune": 1},
         "clocks": clk}), flush=True)
+
+
+def run_passcheck(args):
+    """The 3D step inside a pass against the same kernels launched one step at a
+    time: a source pass (2666 steps, CUDA events around the pass) and then 2000
+    step pairs each followed by a host synchronisation (ertm_time_kernels), with
+    the SM clock and board power sampled during each."""
+    import torch
+    ertm = importlib.import_module(PKG)
+    synth = importlib.import_module(PKG + ".synthetic")
+    wl = workload(False)
+    nz, ny, nx = wl.shape
+    ctx = ertm.Context(ertm.Config(nx=nx, ny=ny, nz=nz, dx=wl.dx, dy=wl.dy, dz=wl.dz, dt_ms=wl.dt_ms,
+                                   nt=wl.nt, order=8, boundary=ertm.BOUNDARY_CPML, pml=(wl.pml,) * 6))
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream(dev)
+    ctx.set_stream(st.cuda_stream)
+    ctx.set_model(ertm.MIGRATION_MODEL, wl.svp, wl.svs, wl.srho)
+    shot = _shot(ertm, wl, synth, 0)
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    ctx.forward_together_using_smoothed_model(shot)          # warm-up pass
+    torch.cuda.synchronize(dev)
+    nsrc = 2 * wl.nt // 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(uuid)
+    e0.record(st)
+    ctx.forward_together_using_smoothed_model(shot)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    c_pass = clk.stop()
+    pass_ms = e0.elapsed_time(e1) / nsrc
+    n = 2000
+    clk = ClockSampler(uuid)
+    ms_s, ms_v = ctx.time_kernels(shot, n)
+    c_sync = clk.stop()
+    print(json.dumps({"workload": wl.name, "pass": {"ms_per_step": round(pass_ms, 4), "steps": nsrc,
+                                                    "clocks": c_pass},
+                      "synchronised": {"stress_ms": round(ms_s / n, 4), "velocity_ms": round(ms_v / n, 4),
+                                       "ms_per_step": round((ms_s + ms_v) / n, 4), "steps": n,
+                                       "clocks": c_sync}}), flush=True)
+    ctx.close()
 
 
 def run_unet(args):
@@ -613,6 +658,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "passcheck":
+        return run_passcheck(args)
     if args.workload == "windows":
         return run_windows(args)
     if args.workload == "unet":
