@@ -492,39 +492,47 @@ cudaError_t gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, 
 // 3x3 convolution over rows of 128 pixels, taps as shifted operand windows
 // ---------------------------------------------------------------------------
 // For a layer whose width is a multiple of 128 and whose input channels come in
-// groups of 16, a CTA computes the 128 x BN output tile of 128 consecutive
-// pixels of one image row.  Per group of 16 input channels a stage holds the
-// three input rows around that output row, 130 pixels each (the padding column
-// on either side, zero outside the image), as planes of 16-byte chunks (8
-// channels of one pixel per chunk, plane [row][chunk]), and the group's weights
-// for the nine taps.  In the K-major no-swizzle layout of tcgen05 an operand row
-// is one 16-byte chunk and 8 consecutive rows form a core matrix, so the A
-// operand of tap (ky, kx) is the plane of row ky read from pixel kx on: nine
-// MMAs of K = 16 per stage read the staged rows in place.  A stage copies
-// 3 x 130 pixels of input against 128 x 9 for an im2col tile.
+// groups of 16, a CTA computes RO output tiles of 128 x BN: 128 consecutive
+// pixels of RO consecutive image rows.  Per group of 16 input channels a stage
+// holds the RO + 2 input rows around those output rows, 130 pixels each (the
+// padding column on either side, zero outside the image), as planes of 16-byte
+// chunks (8 channels of one pixel per chunk, plane [row][chunk]), and the
+// group's weights for the nine taps.  In the K-major no-swizzle layout of
+// tcgen05 an operand row is one 16-byte chunk and 8 consecutive rows form a
+// core matrix, so the A operand of tap (ky, kx) for output row r is the plane of
+// input row r + ky read from pixel kx on: 9 RO MMAs of K = 16 per stage read the
+// staged rows in place, each output row into its own TMEM accumulator.  A stage
+// copies (RO + 2) x 130 pixels of input against RO x 128 x 9 for im2col tiles,
+// and the weights once for RO rows.
 constexpr int CV_PX = 130;                   // pixels per staged row
 constexpr int CV_PLANE = CV_PX * 16;         // bytes of one [row][chunk] plane
-constexpr int CV_A = 6 * CV_PLANE;           // 3 rows x 2 chunks
-template <int BN>
+template <int BN, int RO>
 struct ConvSmem {
     static constexpr int NS = 3;
-    static constexpr int A_PAD = (CV_A + 127) / 128 * 128;
+    static constexpr int A_BYTES = (RO + 2) * 2 * CV_PLANE;   // RO + 2 rows x 2 chunks
+    static constexpr int A_PAD = (A_BYTES + 127) / 128 * 128;
     alignas(128) uint8_t a[NS][A_PAD];
     alignas(128) uint8_t b[NS][9 * 2 * BN * 16];   // [tap][chunk][BN rows x 16 B]
     uint64_t bar[NS];
     uint32_t tmem;
 };
+// TMEM columns of RO accumulators of BN columns (a power of two, at least 32)
+constexpr int conv_tcols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512; }
 
-template <int BN, class EP>
+template <int BN, int RO, class EP>
 __global__ void __launch_bounds__(NT) k_conv3s(Act x, const bf16* __restrict__ w, int N, EP ep, int* err)
 {
     extern __shared__ __align__(128) uint8_t smraw[];
-    ConvSmem<BN>& S = *reinterpret_cast<ConvSmem<BN>*>(smraw);
-    constexpr int NS = ConvSmem<BN>::NS;
-    constexpr int TCOLS = BN < 32 ? 32 : BN;
+    ConvSmem<BN, RO>& S = *reinterpret_cast<ConvSmem<BN, RO>*>(smraw);
+    constexpr int NS = ConvSmem<BN, RO>::NS;
+    constexpr int TCOLS = conv_tcols(RO * BN);
+    static_assert(RO * BN <= 512, "TMEM columns");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int x0 = m0 % x.w, t0 = m0 / x.w, y0 = t0 % x.h, nb = t0 / x.h;
+    const int n0 = blockIdx.y * BN;
+    const int tiles_x = x.w / BM, groups_y = x.h / RO;
+    const int x0 = (int)(blockIdx.x % tiles_x) * BM;
+    const int t1 = (int)(blockIdx.x / tiles_x);
+    const int y0 = (t1 % groups_y) * RO, nb = t1 / groups_y;
     const int G = x.c / 16, ldw = 9 * x.c;
     if (threadIdx.x == 0) {
         for (int q = 0; q < NS; q++) mbar_init(&S.bar[q], 1);
@@ -549,7 +557,7 @@ __global__ void __launch_bounds__(NT) k_conv3s(Act x, const bf16* __restrict__ w
             uint8_t* A = S.a[g % NS];
             uint8_t* Bs = S.b[g % NS];
             const int c0 = x.off + 16 * g;
-            for (int q = threadIdx.x; q < 3 * CV_PX * 2; q += NT) {
+            for (int q = threadIdx.x; q < (RO + 2) * CV_PX * 2; q += NT) {
                 // consecutive threads take the two chunks of consecutive pixels
                 const int kc = q & 1, pr = q >> 1, dy = pr / CV_PX, px = pr - dy * CV_PX;
                 const int yy = y0 + dy - 1, xx = x0 + px - 1;
@@ -576,12 +584,14 @@ __global__ void __launch_bounds__(NT) k_conv3s(Act x, const bf16* __restrict__ w
             tc_fence_after();
             const uint32_t a0 = su32(S.a[sl]), b0 = su32(S.b[sl]);
 #pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
-                const int ky = tap / 3, kx = tap % 3;
-                const uint64_t da = sdesc(a0 + (uint32_t)(ky * 2 * CV_PLANE + kx * 16), CV_PLANE);
-                const uint64_t db = sdesc(b0 + (uint32_t)(tap * 2 * BN * 16), BN * 16);
-                umma(tmem, da, db, IDESC, (g > 0 || tap > 0) ? 1u : 0u);
-            }
+            for (int r = 0; r < RO; r++)
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int ky = tap / 3, kx = tap % 3;
+                    const uint64_t da = sdesc(a0 + (uint32_t)((r + ky) * 2 * CV_PLANE + kx * 16), CV_PLANE);
+                    const uint64_t db = sdesc(b0 + (uint32_t)(tap * 2 * BN * 16), BN * 16);
+                    umma(tmem + (uint32_t)(r * BN), da, db, IDESC, (g > 0 || tap > 0) ? 1u : 0u);
+                }
             umma_commit(&S.bar[sl]);
         }
         // refill slot (g - 1) % NS with group g + NS - 1 once group g-1's MMAs read it
@@ -596,13 +606,16 @@ __global__ void __launch_bounds__(NT) k_conv3s(Act x, const bf16* __restrict__ w
     const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
     tc_fence_after();
     if (G > 0 && all_ok) {
-        const int m = m0 + warp * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 8) {
-            float v[8];
-            tmem_ld8(trow + c, v);
-            ep(m, n0 + c, v);
+        for (int r = 0; r < RO; r++) {
+            const int m = ((nb * x.h + y0 + r) * x.w + x0) + warp * 32 + lane;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 8) {
+                float v[8];
+                tmem_ld8(trow + (uint32_t)(r * BN + c), v);
+                ep(m, n0 + c, v);
+            }
         }
     }
     if (!ok && err) atomicExch(err, NN_WAIT);
@@ -620,17 +633,25 @@ bool conv3s_fits(const Act& x)
            (reinterpret_cast<uintptr_t>(x.p) & 15) == 0;
 }
 
+template <int BN, int RO, class EP>
+cudaError_t conv3s_launch(const Act& x, const bf16* w, int N, const EP& ep, int* err, cudaStream_t st)
+{
+    const size_t smem = sizeof(ConvSmem<BN, RO>);
+    static unsigned long long opted = 0;
+    cudaError_t attr = ertm::smem_opt_in(k_conv3s<BN, RO, EP>, smem, &opted);
+    if (attr != cudaSuccess) return attr;
+    const long long tiles = (long long)x.nb * (x.h / RO) * (x.w / BM);
+    dim3 grid((unsigned)tiles, (N + BN - 1) / BN);
+    k_conv3s<BN, RO, EP><<<grid, NT, smem, st>>>(x, w, N, ep, err);
+    return cudaGetLastError();
+}
+
+// two output rows per CTA where the height allows (the weights are staged once
+// for both), else one
 template <int BN, class EP>
 cudaError_t conv3s_bn(const Act& x, const bf16* w, int N, const EP& ep, int* err, cudaStream_t st)
 {
-    const size_t smem = sizeof(ConvSmem<BN>);
-    static unsigned long long opted = 0;
-    cudaError_t attr = ertm::smem_opt_in(k_conv3s<BN, EP>, smem, &opted);
-    if (attr != cudaSuccess) return attr;
-    const long long M = (long long)x.nb * x.h * x.w;
-    dim3 grid((unsigned)(M / BM), (N + BN - 1) / BN);
-    k_conv3s<BN, EP><<<grid, NT, smem, st>>>(x, w, N, ep, err);
-    return cudaGetLastError();
+    return x.h % 2 == 0 ? conv3s_launch<BN, 2>(x, w, N, ep, err, st) : conv3s_launch<BN, 1>(x, w, N, ep, err, st);
 }
 
 // 3x3 convolution of x with weights w [N][9 * x.c] (tap-major K): the row kernel
