@@ -1,5 +1,8 @@
 """Multi-shot RTM with on-device stacking (ertm_rtm_batch) and the shot-parallel
-driver on one rank (GPU)."""
+driver on one rank (GPU).  The stack is checked against the sum of single-shot
+migrations (ertm_rtm_shot), the call that test_parity_gpu.py pins to the FP64
+oracle on the same kind of grid; the batched windows of test_windows_gpu.py are
+also checked against the oracle directly."""
 import importlib
 
 import numpy as np
